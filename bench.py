@@ -1,0 +1,419 @@
+#!/usr/bin/env python3
+"""Benchmark of the SPEX polarisation hot path on B200: chi0 band-pair TFLOP/s.
+
+Workload (one GPU): N_MB=1200 mixed-basis functions, 64 k points, 40 occupied x
+400 unoccupied bands (P = 1,024,000 band pairs), 24 imaginary frequencies, 1% of
+the pairs near-degenerate (|e_n'-e_n| < 1e-6 eV). One step is one full
+accumulation chi0_IJ(w) = sum_p M_Ip w_p(w) M*_Jp for all 24 frequencies into the
+packed Hermitian output, output zeroed first (as `susceptibility` does).
+
+  value        TFLOP/s of the headline (split-precision) path, inputs resident in
+               HBM; algorithmic flops 8*N^2*P*Nw (full complex Gram)
+  fp64         the plain FP64 drop-in path on the same inputs
+  e2e          the same metric through the host-pointer drop-in call
+               (spx_chi0_accumulate): cprod from pinned host memory every step,
+               susceph copied back every step
+  roofline     dominant kernel (the band-pair accumulation): achieved vs measured peak
+  cpu_baseline the oracle port of the reference loop on the host cores, bounded sample
+  --impl reference  times the reference CPU loop (oracle port) alone.
+
+Multi-GPU: the pair axis is sharded (the reference's Mblocks split over
+(k, occ, unocc)); each rank accumulates its share and the packed output is
+summed with one NCCL reduce to rank 0 (Mreduce analogue).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "chi0 band-pair TFLOP/s, split-precision vs FP64 on one B200 at <=1e-6 rel err"
+UNIT = "TFLOP/s"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), d.get("bf16_tflops_sustained", 1400.0), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for k, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(k)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(w, budget_s: float = 15.0, threads: int = 0):
+    """Faithful reference loop (oracle port) on a bounded sample: all (i<=j) elements of
+    the first J columns, timed, then scaled to the full element count."""
+    import oracle
+    from project1_b200 import inputs
+    threads = threads or os.cpu_count() or 1
+    d = inputs.pair_ediff(w)
+    om = inputs.frequencies(w.nw)
+    wt = oracle.weights(d, om, None, 1.0 / w.nk)
+    # probe with 2 columns (3 elements), then size the sample to the budget
+    ncol = 2
+    m = inputs.cprod_host(w, 0, ncol)
+    t0 = time.perf_counter()
+    oracle.chi0(m, wt, threads=min(threads, 3))
+    per_elem = (time.perf_counter() - t0) / 3 * min(threads, 3)   # thread-seconds per element
+    target = budget_s * threads / per_elem
+    ncol = int(max(2, min(w.nbas, (np.sqrt(8 * target + 1) - 1) / 2)))
+    m = inputs.cprod_host(w, 0, ncol)
+    nel = ncol * (ncol + 1) // 2
+    t0 = time.perf_counter()
+    oracle.chi0(m, wt, threads=threads)
+    dt = time.perf_counter() - t0
+    full_elems = w.nbas * (w.nbas + 1) / 2
+    t_full = dt * full_elems / nel
+    return {"value": w.flops / t_full / 1e12, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"faithful per-(i,j) ddot loop (src/susceptibility.f:1182-1240) over the "
+                      f"{nel} elements i<=j<{ncol} of all {w.nw} frequencies and all {w.npair} pairs, "
+                      f"{dt:.1f} s, scaled by the element count to {full_elems:.0f} elements",
+            "seconds_sample": dt, "seconds_full_estimate": t_full}
+
+
+def run_reference(args):
+    from project1_b200 import inputs
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = inputs.CONFIGS[args.workload]
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(w, budget_s=args.ref_budget)
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(w, budget_s=args.ref_budget))
+    v = statistics.median([x["value"] for x in vals])
+    cb = dict(vals[-1])
+    cb["value"] = v
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * w.flops / (v * 1e12), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(w), "nbas": w.nbas, "npair": w.npair, "nw": w.nw},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def workload_name(w):
+    return (f"{w.name}: chi0 N_MB={w.nbas}, {w.nk} k x {w.nocc} occ x {w.nunocc} unocc "
+            f"(P={w.npair}), {w.nw} imaginary frequencies"
+            + (f", {w.degenerate_frac:.0%} degenerate pairs" if w.degenerate_frac else ""))
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import project1_b200 as spx
+    from project1_b200 import inputs
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    w = inputs.CONFIGS[args.workload]
+    # shard the pair axis: rank r owns a contiguous block of k points (Mblocks over k)
+    P = w.npair
+    p_lo = rank * P // world
+    p_hi = (rank + 1) * P // world
+    Pr = p_hi - p_lo
+    N, nw = w.nbas, w.nw
+    npk = spx.npack(N)
+    ctx = spx.Context(local)
+    stream = torch.cuda.current_stream(dev)
+
+    # inputs resident in HBM: M (N, P) column blocks generated on device, bit-identical
+    # to the host stream; energies / frequencies from the seeded host generator
+    M = torch.empty((N, Pr), dtype=torch.complex128, device=dev)
+    full_rows = P
+    # generate this rank's pair range: element (p, c) of the full matrix
+    gen = torch.empty((1, full_rows), dtype=torch.complex128, device=dev) if world > 1 else None
+    if world == 1:
+        ctx.gen_cmatrix_dev(w.seed, w.stream_id, M, P, scale=w.m_scale, stream=stream.cuda_stream)
+    else:
+        for c in range(N):
+            ctx.gen_cmatrix_dev(w.seed, w.stream_id, gen, P, col0=c, scale=w.m_scale, stream=stream.cuda_stream)
+            M[c].copy_(gen[0, p_lo:p_hi])
+        del gen
+    ediff_h = inputs.pair_ediff(w)
+    ediff = torch.from_numpy(ediff_h[p_lo:p_hi].copy()).to(dev)
+    omega_h = inputs.frequencies(nw)
+    omega = torch.from_numpy(omega_h).to(dev)
+    out = torch.zeros((nw, npk), dtype=torch.complex128, device=dev)
+    torch.cuda.synchronize()
+
+    def step(precision):
+        out.zero_()
+        st = ctx.chi0_accumulate_dev(M, ediff, omega, out, scale_all=1.0 / w.nk, precision=precision,
+                                     stream=stream.cuda_stream, stats=True)
+        if world > 1:
+            dist.reduce(out, 0)
+        return st
+
+    def timed(precision, warmup, steps, sampler=None):
+        for _ in range(warmup):
+            step(precision)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        if sampler:
+            sampler.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        gram_ms = []
+        launches = 0
+        for _ in range(steps):
+            st = step(precision)
+            gram_ms.append(st["ms_gram"])
+            launches += st["kernel_launches"]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        ms = e0.elapsed_time(e1) / steps
+        if world > 1:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, gram_ms, launches, clocks
+
+    avail = {"split": True}
+    try:
+        step("split")
+        torch.cuda.synchronize()
+    except spx.SpexGpuError as e:
+        avail["split"] = False
+        avail["split_error"] = str(e)
+    head = "split" if avail["split"] else "fp64"
+
+    sampler = ClockSampler(local) if rank == 0 else None
+    ms, gram_ms, launches, clocks = timed(head, args.warmup, args.steps, sampler)
+    value = w.flops / (ms * 1e-3) / 1e12   # whole job: all ranks' pairs / max-over-ranks time
+    # FP64 drop-in on the same inputs (secondary line; same kernel every step, 1 warm-up)
+    fp64 = None
+    if head == "split" and args.fp64_steps > 0:
+        ms64, gram64, _, _ = timed("fp64", 1, args.fp64_steps)
+        fp64 = {"value": w.flops / (ms64 * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms64,
+                "steps": args.fp64_steps, "warmup": 1, "kernel_ms": statistics.median(gram64)}
+
+    # e2e through the host-pointer drop-in call, cprod in pinned host memory
+    e2e = None
+    if args.e2e_steps > 0:
+        host = torch.empty((N, Pr), dtype=torch.complex128, pin_memory=True)
+        host.copy_(M)
+        out_h = np.zeros((npk, nw), dtype=np.complex128, order="F")
+        eh = ediff_h[p_lo:p_hi].copy()
+        ctx2 = spx.Context(local)
+        h2d = d2h = 0
+        for it in range(1 + args.e2e_steps):
+            if it == 1:
+                torch.cuda.synchronize()
+                if world > 1:
+                    dist.barrier()
+                t0 = time.perf_counter()
+            out_h[:] = 0
+            st = ctx2.chi0_accumulate_host_ptr(host.data_ptr(), Pr, Pr, N, eh, omega_h, out_h,
+                                               scale_all=1.0 / w.nk, precision=head)
+            if it >= 1:
+                h2d, d2h = st["h2d_bytes"], st["d2h_bytes"]
+        dt = (time.perf_counter() - t0) / args.e2e_steps
+        if world > 1:
+            t = torch.tensor([dt], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        e2e = {"value": w.flops / dt / 1e12, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3, "steps": args.e2e_steps,
+               "warmup": 1, "source": "pinned host memory"}
+        ctx2.close()
+        del host
+
+    # accuracy of the headline path vs the FP64 path, all elements (and FP64 vs oracle samples)
+    acc = None
+    if rank == 0 and world == 1 and head == "split" and args.check:
+        acc = accuracy_check(ctx, w, M, ediff, omega, stream, ediff_h, omega_h)
+
+    hbm, bf16, bf16s, src = peaks()
+    kernel_ms = statistics.median(gram_ms)
+    # the dominant kernel per step is the accumulation over all 24 frequencies: algorithmic
+    # flops 8 N^2 P Nw per step (per rank: its own pairs)
+    ach = w.flops * (Pr / P) / (kernel_ms * 1e-3) / 1e12
+    if head == "split":
+        roof = {"bound": "tensor", "achieved": ach, "peak": bf16s, "unit": UNIT, "frac": ach / bf16s,
+                "traffic": None, "peak_source": f"{src} bf16_tflops_sustained (kernel timed inside a long step)"}
+    else:
+        roof = {"bound": "tensor", "achieved": ach, "peak": None, "unit": UNIT, "frac": None, "traffic": None,
+                "peak_source": "FP64 DMMA has no measured peak on this pool"}
+
+    if rank == 0:
+        res = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16x3->f32->f64" if head == "split" else "f64",
+            "data": "synthetic (seeded Philox4x32-10 normals, uniform energies, Gauss-Legendre frequencies)",
+            "config": {"workload": workload_name(w), "nbas": N, "npair": P, "nw": nw,
+                       "headline_precision": head, "parallelism": f"pairs sharded over {world} GPU(s)",
+                       "l2": "inputs larger than L2 (M = %.1f GB)" % (16 * N * P / 1e9)},
+            "fp64": fp64, "e2e": e2e, "roofline": roof, "clocks": clocks,
+            "gpu_launches": launches, "kernel_ms_per_step": kernel_ms,
+            "flops_per_step": w.flops, "flops_hermitian_per_step": w.flops_hermitian,
+            "accuracy": acc, "split_available": avail,
+        }
+        if fp64:
+            res["speedup_vs_fp64"] = value / fp64["value"]
+        if world == 1 and args.cpu_budget > 0:
+            res["cpu_baseline"] = cpu_baseline(w, budget_s=args.cpu_budget)
+        print(json.dumps(res))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def accuracy_check(ctx, w, M, ediff, omega, stream, ediff_h, omega_h, nsample=24):
+    """Split vs FP64 on every element; FP64 vs the extended-precision oracle on sampled elements."""
+    import torch
+
+    import oracle
+    import project1_b200 as spx
+    from project1_b200 import inputs
+    N, nw = w.nbas, w.nw
+    outs = {}
+    for prec in ("split", "fp64"):
+        o = torch.zeros((nw, spx.npack(N)), dtype=torch.complex128, device=M.device)
+        ctx.chi0_accumulate_dev(M, ediff, omega, o, scale_all=1.0 / w.nk, precision=prec,
+                                stream=stream.cuda_stream)
+        outs[prec] = o
+    torch.cuda.synchronize()
+    a, b = outs["split"], outs["fp64"]
+    j = torch.arange(N, device=M.device)
+    dg = (j * (j + 1) // 2 + j)
+    d = b[:, dg].real.abs()                              # (nw, N)
+    iu = torch.triu_indices(N, N, device=M.device)
+    idx = iu[1] * (iu[1] + 1) // 2 + iu[0]
+    err = (a[:, idx] - b[:, idx]).abs() / torch.sqrt(d[:, iu[0]] * d[:, iu[1]])
+    fro = float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+    raw = (a[:, idx] - b[:, idx]).abs() / b[:, idx].abs().clamp_min(1e-300)
+    res = {"split_vs_fp64_max_normalized": float(err.max()), "split_vs_fp64_frobenius": fro,
+           "split_vs_fp64_raw_rel_median": float(raw.median()),
+           "split_vs_fp64_raw_rel_p99": float(torch.quantile(raw.flatten()[:: max(1, raw.numel() // 1000000)].float(), 0.99)),
+           "normalization": "|d chi_ij| / sqrt(|chi_ii chi_jj|) per frequency"}
+    # FP64 path vs oracle on sampled elements (columns regenerated on the host, same bits)
+    rng = np.random.default_rng(5)
+    wt = oracle.weights(ediff_h, omega_h, None, 1.0 / w.nk)
+    cols = sorted(set(rng.integers(0, N, nsample).tolist()) | {0, N - 1})
+    colv = {c: inputs.cprod_host(w, c, 1)[:, 0] for c in cols}
+    bh = b.cpu().numpy()
+    e64 = 0.0
+    es = 0.0
+    ah = a.cpu().numpy()
+    for k in range(len(cols) - 1):
+        i, jj = cols[k], cols[k + 1]
+        ref = oracle.chi0_element(colv[i], colv[jj], wt)
+        refi = oracle.chi0_element(colv[i], colv[i], wt).real
+        refj = oracle.chi0_element(colv[jj], colv[jj], wt).real
+        sc = np.sqrt(np.abs(refi * refj))
+        p = jj * (jj + 1) // 2 + i
+        e64 = max(e64, float(np.max(np.abs(bh[:, p] - ref) / sc)))
+        es = max(es, float(np.max(np.abs(ah[:, p] - ref) / sc)))
+    res["fp64_vs_oracle_sampled_max_normalized"] = e64
+    res["split_vs_oracle_sampled_max_normalized"] = es
+    res["oracle_samples"] = len(cols) - 1
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c0", "c1", "c2"])
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-budget", type=float, default=10.0)
+    ap.add_argument("--no-check", dest="check", action="store_false")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

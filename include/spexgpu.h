@@ -1,0 +1,146 @@
+/*
+ * spexgpu.h — C ABI of the B200 (sm_100a) Kohn-Sham polarisation library.
+ *
+ * The library replaces, inside SPEX 05.10, the HILBERT NONE band-pair
+ * accumulation of the imaginary-frequency polarisation and the wave-function
+ * products that feed it. Every entry point is `extern "C"`, takes plain
+ * pointers and 64-bit sizes, returns an int status (SPX_OK == 0, negative on
+ * error) and never aborts. spx_last_error() returns the message of the last
+ * failing call on a context.
+ *
+ * Array conventions follow the Fortran caller (column-major, 1-based indices
+ * in the reference become 0-based offsets here):
+ *   - complex arrays are interleaved (re, im) doubles: Fortran complex(8),
+ *     C99 double _Complex and cuDoubleComplex all share this layout;
+ *   - cprod(npair, nbas): band-pair index p fastest, with p = n' + nu*(n + no*k)
+ *     (unoccupied n' fastest, then occupied n, then k; reference
+ *     src/susceptibility.f:861-865 and :956-960), leading dimension ldc >= npair;
+ *   - susceph(nbas*(nbas+1)/2, nw): packed upper triangle, element (i, j) with
+ *     i <= j (0-based) at j*(j+1)/2 + i, frequency outermost
+ *     (src/susceptibility.f:1210, ij = j*(j-1)/2 + i in 1-based form).
+ *
+ * A context is bound to one device, is not thread-safe, and orders all of its
+ * work on one CUDA stream unless a stream is passed explicitly.
+ */
+#ifndef SPEXGPU_H
+#define SPEXGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPX_ABI_VERSION 1
+
+/* status codes */
+#define SPX_OK        0
+#define SPX_EINVAL   -1   /* bad argument (null pointer, negative size, ...)     */
+#define SPX_ENOMEM   -2   /* device or pinned-host allocation failed             */
+#define SPX_ECUDA    -3   /* a CUDA runtime call failed                          */
+#define SPX_ETIMEOUT -4   /* a bounded device-side wait ran out                  */
+#define SPX_ENOTSUP  -5   /* feature not available (no sm_100 device, ...)       */
+#define SPX_ENODEV   -6   /* no CUDA device                                      */
+
+/* precision of the band-pair accumulation */
+#define SPX_FP64  0       /* complex FP64 on the DMMA tensor path: the drop-in   */
+#define SPX_SPLIT 1       /* BF16 hi/mid/lo split on tcgen05, FP32 TMEM partials,
+                             FP64 reduction; weights always in FP64              */
+
+typedef struct spx_ctx spx_ctx;
+
+typedef struct spx_options {
+  int32_t struct_size;      /* sizeof(spx_options), for forward compatibility   */
+  int32_t verbose;          /* 0 = silent                                        */
+  int64_t workspace_limit;  /* device bytes the context may allocate, 0 = auto   */
+  int64_t pinned_limit;     /* pinned host staging bytes, 0 = auto               */
+  int32_t chunk_pairs;      /* band pairs per streamed chunk, 0 = auto           */
+  int32_t timeout_ms;       /* bound on every device-side wait, 0 = 4000 ms      */
+} spx_options;
+
+/* Per-call statistics filled by the accumulation entry points (may be NULL). */
+typedef struct spx_chi0_stats {
+  double  ms_total;         /* wall time of the call, host-observed              */
+  double  ms_gram;          /* device time of the band-pair accumulation kernels */
+  double  ms_prep;          /* device time of weight / operand preparation       */
+  double  flops;            /* algorithmic real flops, 8*N^2*P*nw                */
+  int64_t h2d_bytes;        /* host-to-device bytes moved by the call            */
+  int64_t d2h_bytes;        /* device-to-host bytes moved by the call            */
+  int32_t kernel_launches;  /* kernels launched by the call                      */
+  int32_t precision;        /* precision actually used                           */
+} spx_chi0_stats;
+
+/* ---- library and context --------------------------------------------------- */
+
+int         spx_abi_version(void);
+const char* spx_strerror(int status);
+
+/* Creates a context on `device` (CUDA ordinal). opt may be NULL. */
+int         spx_ctx_create(int device, const spx_options* opt, spx_ctx** out);
+int         spx_ctx_destroy(spx_ctx* ctx);
+const char* spx_last_error(const spx_ctx* ctx);
+/* Waits for all work of the context. */
+int         spx_ctx_synchronize(spx_ctx* ctx);
+
+/* ---- frequency weights (K6) -------------------------------------------------
+ * Replaces the HILBERT NONE weight loop, src/susceptibility.f:950-975:
+ *   w(p, f) = -2*d_p / (omega_f^2 + d_p^2) * scale_p * scale_all,
+ * d_p = e_n'(k+q) - e_n(k) (ediff), omega_f the imaginary-axis magnitude
+ * (frqh(f)/img), scale_p = nkpts(k)/nkpt/nsym1 (wscale, NULL = 1). A pair whose
+ * unoccupied band lies above nband gets scale_p = 0. Device pointers.
+ * w is (npair, nw) column-major with leading dimension npair. */
+int spx_weights_dev(spx_ctx* ctx, int64_t npair, const double* ediff,
+                    const double* wscale, double scale_all,
+                    int32_t nw, const double* omega, double* w, void* stream);
+
+/* ---- band-pair accumulation (K1/K2, with K6 inside) -------------------------
+ * Replaces src/susceptibility.f:950-975 (weights), :1182-1240 (body loop) and
+ * :1766-1789 (spectral_function, HILBERT NONE branch):
+ *   susceph(ij(i,j), f) += sum_p cprod(p,i) * conj(cprod(p,j)) * w(p,f),  i<=j.
+ * The result is ADDED to susceph, like the reference's `+=`; the caller zeroes
+ * it once per q point (src/susceptibility.f:211-223).
+ * Host-pointer form: cprod, ediff, wscale, omega and susceph are host arrays;
+ * the call streams cprod to the device in chunks, overlapping copy and compute,
+ * and returns after susceph has been updated. */
+int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ldc,
+                        int64_t npair, int32_t nbas,
+                        const double* ediff, const double* wscale, double scale_all,
+                        int32_t nw, const double* omega, int32_t precision,
+                        double* susceph, spx_chi0_stats* stats);
+
+/* Device-pointer form of spx_chi0_accumulate; ordered on `stream` (NULL = the
+ * context stream). Returns once the work is enqueued unless stats != NULL. */
+int spx_chi0_accumulate_dev(spx_ctx* ctx, const double* cprod, int64_t ldc,
+                            int64_t npair, int32_t nbas,
+                            const double* ediff, const double* wscale, double scale_all,
+                            int32_t nw, const double* omega, int32_t precision,
+                            double* susceph, void* stream, spx_chi0_stats* stats);
+
+/* Multiplies n complex elements of a device array by a real factor: the spin
+ * factor 2 of src/susceptibility.f:1331-1343 for unpolarised, non-SOC runs. */
+int spx_scale_dev(spx_ctx* ctx, double* z, int64_t n, double factor, void* stream);
+
+/* ---- seeded synthetic inputs (K8) -------------------------------------------
+ * Philox4x32-10 (Salmon et al., SC'11) with a Box-Muller transform written from
+ * basic IEEE operations only, so host and device produce identical bits.
+ * Element e of stream (seed, stream_id) is a standard normal times `scale`;
+ * out[t] receives element offset + t, t < n. */
+void spx_gen_normal_host(uint64_t seed, uint32_t stream_id, int64_t offset,
+                         int64_t n, double scale, double* out);
+int  spx_gen_normal_dev(spx_ctx* ctx, uint64_t seed, uint32_t stream_id,
+                        int64_t offset, int64_t n, double scale, double* out,
+                        void* stream);
+/* Fills a column-major complex (rows x cols, leading dimension ld) matrix whose
+ * column c holds elements [2*rows*c, 2*rows*(c+1)) of the stream, interleaved
+ * re/im: the layout of a cprod packet generated column by column. */
+void spx_gen_cmatrix_host(uint64_t seed, uint32_t stream_id, int64_t rows,
+                          int64_t cols, int64_t ld, int64_t col0, double scale,
+                          double* out);
+int  spx_gen_cmatrix_dev(spx_ctx* ctx, uint64_t seed, uint32_t stream_id,
+                         int64_t rows, int64_t cols, int64_t ld, int64_t col0,
+                         double scale, double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPEXGPU_H */

@@ -1,0 +1,104 @@
+"""ctypes binding of libspexgpu.so (the C ABI in include/spexgpu.h).
+
+The library is the product; this module only declares its signatures. There is
+no fallback: importing a function whose library is missing raises at once.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libspexgpu.so"
+
+SPX_OK, SPX_EINVAL, SPX_ENOMEM, SPX_ECUDA, SPX_ETIMEOUT, SPX_ENOTSUP, SPX_ENODEV = 0, -1, -2, -3, -4, -5, -6
+SPX_FP64, SPX_SPLIT = 0, 1
+
+
+class SpexGpuError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+class spx_options(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_int32),
+        ("verbose", C.c_int32),
+        ("workspace_limit", C.c_int64),
+        ("pinned_limit", C.c_int64),
+        ("chunk_pairs", C.c_int32),
+        ("timeout_ms", C.c_int32),
+    ]
+
+
+class spx_chi0_stats(C.Structure):
+    _fields_ = [
+        ("ms_total", C.c_double),
+        ("ms_gram", C.c_double),
+        ("ms_prep", C.c_double),
+        ("flops", C.c_double),
+        ("h2d_bytes", C.c_int64),
+        ("d2h_bytes", C.c_int64),
+        ("kernel_launches", C.c_int32),
+        ("precision", C.c_int32),
+    ]
+
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_I64 = C.c_int64
+_I32 = C.c_int32
+
+# name -> (restype, argtypes); every symbol declared in include/spexgpu.h
+SIGNATURES = {
+    "spx_abi_version": (C.c_int, []),
+    "spx_strerror": (C.c_char_p, [C.c_int]),
+    "spx_ctx_create": (C.c_int, [C.c_int, C.POINTER(spx_options), C.POINTER(_P)]),
+    "spx_ctx_destroy": (C.c_int, [_P]),
+    "spx_last_error": (C.c_char_p, [_P]),
+    "spx_ctx_synchronize": (C.c_int, [_P]),
+    "spx_weights_dev": (C.c_int, [_P, _I64, _P, _P, C.c_double, _I32, _P, _P, _P]),
+    "spx_chi0_accumulate": (
+        C.c_int,
+        [_P, _P, _I64, _I64, _I32, _P, _P, C.c_double, _I32, _P, _I32, _P, C.POINTER(spx_chi0_stats)],
+    ),
+    "spx_chi0_accumulate_dev": (
+        C.c_int,
+        [_P, _P, _I64, _I64, _I32, _P, _P, C.c_double, _I32, _P, _I32, _P, _P, C.POINTER(spx_chi0_stats)],
+    ),
+    "spx_scale_dev": (C.c_int, [_P, _P, _I64, C.c_double, _P]),
+    "spx_gen_normal_host": (None, [C.c_uint64, C.c_uint32, _I64, _I64, C.c_double, _P]),
+    "spx_gen_normal_dev": (C.c_int, [_P, C.c_uint64, C.c_uint32, _I64, _I64, C.c_double, _P, _P]),
+    "spx_gen_cmatrix_host": (None, [C.c_uint64, C.c_uint32, _I64, _I64, _I64, _I64, C.c_double, _P]),
+    "spx_gen_cmatrix_dev": (
+        C.c_int,
+        [_P, C.c_uint64, C.c_uint32, _I64, _I64, _I64, _I64, C.c_double, _P, _P],
+    ),
+}
+
+_lib = None
+
+
+def load(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Loads libspexgpu.so and binds every declared entry point."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(
+            f"{p} is missing: build it with `python -m project1_b200.build` "
+            "(there is no CPU fallback for this library)")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def strerror(status: int) -> str:
+    return load().spx_strerror(status).decode()

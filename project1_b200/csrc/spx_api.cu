@@ -1,0 +1,485 @@
+// C ABI of libspexgpu: contexts, errors, and the chi0 accumulation driver.
+//
+// The driver replaces the packet loop body of `susceptibility`
+// (src/susceptibility.f:751-1276): for each slab of band pairs it computes the
+// FP64 weights (K6, :950-975) and accumulates the weighted Gram into the packed
+// Hermitian output (K1 FP64 or K2 split precision, :1182-1240). Host-pointer
+// calls stream cprod to the device slab by slab on a copy stream, double
+// buffered, so that transfer and tensor-core work overlap; the slab is the
+// analogue of the reference's MEM packet (:659-713), sized from device memory
+// instead of the MEM keyword.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "spx_common.cuh"
+
+namespace spx {
+
+int launch_weights(spx_ctx*, int64_t, int64_t, const double*, const double*, double, int,
+                   const double*, double*, cudaStream_t);
+int launch_scale(spx_ctx*, double*, int64_t, double, cudaStream_t);
+int launch_gen_normal(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, double, double*,
+                      cudaStream_t);
+int launch_gen_cmatrix(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, int64_t, int64_t,
+                       double, double*, cudaStream_t);
+int launch_chi0_fp64(spx_ctx*, const double2*, int64_t, int64_t, int, const double*, int64_t,
+                     int, double2*, cudaStream_t, int);
+int split_chi0_slab(spx_ctx*, const double2*, int64_t, int64_t, int, const double*, int64_t,
+                    int, double2*, void*, size_t, cudaStream_t, int*, cudaEvent_t);
+size_t split_workspace_bytes(int64_t P, int N, int nw);
+
+int set_error(spx_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int check_cuda(spx_ctx* ctx, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return SPX_OK;
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return set_error(ctx, SPX_ENOMEM, m);
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+    return set_error(ctx, SPX_ENODEV, m);
+  return set_error(ctx, SPX_ECUDA, m);
+}
+
+int ensure_workspace(spx_ctx* ctx, size_t bytes) {
+  if (bytes <= ctx->ws_bytes) return SPX_OK;
+  if (ctx->opt.workspace_limit > 0 && bytes > (size_t)ctx->opt.workspace_limit)
+    return set_error(ctx, SPX_ENOMEM,
+                     "workspace of " + std::to_string(bytes) + " bytes exceeds workspace_limit");
+  if (ctx->ws) {
+    cudaFree(ctx->ws);
+    ctx->ws = nullptr;
+    ctx->ws_bytes = 0;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(ctx, SPX_ENOMEM,
+                     "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " +
+                         cudaGetErrorString(e));
+  }
+  ctx->ws = p;
+  ctx->ws_bytes = bytes;
+  return SPX_OK;
+}
+
+int ensure_pinned(spx_ctx* ctx, size_t bytes) {
+  if (bytes <= ctx->pinned_bytes) return SPX_OK;
+  if (ctx->pinned) {
+    cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_bytes = 0;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMallocHost(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(ctx, SPX_ENOMEM, "cudaMallocHost failed: " + std::string(cudaGetErrorString(e)));
+  }
+  ctx->pinned = p;
+  ctx->pinned_bytes = bytes;
+  return SPX_OK;
+}
+
+int collect_status(spx_ctx* ctx, cudaStream_t stream, const char* what) {
+  int h = 0;
+  int rc = check_cuda(ctx, cudaMemcpyAsync(&h, ctx->d_status, sizeof(int),
+                                           cudaMemcpyDeviceToHost, stream),
+                      what);
+  if (rc) return rc;
+  rc = check_cuda(ctx, cudaStreamSynchronize(stream), what);
+  if (rc) return rc;
+  if (h != 0) {
+    cudaMemsetAsync(ctx->d_status, 0, sizeof(int), stream);
+    cudaStreamSynchronize(stream);
+    if (h == kStatusTimeout)
+      return set_error(ctx, SPX_ETIMEOUT,
+                       std::string(what) + ": a device-side wait exceeded its time limit");
+    return set_error(ctx, SPX_ECUDA, std::string(what) + ": device status " + std::to_string(h));
+  }
+  return SPX_OK;
+}
+
+static bool is_pinned_or_device(const void* p, bool* device) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    *device = false;
+    return false;
+  }
+  *device = a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  return a.type != cudaMemoryTypeUnregistered;
+}
+
+// Validates the arguments shared by both accumulation entry points.
+static int check_chi0_args(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
+                           int32_t nbas, const double* ediff, int32_t nw, const double* omega,
+                           int32_t precision, const double* susceph) {
+  if (!ctx) return SPX_EINVAL;
+  if (npair < 0 || nbas < 0 || nw < 0) return set_error(ctx, SPX_EINVAL, "negative size");
+  if (npair > 0 && nbas > 0 && nw > 0) {
+    if (!cprod || !ediff || !omega || !susceph)
+      return set_error(ctx, SPX_EINVAL, "null array argument");
+    if (ldc < npair) return set_error(ctx, SPX_EINVAL, "ldc < npair");
+  }
+  if (nbas > 46340) return set_error(ctx, SPX_EINVAL, "nbas too large for packed indexing");
+  if (precision != SPX_FP64 && precision != SPX_SPLIT)
+    return set_error(ctx, SPX_EINVAL, "unknown precision");
+  return SPX_OK;
+}
+
+// Accumulates one slab of band pairs already on the device into the device
+// output. `W` is workspace for npair*nw weights (ldw = round_up(npair, 16)).
+static int chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N,
+                     const double* ediff, const double* wscale, double scale_all, int nw,
+                     const double* omega, int precision, double2* out, double* W,
+                     void* split_ws, size_t split_ws_bytes, cudaStream_t s, int* launches,
+                     cudaEvent_t prep_done) {
+  const int64_t ldw = (int64_t)align_up((size_t)std::max<int64_t>(P, 1), 16);
+  int rc = launch_weights(ctx, P, ldw, ediff, wscale, scale_all, nw, omega, W, s);
+  if (rc) return rc;
+  ++*launches;
+  if (precision == SPX_FP64) {
+    if (prep_done) cudaEventRecord(prep_done, s);
+    rc = launch_chi0_fp64(ctx, M, ldc, P, N, W, ldw, nw, out, s, 8);
+    ++*launches;
+    return rc;
+  }
+  // the split path records prep_done itself, after its operand conversion
+  return split_chi0_slab(ctx, M, ldc, P, N, W, ldw, nw, out, split_ws, split_ws_bytes, s,
+                         launches, prep_done);
+}
+
+}  // namespace spx
+
+using namespace spx;
+
+// ---------------------------------------------------------------------------
+
+extern "C" int spx_abi_version(void) { return SPX_ABI_VERSION; }
+
+extern "C" const char* spx_strerror(int s) {
+  switch (s) {
+    case SPX_OK: return "ok";
+    case SPX_EINVAL: return "invalid argument";
+    case SPX_ENOMEM: return "out of memory";
+    case SPX_ECUDA: return "CUDA error";
+    case SPX_ETIMEOUT: return "device wait timed out";
+    case SPX_ENOTSUP: return "not supported";
+    case SPX_ENODEV: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+extern "C" int spx_ctx_create(int device, const spx_options* opt, spx_ctx** out) {
+  if (!out) return SPX_EINVAL;
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return SPX_ENODEV;
+  }
+  if (device < 0 || device >= n) return SPX_EINVAL;
+  spx_ctx* ctx = new spx_ctx();
+  if (opt) {
+    size_t sz = opt->struct_size > 0 ? std::min<size_t>(opt->struct_size, sizeof(spx_options))
+                                     : sizeof(spx_options);
+    std::memcpy(&ctx->opt, opt, sz);
+  }
+  ctx->device = device;
+  int rc;
+  if ((rc = check_cuda(ctx, cudaSetDevice(device), "cudaSetDevice"))) {
+    delete ctx;
+    return rc;
+  }
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, device);
+  ctx->num_sms = prop.multiProcessorCount;
+  ctx->cc_major = prop.major;
+  ctx->cc_minor = prop.minor;
+  if (prop.major != 10) {
+    delete ctx;
+    return SPX_ENOTSUP;  // kernels are built for sm_100a only
+  }
+  if ((rc = check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking),
+                       "stream")) ||
+      (rc = check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking),
+                       "stream")) ||
+      (rc = check_cuda(ctx, cudaMalloc(&ctx->d_status, sizeof(int)), "status word")) ||
+      (rc = check_cuda(ctx, cudaMemset(ctx->d_status, 0, sizeof(int)), "status word"))) {
+    spx_ctx_destroy(ctx);
+    return rc;
+  }
+  for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+  *out = ctx;
+  return SPX_OK;
+}
+
+extern "C" int spx_ctx_destroy(spx_ctx* ctx) {
+  if (!ctx) return SPX_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  for (auto& ev : ctx->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (ctx->ws) cudaFree(ctx->ws);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  delete ctx;
+  return SPX_OK;
+}
+
+extern "C" const char* spx_last_error(const spx_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : "null context";
+}
+
+extern "C" int spx_ctx_synchronize(spx_ctx* ctx) {
+  if (!ctx) return SPX_EINVAL;
+  cudaSetDevice(ctx->device);
+  int rc = check_cuda(ctx, cudaStreamSynchronize(ctx->copy_stream), "synchronize");
+  if (rc) return rc;
+  return collect_status(ctx, ctx->stream, "synchronize");
+}
+
+extern "C" int spx_weights_dev(spx_ctx* ctx, int64_t npair, const double* ediff,
+                               const double* wscale, double scale_all, int32_t nw,
+                               const double* omega, double* w, void* stream) {
+  if (!ctx) return SPX_EINVAL;
+  if (npair < 0 || nw < 0) return set_error(ctx, SPX_EINVAL, "negative size");
+  if (npair == 0 || nw == 0) return SPX_OK;
+  if (!ediff || !omega || !w) return set_error(ctx, SPX_EINVAL, "null array argument");
+  cudaSetDevice(ctx->device);
+  return launch_weights(ctx, npair, npair, ediff, wscale, scale_all, nw, omega, w,
+                        pick_stream(ctx, stream));
+}
+
+extern "C" int spx_scale_dev(spx_ctx* ctx, double* z, int64_t n, double factor, void* stream) {
+  if (!ctx) return SPX_EINVAL;
+  if (n < 0) return set_error(ctx, SPX_EINVAL, "negative size");
+  if (n > 0 && !z) return set_error(ctx, SPX_EINVAL, "null array argument");
+  cudaSetDevice(ctx->device);
+  return launch_scale(ctx, z, n, factor, pick_stream(ctx, stream));
+}
+
+extern "C" int spx_gen_normal_dev(spx_ctx* ctx, uint64_t seed, uint32_t stream_id,
+                                  int64_t offset, int64_t n, double scale, double* out,
+                                  void* stream) {
+  if (!ctx) return SPX_EINVAL;
+  if (n < 0 || offset < 0) return set_error(ctx, SPX_EINVAL, "negative size");
+  if (n > 0 && !out) return set_error(ctx, SPX_EINVAL, "null array argument");
+  cudaSetDevice(ctx->device);
+  return launch_gen_normal(ctx, seed, stream_id, offset, n, scale, out,
+                           pick_stream(ctx, stream));
+}
+
+extern "C" int spx_gen_cmatrix_dev(spx_ctx* ctx, uint64_t seed, uint32_t stream_id,
+                                   int64_t rows, int64_t cols, int64_t ld, int64_t col0,
+                                   double scale, double* out, void* stream) {
+  if (!ctx) return SPX_EINVAL;
+  if (rows < 0 || cols < 0 || col0 < 0) return set_error(ctx, SPX_EINVAL, "negative size");
+  if (rows > 0 && cols > 0 && (!out || ld < rows))
+    return set_error(ctx, SPX_EINVAL, "bad output array");
+  cudaSetDevice(ctx->device);
+  return launch_gen_cmatrix(ctx, seed, stream_id, rows, cols, ld, col0, scale, out,
+                            pick_stream(ctx, stream));
+}
+
+extern "C" int spx_chi0_accumulate_dev(spx_ctx* ctx, const double* cprod, int64_t ldc,
+                                       int64_t npair, int32_t nbas, const double* ediff,
+                                       const double* wscale, double scale_all, int32_t nw,
+                                       const double* omega, int32_t precision,
+                                       double* susceph, void* stream, spx_chi0_stats* stats) {
+  int rc = check_chi0_args(ctx, cprod, ldc, npair, nbas, ediff, nw, omega, precision, susceph);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  auto t0 = std::chrono::steady_clock::now();
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->precision = precision;
+    stats->flops = 8.0 * (double)nbas * nbas * (double)npair * nw;
+  }
+  if (npair == 0 || nbas == 0 || nw == 0) return SPX_OK;
+  cudaStream_t s = pick_stream(ctx, stream);
+  const int64_t ldw = (int64_t)align_up((size_t)npair, 16);
+  size_t wbytes = align_up(sizeof(double) * (size_t)ldw * nw, 256);
+  size_t sbytes = precision == SPX_SPLIT ? split_workspace_bytes(npair, nbas, nw) : 0;
+  if ((rc = ensure_workspace(ctx, wbytes + sbytes))) return rc;
+  double* W = (double*)ctx->ws;
+  void* sws = (char*)ctx->ws + wbytes;
+  int launches = 0;
+  if (stats) cudaEventRecord(ctx->ev[0], s);
+  rc = chi0_slab(ctx, reinterpret_cast<const double2*>(cprod), ldc, npair, nbas, ediff, wscale,
+                 scale_all, nw, omega, precision, reinterpret_cast<double2*>(susceph), W, sws,
+                 sbytes, s, &launches, stats ? ctx->ev[1] : nullptr);
+  if (rc) return rc;
+  if (stats) {
+    cudaEventRecord(ctx->ev[6], s);
+    rc = collect_status(ctx, s, "chi0_accumulate_dev");
+    if (rc) return rc;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    stats->ms_prep = ms;
+    cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[6]);
+    stats->ms_gram = ms;
+    stats->kernel_launches = launches;
+    stats->ms_total =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return SPX_OK;
+}
+
+// Copies columns [0, nbas) of rows [p0, p0+len) of a host cprod(ldc, nbas) into a
+// dense pinned slab (len, nbas), using `nthr` host threads.
+static void gather_slab(const double* cprod, int64_t ldc, int64_t p0, int64_t len, int nbas,
+                        double* dst, int nthr) {
+  auto work = [&](int t) {
+    for (int c = t; c < nbas; c += nthr)
+      std::memcpy(dst + 2 * (int64_t)c * len, cprod + 2 * ((int64_t)c * ldc + p0),
+                  sizeof(double) * 2 * (size_t)len);
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < nthr; ++t) th.emplace_back(work, t);
+  work(0);
+  for (auto& x : th) x.join();
+}
+
+extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ldc,
+                                   int64_t npair, int32_t nbas, const double* ediff,
+                                   const double* wscale, double scale_all, int32_t nw,
+                                   const double* omega, int32_t precision, double* susceph,
+                                   spx_chi0_stats* stats) {
+  int rc = check_chi0_args(ctx, cprod, ldc, npair, nbas, ediff, nw, omega, precision, susceph);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  auto t0 = std::chrono::steady_clock::now();
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->precision = precision;
+    stats->flops = 8.0 * (double)nbas * nbas * (double)npair * nw;
+  }
+  if (npair == 0 || nbas == 0 || nw == 0) return SPX_OK;
+  bool dev = false;
+  const bool pinned = is_pinned_or_device(cprod, &dev);
+  if (dev) return set_error(ctx, SPX_EINVAL, "cprod is a device pointer; use spx_chi0_accumulate_dev");
+
+  // slab size: band pairs per streamed chunk
+  int64_t slab = ctx->opt.chunk_pairs > 0 ? ctx->opt.chunk_pairs : 65536;
+  slab = std::min<int64_t>(slab, npair);
+  slab = (int64_t)align_up((size_t)slab, 16);
+  const int nslab_buf = 2;
+  const int64_t npack = (int64_t)nbas * (nbas + 1) / 2;
+  const size_t out_bytes = align_up(sizeof(double) * 2 * (size_t)npack * nw, 256);
+  const size_t slab_bytes = align_up(sizeof(double) * 2 * (size_t)slab * nbas, 256);
+  const size_t e_bytes = align_up(sizeof(double) * (size_t)slab, 256);
+  const size_t om_bytes = align_up(sizeof(double) * (size_t)nw, 256);
+  const size_t w_bytes = align_up(sizeof(double) * (size_t)slab * nw, 256);
+  const size_t s_bytes = precision == SPX_SPLIT ? split_workspace_bytes(slab, nbas, nw) : 0;
+  size_t total = out_bytes + nslab_buf * (slab_bytes + 2 * e_bytes) + om_bytes + w_bytes + s_bytes;
+  if ((rc = ensure_workspace(ctx, total))) return rc;
+  char* base = (char*)ctx->ws;
+  double2* d_out = (double2*)base;
+  base += out_bytes;
+  double2* d_slab[2];
+  double* d_e[2];
+  double* d_ws[2];
+  for (int b = 0; b < 2; ++b) {
+    d_slab[b] = (double2*)base;
+    base += slab_bytes;
+    d_e[b] = (double*)base;
+    base += e_bytes;
+    d_ws[b] = (double*)base;
+    base += e_bytes;
+  }
+  double* d_om = (double*)base;
+  base += om_bytes;
+  double* d_w = (double*)base;
+  base += w_bytes;
+  void* d_split = s_bytes ? (void*)base : nullptr;
+
+  double* stage = nullptr;
+  if (!pinned) {
+    if ((rc = ensure_pinned(ctx, 2 * slab_bytes))) return rc;
+    stage = (double*)ctx->pinned;
+  }
+  cudaStream_t cs = ctx->stream, xs = ctx->copy_stream;
+  int64_t h2d = 0, d2h = 0;
+  int launches = 0;
+  const size_t out_host_bytes = sizeof(double) * 2 * (size_t)npack * nw;
+  // the output accumulates: bring the caller's values to the device once
+  if ((rc = check_cuda(ctx, cudaMemcpyAsync(d_out, susceph, out_host_bytes,
+                                            cudaMemcpyHostToDevice, cs),
+                       "copy susceph")))
+    return rc;
+  h2d += out_host_bytes;
+  if ((rc = check_cuda(ctx, cudaMemcpyAsync(d_om, omega, sizeof(double) * nw,
+                                            cudaMemcpyHostToDevice, cs),
+                       "copy omega")))
+    return rc;
+  h2d += sizeof(double) * nw;
+  cudaEvent_t ev_copied[2] = {ctx->ev[2], ctx->ev[3]};
+  cudaEvent_t ev_free[2] = {ctx->ev[4], ctx->ev[5]};
+  cudaEventRecord(ev_free[0], cs);
+  cudaEventRecord(ev_free[1], cs);
+  const int nthr = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  int64_t k = 0;
+  for (int64_t p0 = 0; p0 < npair; p0 += slab, ++k) {
+    const int b = (int)(k & 1);
+    const int64_t len = std::min<int64_t>(slab, npair - p0);
+    cudaStreamWaitEvent(xs, ev_free[b], 0);
+    const size_t bytes = sizeof(double) * 2 * (size_t)len;
+    if (pinned) {
+      rc = check_cuda(ctx, cudaMemcpy2DAsync(d_slab[b], bytes, cprod + 2 * p0, sizeof(double) * 2 * ldc,
+                                             bytes, nbas, cudaMemcpyHostToDevice, xs),
+                      "copy cprod slab");
+    } else {
+      // the staging half `b` is free once the previous copy out of it finished
+      cudaEventSynchronize(ev_free[b]);
+      double* st = stage + (size_t)b * (slab_bytes / sizeof(double));
+      gather_slab(cprod, ldc, p0, len, nbas, st, nthr);
+      rc = check_cuda(ctx, cudaMemcpyAsync(d_slab[b], st, bytes * nbas, cudaMemcpyHostToDevice, xs),
+                      "copy cprod slab");
+    }
+    if (rc) return rc;
+    h2d += (int64_t)bytes * nbas;
+    cudaMemcpyAsync(d_e[b], ediff + p0, sizeof(double) * len, cudaMemcpyHostToDevice, xs);
+    h2d += sizeof(double) * len;
+    if (wscale) {
+      cudaMemcpyAsync(d_ws[b], wscale + p0, sizeof(double) * len, cudaMemcpyHostToDevice, xs);
+      h2d += sizeof(double) * len;
+    }
+    cudaEventRecord(ev_copied[b], xs);
+    cudaStreamWaitEvent(cs, ev_copied[b], 0);
+    rc = chi0_slab(ctx, d_slab[b], len, len, nbas, d_e[b], wscale ? d_ws[b] : nullptr, scale_all,
+                   nw, d_om, precision, d_out, d_w, d_split, s_bytes, cs, &launches, nullptr);
+    if (rc) return rc;
+    cudaEventRecord(ev_free[b], cs);
+  }
+  if ((rc = check_cuda(ctx, cudaMemcpyAsync(susceph, d_out, out_host_bytes,
+                                            cudaMemcpyDeviceToHost, cs),
+                       "copy susceph back")))
+    return rc;
+  d2h += out_host_bytes;
+  rc = collect_status(ctx, cs, "chi0_accumulate");
+  if (rc) return rc;
+  if (stats) {
+    stats->h2d_bytes = h2d;
+    stats->d2h_bytes = d2h;
+    stats->kernel_launches = launches;
+    stats->ms_total =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return SPX_OK;
+}

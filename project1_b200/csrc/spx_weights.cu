@@ -1,0 +1,117 @@
+// K6: FP64 frequency weights, spin factor, and the seeded input generator (K8).
+#include <cuda_runtime.h>
+
+#include "spx_common.cuh"
+#include "spx_philox.h"
+
+namespace spx {
+
+// HILBERT NONE weights of src/susceptibility.f:950-975,
+//   wghtSr(p, f) = -2*rdum / ((frqh(f)/img)**2 + rdum**2) / nkpt / nsym1 * nkpts(k),
+// rdum = ediff[p], frqh(f)/img = omega[f], nkpts(k)/nkpt/nsym1 = wscale[p]*scale_all.
+// Always FP64: near-degenerate pairs (|rdum| ~ 1e-6 eV) keep full relative
+// accuracy because rdum is taken as given, never recomputed from energies in a
+// narrower type. Rows [P, ldw) of every column are zeroed.
+__global__ void weights_kernel(int64_t P, int64_t ldw, const double* __restrict__ ediff,
+                               const double* __restrict__ wscale, double scale_all, int nw,
+                               const double* __restrict__ omega, double* __restrict__ w) {
+  const int64_t total = ldw * nw;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = t % ldw;
+    const int f = (int)(t / ldw);
+    double v = 0.0;
+    if (p < P) {
+      const double d = ediff[p];
+      const double om = omega[f];
+      const double s = (wscale ? wscale[p] : 1.0) * scale_all;
+      v = -2.0 * d / (om * om + d * d) * s;
+    }
+    w[t] = v;
+  }
+}
+
+int launch_weights(spx_ctx* ctx, int64_t P, int64_t ldw, const double* ediff,
+                   const double* wscale, double scale_all, int nw, const double* omega,
+                   double* w, cudaStream_t stream) {
+  const int64_t total = ldw * nw;
+  if (total <= 0) return SPX_OK;
+  int grid = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 16);
+  weights_kernel<<<grid, 256, 0, stream>>>(P, ldw, ediff, wscale, scale_all, nw, omega, w);
+  return check_cuda(ctx, cudaGetLastError(), "weights_kernel launch");
+}
+
+__global__ void scale_kernel(double* z, int64_t n2, double factor) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n2;
+       t += (int64_t)gridDim.x * blockDim.x)
+    z[t] *= factor;
+}
+
+int launch_scale(spx_ctx* ctx, double* z, int64_t n, double factor, cudaStream_t stream) {
+  if (n <= 0) return SPX_OK;
+  int grid = (int)std::min<int64_t>((2 * n + 255) / 256, (int64_t)ctx->num_sms * 16);
+  scale_kernel<<<grid, 256, 0, stream>>>(z, 2 * n, factor);
+  return check_cuda(ctx, cudaGetLastError(), "scale_kernel launch");
+}
+
+// out[t] = scale * normal(offset + t)
+__global__ void gen_normal_kernel(uint64_t seed, uint32_t sid, int64_t offset, int64_t n,
+                                  double scale, double* out) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x)
+    out[t] = __dmul_rn(scale, normal_at(seed, sid, (uint64_t)(offset + t)));
+}
+
+// Complex matrix: element (p, c) re/im = stream elements 2*rows*(col0+c) + 2p + {0,1}.
+// One thread per complex element; a Philox block yields exactly that pair.
+__global__ void gen_cmatrix_kernel(uint64_t seed, uint32_t sid, int64_t rows, int64_t cols,
+                                   int64_t ld, int64_t col0, double scale, double2* out) {
+  const int64_t total = rows * cols;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = t / rows, p = t - c * rows;
+    const uint64_t e = (uint64_t)(2 * rows * (col0 + c) + 2 * p);
+    double z0, z1;
+    normal_pair(seed, sid, e >> 1, &z0, &z1);  // e is even: (z0, z1) = elements e, e+1
+    out[c * ld + p] = make_double2(__dmul_rn(scale, z0), __dmul_rn(scale, z1));
+  }
+}
+
+int launch_gen_normal(spx_ctx* ctx, uint64_t seed, uint32_t sid, int64_t offset, int64_t n,
+                      double scale, double* out, cudaStream_t stream) {
+  if (n <= 0) return SPX_OK;
+  int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 32);
+  gen_normal_kernel<<<grid, 256, 0, stream>>>(seed, sid, offset, n, scale, out);
+  return check_cuda(ctx, cudaGetLastError(), "gen_normal_kernel launch");
+}
+
+int launch_gen_cmatrix(spx_ctx* ctx, uint64_t seed, uint32_t sid, int64_t rows, int64_t cols,
+                       int64_t ld, int64_t col0, double scale, double* out,
+                       cudaStream_t stream) {
+  if (rows <= 0 || cols <= 0) return SPX_OK;
+  int grid = (int)std::min<int64_t>((rows * cols + 255) / 256, (int64_t)ctx->num_sms * 32);
+  gen_cmatrix_kernel<<<grid, 256, 0, stream>>>(seed, sid, rows, cols, ld, col0, scale,
+                                               reinterpret_cast<double2*>(out));
+  return check_cuda(ctx, cudaGetLastError(), "gen_cmatrix_kernel launch");
+}
+
+}  // namespace spx
+
+// host generators (same arithmetic as the kernels above)
+extern "C" void spx_gen_normal_host(uint64_t seed, uint32_t stream_id, int64_t offset,
+                                    int64_t n, double scale, double* out) {
+  for (int64_t t = 0; t < n; ++t) out[t] = scale * spx::normal_at(seed, stream_id, offset + t);
+}
+
+extern "C" void spx_gen_cmatrix_host(uint64_t seed, uint32_t stream_id, int64_t rows,
+                                     int64_t cols, int64_t ld, int64_t col0, double scale,
+                                     double* out) {
+  for (int64_t c = 0; c < cols; ++c)
+    for (int64_t p = 0; p < rows; ++p) {
+      const uint64_t e = (uint64_t)(2 * rows * (col0 + c) + 2 * p);
+      double z0, z1;
+      spx::normal_pair(seed, stream_id, e >> 1, &z0, &z1);
+      out[2 * (c * ld + p)] = scale * z0;
+      out[2 * (c * ld + p) + 1] = scale * z1;
+    }
+}

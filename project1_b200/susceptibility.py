@@ -1,0 +1,218 @@
+"""Host-side mirror of SPEX's `susceptibility` call surface for the HILBERT NONE
+imaginary-frequency polarisation, running on libspexgpu.
+
+Reference: src/susceptibility.f:100-102 (signature), :211-223 (outputs zeroed on
+entry), :751-1276 (packet loop: products, weights, body accumulation),
+:1331-1343 (spin factor 2). The Fortran routine reads its band-pair products
+from module state after `wavefproducts2_*`; here they are explicit arguments.
+
+Array conventions (those of the Fortran caller):
+  cprod    complex128 (npair, nbas), Fortran order: column I holds M_I,p for all
+           band pairs p = n' + nu*(n + no*k)          (src/susceptibility.f:861-865)
+  ediff    float64 (npair,) e_n'(k+q) - e_n(k)
+  frqh     complex128 (nw,) imaginary frequencies i*omega (frqh/img = omega)
+  susceph  complex128 (nbas*(nbas+1)/2, nw), Fortran order, packed upper triangle
+           ij = j*(j+1)/2 + i (0-based, i <= j)        (src/susceptibility.f:1210)
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import SPX_FP64, SPX_SPLIT, SpexGpuError
+
+PRECISIONS = {"fp64": SPX_FP64, "split": SPX_SPLIT}
+
+
+def _ptr(a) -> C.c_void_p:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return C.c_void_p(a.ctypes.data)
+    return C.c_void_p(int(a.data_ptr()))  # torch tensor
+
+
+def npack(nbas: int) -> int:
+    return nbas * (nbas + 1) // 2
+
+
+def packed_index(i: int, j: int) -> int:
+    """0-based packed upper-triangle index of (i, j), i <= j."""
+    return j * (j + 1) // 2 + i
+
+
+def unpack_hermitian(susceph: np.ndarray, nbas: int) -> np.ndarray:
+    """Packed (npack, nw) -> full Hermitian (nw, nbas, nbas)."""
+    sp = np.asarray(susceph)
+    nw = sp.shape[1]
+    out = np.zeros((nw, nbas, nbas), dtype=np.complex128)
+    iu, ju = np.triu_indices(nbas)
+    idx = ju * (ju + 1) // 2 + iu
+    for f in range(nw):
+        out[f, iu, ju] = sp[idx, f]
+        out[f, ju, iu] = np.conj(sp[idx, f])
+    return out
+
+
+class Context:
+    """One libspexgpu context: a device, its streams and workspace."""
+
+    def __init__(self, device: int = 0, workspace_limit: int = 0, chunk_pairs: int = 0,
+                 timeout_ms: int = 0, pinned_limit: int = 0):
+        self.lib = _lib.load()
+        opt = _lib.spx_options(C.sizeof(_lib.spx_options), 0, workspace_limit, pinned_limit,
+                               chunk_pairs, timeout_ms)
+        h = C.c_void_p()
+        rc = self.lib.spx_ctx_create(device, C.byref(opt), C.byref(h))
+        if rc != 0:
+            raise SpexGpuError(rc, f"spx_ctx_create: {_lib.strerror(rc)}")
+        self.handle = h
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.spx_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            msg = self.lib.spx_last_error(self.handle).decode()
+            raise SpexGpuError(rc, f"{what}: {_lib.strerror(rc)}: {msg}")
+
+    def synchronize(self) -> None:
+        self._check(self.lib.spx_ctx_synchronize(self.handle), "spx_ctx_synchronize")
+
+    # ---- band-pair accumulation ------------------------------------------------
+
+    def chi0_accumulate(self, cprod: np.ndarray, ediff: np.ndarray, omega: np.ndarray,
+                        susceph: np.ndarray, wscale: Optional[np.ndarray] = None,
+                        scale_all: float = 1.0, precision: str = "fp64") -> dict:
+        """susceph += sum_p cprod(p,i) conj(cprod(p,j)) w(p,f) on host arrays (drop-in)."""
+        cprod = np.asarray(cprod)
+        if cprod.dtype != np.complex128 or not cprod.flags.f_contiguous:
+            raise ValueError("cprod must be a Fortran-ordered complex128 (npair, nbas) array")
+        if susceph.dtype != np.complex128 or not susceph.flags.f_contiguous:
+            raise ValueError("susceph must be a Fortran-ordered complex128 (npack, nw) array")
+        npair, nbas = cprod.shape
+        ediff = np.ascontiguousarray(ediff, dtype=np.float64)
+        omega = np.ascontiguousarray(omega, dtype=np.float64)
+        ws = None if wscale is None else np.ascontiguousarray(wscale, dtype=np.float64)
+        st = _lib.spx_chi0_stats()
+        rc = self.lib.spx_chi0_accumulate(self.handle, _ptr(cprod), npair, npair, nbas, _ptr(ediff),
+                                          _ptr(ws), scale_all, len(omega), _ptr(omega),
+                                          PRECISIONS[precision], _ptr(susceph), C.byref(st))
+        self._check(rc, "spx_chi0_accumulate")
+        return _stats(st)
+
+    def chi0_accumulate_host_ptr(self, cprod_ptr: int, ldc: int, npair: int, nbas: int,
+                                 ediff: np.ndarray, omega: np.ndarray, susceph: np.ndarray,
+                                 wscale: Optional[np.ndarray] = None, scale_all: float = 1.0,
+                                 precision: str = "fp64") -> dict:
+        """Same as chi0_accumulate on a raw host pointer (e.g. pinned torch memory)."""
+        ediff = np.ascontiguousarray(ediff, dtype=np.float64)
+        omega = np.ascontiguousarray(omega, dtype=np.float64)
+        ws = None if wscale is None else np.ascontiguousarray(wscale, dtype=np.float64)
+        st = _lib.spx_chi0_stats()
+        rc = self.lib.spx_chi0_accumulate(self.handle, C.c_void_p(cprod_ptr), ldc, npair, nbas,
+                                          _ptr(ediff), _ptr(ws), scale_all, len(omega), _ptr(omega),
+                                          PRECISIONS[precision], _ptr(susceph), C.byref(st))
+        self._check(rc, "spx_chi0_accumulate")
+        return _stats(st)
+
+    def chi0_accumulate_dev(self, cprod, ediff, omega, susceph, wscale=None, scale_all: float = 1.0,
+                            precision: str = "fp64", stream=None, npair: Optional[int] = None,
+                            stats: bool = False) -> Optional[dict]:
+        """Device form on torch CUDA tensors.
+
+        cprod: complex128 (nbas, ldc) row-major == Fortran (ldc, nbas); npair <= ldc.
+        susceph: complex128 (nw, npack) row-major == Fortran (npack, nw).
+        """
+        nbas, ldc = cprod.shape
+        npair = ldc if npair is None else npair
+        nw = omega.shape[0]
+        st = _lib.spx_chi0_stats() if stats else None
+        rc = self.lib.spx_chi0_accumulate_dev(
+            self.handle, _ptr(cprod), ldc, npair, nbas, _ptr(ediff), _ptr(wscale), scale_all, nw,
+            _ptr(omega), PRECISIONS[precision], _ptr(susceph),
+            None if stream is None else C.c_void_p(int(stream)), C.byref(st) if st is not None else None)
+        self._check(rc, "spx_chi0_accumulate_dev")
+        return _stats(st) if st is not None else None
+
+    def weights_dev(self, ediff, omega, w, wscale=None, scale_all: float = 1.0, stream=None) -> None:
+        rc = self.lib.spx_weights_dev(self.handle, ediff.shape[0], _ptr(ediff), _ptr(wscale), scale_all,
+                                      omega.shape[0], _ptr(omega), _ptr(w),
+                                      None if stream is None else C.c_void_p(int(stream)))
+        self._check(rc, "spx_weights_dev")
+
+    def scale_dev(self, z, factor: float, stream=None) -> None:
+        rc = self.lib.spx_scale_dev(self.handle, _ptr(z), z.numel(), factor,
+                                    None if stream is None else C.c_void_p(int(stream)))
+        self._check(rc, "spx_scale_dev")
+
+    def gen_cmatrix_dev(self, seed: int, stream_id: int, out, rows: int, col0: int = 0,
+                        scale: float = 1.0, stream=None) -> None:
+        """Fills torch complex128 (cols, ld) with the seeded normal matrix (see spx_gen_cmatrix_host)."""
+        cols, ld = out.shape
+        rc = self.lib.spx_gen_cmatrix_dev(self.handle, seed, stream_id, rows, cols, ld, col0, scale,
+                                          _ptr(out), None if stream is None else C.c_void_p(int(stream)))
+        self._check(rc, "spx_gen_cmatrix_dev")
+
+
+def _stats(st) -> dict:
+    return {k: getattr(st, k) for k, _ in st._fields_}
+
+
+def gen_cmatrix_host(seed: int, stream_id: int, rows: int, cols: int, col0: int = 0,
+                     scale: float = 1.0) -> np.ndarray:
+    """Seeded complex normal matrix (rows, cols), Fortran order; identical bits to the device form."""
+    out = np.empty((rows, cols), dtype=np.complex128, order="F")
+    _lib.load().spx_gen_cmatrix_host(seed, stream_id, rows, cols, rows, col0, scale, _ptr(out))
+    return out
+
+
+def gen_normal_host(seed: int, stream_id: int, offset: int, n: int, scale: float = 1.0) -> np.ndarray:
+    out = np.empty(n, dtype=np.float64)
+    _lib.load().spx_gen_normal_host(seed, stream_id, offset, n, scale, _ptr(out))
+    return out
+
+
+def susceptibility(ctx: Context, cprod: np.ndarray, ediff: np.ndarray, frqh: np.ndarray, nkpt: int,
+                   nsym1: int = 1, nkpts: Optional[np.ndarray] = None, nspin: int = 1,
+                   l_soc: bool = False, precision: str = "fp64",
+                   packets: Optional[list] = None) -> np.ndarray:
+    """HILBERT NONE susceph for one q point and spin, as `susceptibility` returns it.
+
+    `nkpts` (per pair) is the weight of the k point of each pair; the pair weight
+    is nkpts(k)/nkpt/nsym1 (src/susceptibility.f:965). `packets` optionally
+    lists (p_begin, p_end) band-pair ranges accumulated one after another, as the
+    reference's MEM packets are (:751-758); the result does not depend on them.
+    """
+    cprod = np.asfortranarray(cprod, dtype=np.complex128)
+    npair, nbas = cprod.shape
+    omega = np.asarray(np.asarray(frqh) / 1j).real.astype(np.float64)
+    nw = omega.shape[0]
+    susceph = np.zeros((npack(nbas), nw), dtype=np.complex128, order="F")   # intent(out), zeroed
+    wscale = None if nkpts is None else np.asarray(nkpts, dtype=np.float64)
+    scale_all = 1.0 / nkpt / nsym1
+    for (b, e) in (packets or [(0, npair)]):
+        ctx.chi0_accumulate(np.asfortranarray(cprod[b:e]), ediff[b:e], omega, susceph,
+                            wscale=None if wscale is None else wscale[b:e], scale_all=scale_all,
+                            precision=precision)
+    if not l_soc and nspin == 1:
+        susceph *= 2.0                                                        # :1336
+    return susceph

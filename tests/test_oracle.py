@@ -1,0 +1,67 @@
+"""The CPU oracle against the independent numpy golden vectors (no GPU)."""
+import numpy as np
+import pytest
+
+import oracle
+
+G = np.load(__import__("pathlib").Path(__file__).parent / "golden" / "chi0_golden.npz")
+CASES = sorted({k.split("/")[0] for k in G.files if "/" in k})
+
+
+def case(name):
+    ws = G[f"{name}/wscale"] if f"{name}/wscale" in G.files else None
+    return (G[f"{name}/cprod"], G[f"{name}/ediff"], G[f"{name}/omega"], ws,
+            G[f"{name}/w"], G[f"{name}/susceph"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_weights_match_golden(name):
+    m, d, om, ws, w, _ = case(name)
+    got = oracle.weights(d, om, ws, float(G["scale_all"]))
+    np.testing.assert_allclose(got, w, rtol=1e-14, atol=0)
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("accurate", [False, True])
+def test_chi0_matches_golden(name, accurate):
+    m, d, om, ws, w, ref = case(name)
+    got = oracle.chi0(m, w, accurate=accurate, threads=2)
+    scale = np.max(np.abs(ref))
+    assert np.max(np.abs(got - ref)) <= 1e-13 * scale
+
+
+def test_packet_split_invariance():
+    """Accumulating MEM packets one after another gives the same chi (src/susceptibility.f:751-758)."""
+    m, d, om, ws, w, ref = case("small_degenerate")
+    acc = None
+    for b, e in [(0, 13), (13, 40), (40, 60)]:
+        acc = oracle.chi0(m[b:e], w[b:e], susceph=acc)
+    assert np.max(np.abs(acc - ref)) <= 1e-13 * np.max(np.abs(ref))
+
+
+def test_hermitian_diagonal_real_and_negative():
+    """Single-sign weights: chi(iw) is Hermitian negative semi-definite, so the diagonal is real <= 0."""
+    m, d, om, ws, w, ref = case("ragged")
+    n = m.shape[1]
+    diag = np.array([j * (j + 1) // 2 + j for j in range(n)])
+    assert np.all(np.abs(ref[diag].imag) <= 1e-15 * np.abs(ref[diag].real).max())
+    assert np.all(ref[diag].real <= 0)
+    for f in range(ref.shape[1]):
+        full = np.zeros((n, n), complex)
+        iu, ju = np.triu_indices(n)
+        full[iu, ju] = ref[ju * (ju + 1) // 2 + iu, f]
+        full[ju, iu] = np.conj(full[iu, ju])
+        assert np.linalg.eigvalsh(full).max() <= 1e-14 * np.abs(full).max()
+
+
+def test_element_sampler_matches_full():
+    m, d, om, ws, w, ref = case("small_degenerate")
+    for (i, j) in [(0, 0), (3, 17), (23, 23), (5, 6)]:
+        got = oracle.chi0_element(m[:, i], m[:, j], w)
+        np.testing.assert_allclose(got, ref[j * (j + 1) // 2 + i], rtol=1e-13, atol=1e-16)
+
+
+def test_linearity_in_weights():
+    m, d, om, ws, w, ref = case("tiny")
+    a = oracle.chi0(m, 2.5 * w)
+    np.testing.assert_allclose(a, 2.5 * ref, rtol=1e-13, atol=1e-17)
