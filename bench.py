@@ -145,7 +145,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    w = inputs.CONFIGS[args.workload]
+    w = workload_from_args(args)
     vals = []
     for _ in range(args.warmup):
         cpu_baseline(w, budget_s=args.ref_budget)
@@ -163,6 +163,16 @@ def run_reference(args):
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def workload_from_args(args):
+    """The named workload, optionally shrunk (--kpts / --freqs) for profiling captures."""
+    import dataclasses
+    from project1_b200 import inputs
+    w = inputs.CONFIGS[args.workload]
+    if args.kpts or args.freqs:
+        w = dataclasses.replace(w, name=w.name + "-small", nk=args.kpts or w.nk, nw=args.freqs or w.nw)
+    return w
 
 
 def workload_name(w):
@@ -187,7 +197,7 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
-    w = inputs.CONFIGS[args.workload]
+    w = workload_from_args(args)
     # shard the pair axis: rank r owns a contiguous block of k points (Mblocks over k)
     P = w.npair
     p_lo = rank * P // world
@@ -254,13 +264,16 @@ def run_ours(args):
         return ms, gram_ms, launches, clocks
 
     avail = {"split": True}
-    try:
-        step("split")
-        torch.cuda.synchronize()
-    except spx.SpexGpuError as e:
-        avail["split"] = False
-        avail["split_error"] = str(e)
+    if args.precision != "fp64":
+        try:
+            step("split")
+            torch.cuda.synchronize()
+        except spx.SpexGpuError as e:
+            avail["split"] = False
+            avail["split_error"] = str(e)
     head = "split" if avail["split"] else "fp64"
+    if args.precision:
+        head = args.precision
 
     sampler = ClockSampler(local) if rank == 0 else None
     ms, gram_ms, launches, clocks = timed(head, args.warmup, args.steps, sampler)
@@ -408,6 +421,10 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=10.0)
     ap.add_argument("--no-check", dest="check", action="store_false")
+    ap.add_argument("--precision", choices=["split", "fp64"], default=None,
+                    help="force the measured path (profiling captures)")
+    ap.add_argument("--kpts", type=int, default=0, help="override the k-point count (profiling)")
+    ap.add_argument("--freqs", type=int, default=0, help="override the frequency count (profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

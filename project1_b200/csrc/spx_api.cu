@@ -36,6 +36,32 @@ int split_chi0_slab(spx_ctx*, const double2*, int64_t, int64_t, int, const doubl
                     int, double2*, void*, size_t, cudaStream_t, int*, cudaEvent_t);
 size_t split_workspace_bytes(int64_t P, int N, int nw);
 
+void timing_mark(spx_ctx* ctx, cudaStream_t s, int kind) {
+  if (!ctx->timing) return;
+  if (ctx->nmarks == ctx->mark_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    ctx->mark_pool.push_back(e);
+    ctx->mark_kind.push_back(0);
+  }
+  cudaEventRecord(ctx->mark_pool[ctx->nmarks], s);
+  ctx->mark_kind[ctx->nmarks] = kind;
+  ++ctx->nmarks;
+}
+
+void timing_collect(spx_ctx* ctx, double* ms_prep, double* ms_gram) {
+  double prep = 0, gram = 0;
+  for (size_t k = 0; k + 1 < ctx->nmarks; ++k) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->mark_pool[k], ctx->mark_pool[k + 1]);
+    if (ctx->mark_kind[k] == 0) prep += ms;
+    if (ctx->mark_kind[k] == 1) gram += ms;
+  }
+  ctx->nmarks = 0;
+  if (ms_prep) *ms_prep = prep;
+  if (ms_gram) *ms_gram = gram;
+}
+
 int set_error(spx_ctx* ctx, int code, const std::string& msg) {
   if (ctx) ctx->err = msg;
   return code;
@@ -143,21 +169,23 @@ static int check_chi0_args(spx_ctx* ctx, const double* cprod, int64_t ldc, int64
 static int chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N,
                      const double* ediff, const double* wscale, double scale_all, int nw,
                      const double* omega, int precision, double2* out, double* W,
-                     void* split_ws, size_t split_ws_bytes, cudaStream_t s, int* launches,
-                     cudaEvent_t prep_done) {
+                     void* split_ws, size_t split_ws_bytes, cudaStream_t s, int* launches) {
   const int64_t ldw = (int64_t)align_up((size_t)std::max<int64_t>(P, 1), 16);
+  timing_mark(ctx, s, 0);
   int rc = launch_weights(ctx, P, ldw, ediff, wscale, scale_all, nw, omega, W, s);
   if (rc) return rc;
   ++*launches;
   if (precision == SPX_FP64) {
-    if (prep_done) cudaEventRecord(prep_done, s);
+    timing_mark(ctx, s, 1);
     rc = launch_chi0_fp64(ctx, M, ldc, P, N, W, ldw, nw, out, s, 8);
     ++*launches;
-    return rc;
+  } else {
+    // the split path marks its own preparation / accumulation phases
+    rc = split_chi0_slab(ctx, M, ldc, P, N, W, ldw, nw, out, split_ws, split_ws_bytes, s,
+                         launches, nullptr);
   }
-  // the split path records prep_done itself, after its operand conversion
-  return split_chi0_slab(ctx, M, ldc, P, N, W, ldw, nw, out, split_ws, split_ws_bytes, s,
-                         launches, prep_done);
+  timing_mark(ctx, s, 2);
+  return rc;
 }
 
 }  // namespace spx
@@ -233,6 +261,7 @@ extern "C" int spx_ctx_destroy(spx_ctx* ctx) {
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   for (auto& ev : ctx->ev)
     if (ev) cudaEventDestroy(ev);
+  for (auto& ev : ctx->mark_pool) cudaEventDestroy(ev);
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->d_status) cudaFree(ctx->d_status);
@@ -320,20 +349,17 @@ extern "C" int spx_chi0_accumulate_dev(spx_ctx* ctx, const double* cprod, int64_
   double* W = (double*)ctx->ws;
   void* sws = (char*)ctx->ws + wbytes;
   int launches = 0;
-  if (stats) cudaEventRecord(ctx->ev[0], s);
+  ctx->timing = stats != nullptr;
+  ctx->nmarks = 0;
   rc = chi0_slab(ctx, reinterpret_cast<const double2*>(cprod), ldc, npair, nbas, ediff, wscale,
                  scale_all, nw, omega, precision, reinterpret_cast<double2*>(susceph), W, sws,
-                 sbytes, s, &launches, stats ? ctx->ev[1] : nullptr);
+                 sbytes, s, &launches);
+  ctx->timing = false;
   if (rc) return rc;
   if (stats) {
-    cudaEventRecord(ctx->ev[6], s);
     rc = collect_status(ctx, s, "chi0_accumulate_dev");
     if (rc) return rc;
-    float ms = 0;
-    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
-    stats->ms_prep = ms;
-    cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[6]);
-    stats->ms_gram = ms;
+    timing_collect(ctx, &stats->ms_prep, &stats->ms_gram);
     stats->kernel_launches = launches;
     stats->ms_total =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -463,7 +489,7 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
     cudaEventRecord(ev_copied[b], xs);
     cudaStreamWaitEvent(cs, ev_copied[b], 0);
     rc = chi0_slab(ctx, d_slab[b], len, len, nbas, d_e[b], wscale ? d_ws[b] : nullptr, scale_all,
-                   nw, d_om, precision, d_out, d_w, d_split, s_bytes, cs, &launches, nullptr);
+                   nw, d_om, precision, d_out, d_w, d_split, s_bytes, cs, &launches);
     if (rc) return rc;
     cudaEventRecord(ev_free[b], cs);
   }

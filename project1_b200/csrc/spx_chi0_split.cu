@@ -1,9 +1,543 @@
-// K2 placeholder: split-precision accumulation is enqueued here.
+// K2: split-precision band-pair accumulation on the 5th-generation tensor cores.
+//
+// The sum chi_f(i, j) = sum_p M(p, i) conj(M(p, j)) w(p, f) (src/susceptibility.f:
+// 1182-1240 with the HILBERT NONE weights of :950-975) is evaluated as an exact
+// integer contraction of 8-bit digit slices (an Ozaki-type error-free split):
+//
+//   x = s/127 * (d0 + d1/254 + d2/254^2 + d3/254^3 + r),  |d_t| <= 127, |r| <= 1/2,
+//
+// with s the largest |Re|, |Im| of the column over a slab of band pairs. The
+// unweighted operand A = M keeps 3 slices, the weighted operand B = w_f M keeps 4
+// (its column scale is s_j * max_p |w(p,f)|, so its relative resolution must
+// absorb the spread of the weights). Digit products with t + u <= 3 are summed on
+// tcgen05.mma kind::i8 into four int32 accumulators in tensor memory, one per
+// order g = t + u, which is exact: no rounding happens inside the contraction.
+// Once per slab of 32768 pairs (the int32 headroom) the epilogue forms
+// ((D0*254 + D1)*254 + D2)*254 + D3 exactly in int64 and adds
+// s_i s_j wmax_f / (127^2 254^3) times it to the FP64 output. The weights and
+// the scale factors stay FP64 throughout; near-degenerate pairs therefore keep
+// their FP64 weights.
+//
+// Error (per element, relative to sqrt|chi_ii chi_jj|): slicing of A <= 2^-24.9
+// times the column crest factor, slicing of B <= 2^-31.9 times the weighted crest
+// factor, dropped orders g >= 4 bounded by the same; see the accuracy tests.
+//
+// Tile layout: a 64 x 64 complex tile is a 128 x 128 real-stacked product: A rows
+// are (Re M_i | Im M_i) for 64 mixed-basis functions, B rows likewise for the
+// 64 columns j; D[(c,i)][(c',j)] holds the four real products, combined in the
+// epilogue as re = D[re_i][re_j] + D[im_i][im_j], im = D[im_i][re_j] - D[re_i][im_j]
+// (the two halves live in different TMEM lane quarters and meet in shared memory).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
 #include "spx_common.cuh"
+#include "spx_tcgen05.cuh"
+
 namespace spx {
-size_t split_workspace_bytes(int64_t, int, int) { return 0; }
-int split_chi0_slab(spx_ctx* ctx, const double2*, int64_t, int64_t, int, const double*, int64_t,
-                    int, double2*, void*, size_t, cudaStream_t, int*, cudaEvent_t) {
-  return set_error(ctx, SPX_ENOTSUP, "split precision not built");
+
+constexpr int SP_TILE = 64;            // complex rows / columns per tile
+constexpr int SP_ROWS = 128;           // real-stacked rows per tile (re | im)
+constexpr int SP_KB = 32;              // band pairs per pipeline stage = one int8 MMA K step
+constexpr int SP_SA = 3;               // digit slices of the unweighted operand
+constexpr int SP_SB = 4;               // digit slices of the weighted operand
+constexpr int SP_ST = 6;               // pipeline stages
+constexpr int SP_SLAB = 32768;         // band pairs per exact int32 accumulation
+constexpr int SP_THREADS = 192;        // warp 0 TMA, warp 1 MMA + TMEM, warps 2-5 epilogue
+constexpr int SP_PLANE = SP_ROWS * SP_KB;  // bytes of one slice of one stage
+constexpr int SP_TMEM_COLS = 512;      // 4 orders x 128 columns of int32
+constexpr double SP_RADIX = 254.0;
+
+// idesc for kind::i8: D s32 (bits 4-5 = 2), A/B signed int8 (bits 7-9, 10-12 = 1),
+// K-major A and B, N = 128 (bits 17-22 = N/8), M = 128 (bits 24-28 = M/16).
+constexpr uint32_t SP_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(SP_ROWS / 8) << 17) |
+                              ((uint32_t)(SP_ROWS / 16) << 24);
+
+struct __align__(1024) SplitSmem {
+  uint8_t a[SP_ST][SP_SA][SP_PLANE];
+  uint8_t b[SP_ST][SP_SB][SP_PLANE];
+  long long xchg[2][SP_TILE][33];      // epilogue exchange of the (row, Im col) halves
+  uint64_t full[SP_ST];
+  uint64_t empty[SP_ST];
+  uint64_t tfull, tempty, xfull, xfree, mdone;
+  uint32_t tmem_base;
+};
+
+struct SplitParams {
+  int N;
+  int ntile;
+  int nw;
+  int nitems;
+  int nk;                 // pipeline stages per item (pairs of the slab / 32)
+  const double* sA;       // column scales of the slab
+  const double* wmax;     // max |w(p, f)| of the slab
+  double* out;            // packed complex output, as doubles
+  int64_t npack;
+  int* status;
+  uint64_t timeout_ns;
+};
+
+__device__ __forceinline__ void split_decode_tile(int t, int* bi, int* bj) {
+  int j = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
+  while (j * (j + 1) / 2 > t) --j;
+  while ((j + 1) * (j + 2) / 2 <= t) ++j;
+  *bj = j;
+  *bi = t - j * (j + 1) / 2;
 }
+
+// T = ((D0*254 + D1)*254 + D2)*254 + D3 for 32 columns starting at `taddr`, where
+// D_g sits 128 g columns further: the exact integer value of the slab's sum.
+__device__ __forceinline__ void load_orders(uint32_t taddr, long long (&T)[32]) {
+  int32_t r[32];
+  tmem_ld32(taddr, r);
+  tmem_wait_ld();
+#pragma unroll
+  for (int k = 0; k < 32; ++k) T[k] = r[k];
+#pragma unroll
+  for (int g = 1; g < 4; ++g) {
+    tmem_ld32(taddr + (uint32_t)(g * 128), r);
+    tmem_wait_ld();
+#pragma unroll
+    for (int k = 0; k < 32; ++k) T[k] = T[k] * 254 + r[k];
+  }
+}
+
+__global__ void __launch_bounds__(SP_THREADS, 1)
+    split_gram_kernel(const __grid_constant__ CUtensorMap mapA,
+                      const __grid_constant__ CUtensorMap mapB, SplitParams prm) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  SplitSmem& sm = *reinterpret_cast<SplitSmem*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < SP_ST; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], 1);
+    }
+    mbar_init(&sm.tfull, 1);
+    mbar_init(&sm.tempty, 4);
+    mbar_init(&sm.xfull, 4);
+    mbar_init(&sm.xfree, 4);
+    mbar_init(&sm.mdone, 1);
+    fence_barrier_init();
+  }
+  if (warp == 1) tmem_alloc(&sm.tmem_base, SP_TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sm.tmem_base;
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      int st = 0;
+      uint32_t ph = 0;
+      bool issued[SP_ST];
+      uint32_t last_ph[SP_ST];
+      for (int s = 0; s < SP_ST; ++s) issued[s] = false, last_ph[s] = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; item < prm.nitems && ok; item += gridDim.x) {
+        const int f = item / prm.ntile;
+        int bi, bj;
+        split_decode_tile(item % prm.ntile, &bi, &bj);
+        for (int ks = 0; ks < prm.nk; ++ks) {
+          if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&sm.full[st], (uint32_t)((SP_SA + SP_SB) * SP_PLANE));
+          tma_load_3d(&sm.a[st][0][0], &mapA, ks * SP_KB, bi * SP_ROWS, 0, &sm.full[st]);
+          tma_load_3d(&sm.b[st][0][0], &mapB, ks * SP_KB, bj * SP_ROWS, f * SP_SB, &sm.full[st]);
+          issued[st] = true;
+          last_ph[st] = ph;
+          if (++st == SP_ST) st = 0, ph ^= 1u;
+        }
+      }
+      // copies still landing must finish before this CTA's shared memory goes away
+      for (int s = 0; s < SP_ST; ++s)
+        if (issued[s]) mbar_drain(&sm.full[s], last_ph[s], prm.timeout_ns);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      int st = 0;
+      uint32_t ph = 0;
+      int j = 0;
+      bool committed = false;
+      for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j) {
+        // accumulators free (first item: immediately)
+        if (!mbar_wait(&sm.tempty, (uint32_t)(j & 1) ^ 1u, prm.timeout_ns, prm.status)) break;
+        tc_fence_after();
+        bool ok = true;
+        for (int ks = 0; ks < prm.nk; ++ks) {
+          if (!mbar_wait(&sm.full[st], ph, prm.timeout_ns, prm.status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          uint64_t da[SP_SA], db[SP_SB];
+#pragma unroll
+          for (int t = 0; t < SP_SA; ++t) da[t] = desc_sw32(&sm.a[st][t][0]);
+#pragma unroll
+          for (int u = 0; u < SP_SB; ++u) db[u] = desc_sw32(&sm.b[st][u][0]);
+          // order g = t + u lives at TMEM columns [128 g, 128 g + 128); the first
+          // product of every order in a slab (t == 0, ks == 0) overwrites it
+          const uint32_t k0 = ks > 0;
+          mma_i8<1>(tmem + 0 * 128, da[0], db[0], SP_IDESC, k0);
+          mma_i8<2>(tmem + 1 * 128, da[0], db[1], SP_IDESC, k0);
+          mma_i8<2>(tmem + 2 * 128, da[0], db[2], SP_IDESC, k0);
+          mma_i8<3>(tmem + 3 * 128, da[0], db[3], SP_IDESC, k0);
+          mma_i8<1>(tmem + 1 * 128, da[1], db[0], SP_IDESC, 1u);
+          mma_i8<2>(tmem + 2 * 128, da[1], db[1], SP_IDESC, 1u);
+          mma_i8<3>(tmem + 3 * 128, da[1], db[2], SP_IDESC, 1u);
+          mma_i8<1>(tmem + 2 * 128, da[2], db[0], SP_IDESC, 1u);
+          mma_i8<3>(tmem + 3 * 128, da[2], db[1], SP_IDESC, 1u);
+          tc_commit(&sm.empty[st]);  // stage free once these MMAs have read it
+          committed = true;
+          if (++st == SP_ST) st = 0, ph ^= 1u;
+        }
+        if (!ok) break;
+        tc_commit(&sm.tfull);  // accumulators complete
+      }
+      // every MMA issued by this thread must retire before TMEM is released: a
+      // commit issued now arrives once all of them are done
+      if (committed) {
+        tc_commit(&sm.mdone);
+        mbar_drain(&sm.mdone, 0u, prm.timeout_ns);
+      }
+    }
+  } else {
+    // ---------------- epilogue: 4 warps, one TMEM lane quarter each ----------------
+    const int q = warp & 3;                 // lane quarter
+    const bool is_re = q < 2;               // lanes 0-63: Re rows, 64-127: Im rows
+    const int ii = (q & 1) * 32 + lane;     // complex row within the tile
+    const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16);
+    int j = 0;
+    uint32_t xseq = 0;
+    for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j) {
+      if (!mbar_wait(&sm.tfull, (uint32_t)(j & 1), prm.timeout_ns, prm.status)) break;
+      tc_fence_after();
+      const int f = item / prm.ntile;
+      int bi, bj;
+      split_decode_tile(item % prm.ntile, &bi, &bj);
+      const int gi = bi * SP_TILE + ii;
+      const double si = gi < prm.N ? prm.sA[gi] : 0.0;
+      const double fac =
+          si * prm.wmax[f] / (127.0 * 127.0 * SP_RADIX * SP_RADIX * SP_RADIX);
+      double* outf = prm.out + 2 * (int64_t)f * prm.npack;
+      bool ok = true;
+      for (int js = 0; js < 2 && ok; ++js, ++xseq) {
+        long long tre[32], tim[32];  // T[row][Re col], T[row][Im col] for 32 columns j
+        load_orders(tl + (uint32_t)(js * 32), tre);
+        load_orders(tl + (uint32_t)(64 + js * 32), tim);
+        // exchange the Im-column halves between the Re and Im rows of each i
+        if (!mbar_wait(&sm.xfree, (xseq & 1u) ^ 1u, prm.timeout_ns, prm.status)) {
+          ok = false;
+          break;
+        }
+#pragma unroll
+        for (int k = 0; k < 32; ++k) sm.xchg[is_re ? 0 : 1][ii][k] = tim[k];
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.xfull);
+        if (!mbar_wait(&sm.xfull, xseq & 1u, prm.timeout_ns, prm.status)) {
+          ok = false;
+          break;
+        }
+        // Re rows: chi_re = T[re_i][re_j] + T[im_i][im_j]; Im rows: chi_im = T[im_i][re_j] - T[re_i][im_j]
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+          const int gj = bj * SP_TILE + js * 32 + k;
+          const long long partner = sm.xchg[is_re ? 1 : 0][ii][k];
+          const long long v = is_re ? tre[k] + partner : tre[k] - partner;
+          if (gi <= gj && gj < prm.N) {
+            double* o = outf + 2 * ((int64_t)gj * (gj + 1) / 2 + gi) + (is_re ? 0 : 1);
+            *o += fac * prm.sA[gj] * (double)v;
+          }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.xfree);
+      }
+      if (!ok) break;
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.tempty);
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc(tmem, SP_TMEM_COLS);
+}
+
+// ---------------------------------------------------------------------------
+// operand preparation
+
+// Column scales of one slab: sA[i] = max_p max(|Re M(p,i)|, |Im M(p,i)|).
+__global__ void split_colmax_kernel(const double2* __restrict__ M, int64_t ldc, int64_t p0,
+                                    int len, double* __restrict__ sA) {
+  const int i = blockIdx.x;
+  const double2* col = M + (int64_t)i * ldc + p0;
+  double m = 0.0;
+  for (int p = threadIdx.x; p < len; p += blockDim.x) {
+    const double2 v = col[p];
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) sA[i] = m;
+  }
+}
+
+// wmax[f] = max_p |w(p, f)| over the slab.
+__global__ void split_wmax_kernel(const double* __restrict__ W, int64_t ldw, int64_t p0, int len,
+                                  double* __restrict__ wmax) {
+  const int f = blockIdx.x;
+  const double* wf = W + (int64_t)f * ldw + p0;
+  double m = 0.0;
+  for (int p = threadIdx.x; p < len; p += blockDim.x) m = fmax(m, fabs(wf[p]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) wmax[f] = m;
+  }
+}
+
+// Digits of y, |y| <= 127: y = d0 + d1/254 + ... (round to nearest at every step).
+template <int S>
+__device__ __forceinline__ void digits(double y, int (&d)[S]) {
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    const double r = rint(y);
+    d[t] = (int)r;
+    y = (y - r) * SP_RADIX;
+  }
+}
+
+// One thread = one complex column i and 16 consecutive pairs of the slab. Writes
+// 16-byte runs of every digit plane: A planes [t][row][p], B planes [f][u][row][p],
+// rows real-stacked (block b of 64 columns -> rows 128 b + {0..63 Re, 64..127 Im}).
+__global__ void split_quantize_kernel(const double2* __restrict__ M, int64_t ldc, int64_t p0,
+                                      int len, int nchunk, int N, int npad, int64_t R, int64_t Ps,
+                                      const double* __restrict__ W, int64_t ldw, int nw,
+                                      const double* __restrict__ sA,
+                                      const double* __restrict__ wmax, int8_t* __restrict__ A,
+                                      int8_t* __restrict__ B) {
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (tid >= (int64_t)npad * nchunk) return;
+  const int i = (int)(tid / nchunk);
+  const int p = (int)(tid % nchunk) * 16;
+  const int64_t r_re = (int64_t)(i / SP_TILE) * SP_ROWS + (i % SP_TILE);
+  const int64_t r_im = r_re + SP_TILE;
+  double xr[16], xi[16];
+  const bool col_ok = i < N;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    double2 v = make_double2(0.0, 0.0);
+    if (col_ok && p + k < len) v = M[(int64_t)i * ldc + p0 + p + k];
+    xr[k] = v.x;
+    xi[k] = v.y;
+  }
+  const double s = col_ok ? sA[i] : 0.0;
+  const double inv = s > 0.0 ? 127.0 / s : 0.0;
+  // unweighted operand: 3 slices
+  {
+    uint32_t pr[SP_SA][4], pi[SP_SA][4];
+#pragma unroll
+    for (int t = 0; t < SP_SA; ++t)
+#pragma unroll
+      for (int w = 0; w < 4; ++w) pr[t][w] = pi[t][w] = 0u;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      int dr[SP_SA], di[SP_SA];
+      digits<SP_SA>(xr[k] * inv, dr);
+      digits<SP_SA>(xi[k] * inv, di);
+#pragma unroll
+      for (int t = 0; t < SP_SA; ++t) {
+        pr[t][k >> 2] |= ((uint32_t)dr[t] & 0xffu) << (8 * (k & 3));
+        pi[t][k >> 2] |= ((uint32_t)di[t] & 0xffu) << (8 * (k & 3));
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < SP_SA; ++t) {
+      *reinterpret_cast<uint4*>(A + (t * R + r_re) * Ps + p) =
+          make_uint4(pr[t][0], pr[t][1], pr[t][2], pr[t][3]);
+      *reinterpret_cast<uint4*>(A + (t * R + r_im) * Ps + p) =
+          make_uint4(pi[t][0], pi[t][1], pi[t][2], pi[t][3]);
+    }
+  }
+  // weighted operand, one frequency at a time: 4 slices
+  for (int f = 0; f < nw; ++f) {
+    const double wm = wmax[f];
+    const double g = (s > 0.0 && wm > 0.0) ? 127.0 / (wm * s) : 0.0;
+    const double* wf = W + (int64_t)f * ldw + p0 + p;
+    uint32_t pr[SP_SB][4], pi[SP_SB][4];
+#pragma unroll
+    for (int u = 0; u < SP_SB; ++u)
+#pragma unroll
+      for (int w = 0; w < 4; ++w) pr[u][w] = pi[u][w] = 0u;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const double wk = (p + k < len) ? wf[k] * g : 0.0;
+      int dr[SP_SB], di[SP_SB];
+      digits<SP_SB>(xr[k] * wk, dr);
+      digits<SP_SB>(xi[k] * wk, di);
+#pragma unroll
+      for (int u = 0; u < SP_SB; ++u) {
+        pr[u][k >> 2] |= ((uint32_t)dr[u] & 0xffu) << (8 * (k & 3));
+        pi[u][k >> 2] |= ((uint32_t)di[u] & 0xffu) << (8 * (k & 3));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < SP_SB; ++u) {
+      const int64_t plane = (int64_t)f * SP_SB + u;
+      *reinterpret_cast<uint4*>(B + (plane * R + r_re) * Ps + p) =
+          make_uint4(pr[u][0], pr[u][1], pr[u][2], pr[u][3]);
+      *reinterpret_cast<uint4*>(B + (plane * R + r_im) * Ps + p) =
+          make_uint4(pi[u][0], pi[u][1], pi[u][2], pi[u][3]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn get_encode() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+int make_tmap_u8_3d(spx_ctx* ctx, CUtensorMap* map, const void* base, uint64_t d0, uint64_t d1,
+                    uint64_t d2, uint64_t s1, uint64_t s2, uint32_t b0, uint32_t b1, uint32_t b2,
+                    CUtensorMapSwizzle swz) {
+  auto enc = get_encode();
+  if (!enc) return set_error(ctx, SPX_ECUDA, "cuTensorMapEncodeTiled unavailable");
+  cuuint64_t dims[3] = {d0, d1, d2};
+  cuuint64_t strides[2] = {s1, s2};
+  cuuint32_t box[3] = {b0, b1, b2};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides,
+                   box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return set_error(ctx, SPX_ECUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return SPX_OK;
+}
+
+struct SplitLayout {
+  int64_t Ps, R;
+  int nblk;
+  size_t a_bytes, b_bytes, s_bytes, w_bytes;
+};
+
+static SplitLayout split_layout(int64_t P, int N, int nw) {
+  SplitLayout L;
+  L.Ps = std::min<int64_t>((int64_t)align_up((size_t)std::max<int64_t>(P, 1), SP_KB), SP_SLAB);
+  L.nblk = (N + SP_TILE - 1) / SP_TILE;
+  L.R = (int64_t)L.nblk * SP_ROWS;
+  L.a_bytes = align_up((size_t)SP_SA * L.R * L.Ps, 1024);
+  L.b_bytes = align_up((size_t)SP_SB * nw * L.R * L.Ps, 1024);
+  L.s_bytes = align_up(sizeof(double) * (size_t)std::max(N, 1), 256);
+  L.w_bytes = align_up(sizeof(double) * (size_t)std::max(nw, 1), 256);
+  return L;
+}
+
+size_t split_workspace_bytes(int64_t P, int N, int nw) {
+  SplitLayout L = split_layout(P, N, nw);
+  return L.a_bytes + L.b_bytes + L.s_bytes + L.w_bytes + 1024;
+}
+
+void timing_mark(spx_ctx* ctx, cudaStream_t s, int kind);
+
+int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N, const double* W,
+                    int64_t ldw, int nw, double2* out, void* ws, size_t ws_bytes,
+                    cudaStream_t stream, int* launches, cudaEvent_t /*prep_done*/) {
+  if (P <= 0 || N <= 0 || nw <= 0) return SPX_OK;
+  SplitLayout L = split_layout(P, N, nw);
+  if (!ws || ws_bytes < split_workspace_bytes(P, N, nw))
+    return set_error(ctx, SPX_EINVAL, "split workspace too small");
+  uint8_t* base = (uint8_t*)align_up((size_t)ws, 1024);
+  int8_t* A = (int8_t*)base;
+  int8_t* B = (int8_t*)(base + L.a_bytes);
+  double* sA = (double*)(base + L.a_bytes + L.b_bytes);
+  double* wmax = (double*)(base + L.a_bytes + L.b_bytes + L.s_bytes);
+
+  CUtensorMap mapA, mapB;
+  int rc = make_tmap_u8_3d(ctx, &mapA, A, L.Ps, L.R, SP_SA, L.Ps, L.R * L.Ps, SP_KB, SP_ROWS, SP_SA,
+                           CU_TENSOR_MAP_SWIZZLE_32B);
+  if (rc) return rc;
+  rc = make_tmap_u8_3d(ctx, &mapB, B, L.Ps, L.R, (uint64_t)SP_SB * nw, L.Ps, L.R * L.Ps, SP_KB,
+                       SP_ROWS, SP_SB, CU_TENSOR_MAP_SWIZZLE_32B);
+  if (rc) return rc;
+
+  const size_t smem = sizeof(SplitSmem) + 1024;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(split_gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_set = true;
+  }
+  const int ntile = L.nblk * (L.nblk + 1) / 2;
+  const int nitems = ntile * nw;
+  const int grid = std::min(nitems, ctx->num_sms);
+  const int npad = L.nblk * SP_TILE;
+
+  for (int64_t p0 = 0; p0 < P; p0 += L.Ps) {
+    const int len = (int)std::min<int64_t>(L.Ps, P - p0);
+    const int lenp = (int)align_up((size_t)len, SP_KB);
+    const int nchunk = lenp / 16;
+    timing_mark(ctx, stream, 0);
+    split_colmax_kernel<<<N, 256, 0, stream>>>(M, ldc, p0, len, sA);
+    split_wmax_kernel<<<nw, 256, 0, stream>>>(W, ldw, p0, len, wmax);
+    const int64_t nthr = (int64_t)npad * nchunk;
+    split_quantize_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, stream>>>(
+        M, ldc, p0, len, nchunk, N, npad, L.R, L.Ps, W, ldw, nw, sA, wmax, A, B);
+    rc = check_cuda(ctx, cudaGetLastError(), "split operand preparation");
+    if (rc) return rc;
+    timing_mark(ctx, stream, 1);
+    SplitParams prm;
+    prm.N = N;
+    prm.ntile = ntile;
+    prm.nw = nw;
+    prm.nitems = nitems;
+    prm.nk = lenp / SP_KB;
+    prm.sA = sA;
+    prm.wmax = wmax;
+    prm.out = reinterpret_cast<double*>(out);
+    prm.npack = (int64_t)N * (N + 1) / 2;
+    prm.status = ctx->d_status;
+    prm.timeout_ns =
+        (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
+    split_gram_kernel<<<grid, SP_THREADS, smem, stream>>>(mapA, mapB, prm);
+    rc = check_cuda(ctx, cudaGetLastError(), "split_gram_kernel launch");
+    if (rc) return rc;
+    *launches += 4;
+  }
+  return SPX_OK;
+}
+
 }  // namespace spx

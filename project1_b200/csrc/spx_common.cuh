@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/spexgpu.h"
 
@@ -26,6 +27,11 @@ struct spx_ctx {
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
   cudaEvent_t ev[8] = {};
+  // optional per-kernel timing: marks recorded on the stream, summed after a sync
+  bool timing = false;
+  std::vector<cudaEvent_t> mark_pool;
+  std::vector<int> mark_kind;
+  size_t nmarks = 0;
 };
 
 namespace spx {
@@ -40,6 +46,11 @@ int ensure_workspace(spx_ctx* ctx, size_t bytes);
 int ensure_pinned(spx_ctx* ctx, size_t bytes);
 // Reads and clears the device status word (synchronises `stream`).
 int collect_status(spx_ctx* ctx, cudaStream_t stream, const char* what);
+// Records a timing mark of `kind` (0 = operand preparation, 1 = band-pair
+// accumulation, 2 = end) when ctx->timing is set.
+void timing_mark(spx_ctx* ctx, cudaStream_t s, int kind);
+// Sums the intervals between consecutive marks per kind (after a sync) and clears them.
+void timing_collect(spx_ctx* ctx, double* ms_prep, double* ms_gram);
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 inline cudaStream_t pick_stream(spx_ctx* ctx, void* s) {
   return s ? (cudaStream_t)s : ctx->stream;

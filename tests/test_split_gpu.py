@@ -1,0 +1,95 @@
+"""Split-precision (int8 digit slices on tcgen05) accumulation against the FP64 oracle."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+import oracle
+import project1_b200 as spx
+from project1_b200 import inputs
+from chi0_util import normalized_error
+from test_chi0_gpu import DEV, G, random_case, run_dev
+
+pytestmark = pytest.mark.gpu
+SPLIT_TOL = 1e-6       # per-element error / sqrt(|chi_ii chi_jj|), split path
+SPLIT_FRO = 1e-7       # Frobenius relative error, split path
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = spx.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("name", sorted({k.split("/")[0] for k in G.files if "/" in k}))
+def test_split_matches_golden(ctx, name):
+    m, d, om = G[f"{name}/cprod"], G[f"{name}/ediff"], G[f"{name}/omega"]
+    ws = G[f"{name}/wscale"] if f"{name}/wscale" in G.files else None
+    ref = G[f"{name}/susceph"]
+    got = run_dev(ctx, np.asfortranarray(m), d, om, ws, float(G["scale_all"]), precision="split")
+    emax, fro = normalized_error(got, ref, m.shape[1])
+    assert emax <= SPLIT_TOL and fro <= SPLIT_FRO, (emax, fro)
+
+
+@pytest.mark.parametrize("nbas,npair,nw,degfrac", [
+    (1, 1, 1, 0.0), (7, 5, 3, 0.0), (64, 32, 1, 0.0), (65, 33, 2, 0.1), (130, 100, 3, 0.01),
+    (200, 5000, 3, 0.01), (257, 64, 1, 0.0)])
+def test_split_matches_oracle_shapes(ctx, nbas, npair, nw, degfrac):
+    m, d, om = random_case(nbas, npair, nw, seed=7 * nbas + npair, degfrac=degfrac)
+    ref = oracle.chi0(m, oracle.weights(d, om), accurate=True)
+    got = run_dev(ctx, m, d, om, precision="split")
+    emax, fro = normalized_error(got, ref, nbas)
+    assert emax <= SPLIT_TOL and fro <= SPLIT_FRO, (emax, fro)
+
+
+def test_split_several_slabs(ctx):
+    """P above one exact int32 slab (32768 pairs): slabs are reduced in FP64."""
+    m, d, om = random_case(80, 70000, 2, seed=3, degfrac=0.01)
+    ref = oracle.chi0(m, oracle.weights(d, om, None, 1 / 64), accurate=True)
+    got = run_dev(ctx, m, d, om, None, 1 / 64, precision="split")
+    emax, fro = normalized_error(got, ref, 80)
+    assert emax <= SPLIT_TOL and fro <= SPLIT_FRO, (emax, fro)
+
+
+def test_split_c0_full_config(ctx):
+    w = inputs.CONFIGS["c0"]
+    m = inputs.cprod_host(w)
+    d = inputs.pair_ediff(w)
+    om = inputs.frequencies(w.nw)
+    ref = oracle.chi0(m, oracle.weights(d, om, None, 1.0 / w.nk), accurate=True)
+    got = run_dev(ctx, m, d, om, None, 1.0 / w.nk, precision="split")
+    emax, fro = normalized_error(got, ref, w.nbas)
+    print(f"c0 split: max normalised {emax:.3e}, Frobenius {fro:.3e}")
+    assert emax <= SPLIT_TOL and fro <= SPLIT_FRO, (emax, fro)
+
+
+def test_split_degenerate_pairs_keep_fp64_weights(ctx):
+    """Pairs with |e_n'-e_n| < 1e-6 eV carry weights ~1e-5 of the rest; they must still count."""
+    rng = np.random.default_rng(4)
+    nbas, npair = 48, 400
+    m = np.asfortranarray((rng.standard_normal((npair, nbas)) + 1j * rng.standard_normal((npair, nbas))) / 7)
+    d = rng.uniform(0, 1e-6, npair)          # every pair degenerate
+    om = inputs.frequencies(3)
+    ref = oracle.chi0(m, oracle.weights(d, om), accurate=True)
+    got = run_dev(ctx, m, d, om, precision="split")
+    emax, fro = normalized_error(got, ref, nbas)
+    assert emax <= SPLIT_TOL and fro <= SPLIT_FRO, (emax, fro)
+
+
+def test_split_host_path(ctx):
+    m, d, om = random_case(96, 1000, 3, seed=11)
+    ref = oracle.chi0(m, oracle.weights(d, om, None, 0.25), accurate=True)
+    with spx.Context(0, chunk_pairs=320) as c:
+        out = np.zeros((96 * 97 // 2, 3), complex, order="F")
+        c.chi0_accumulate(m, d, om, out, scale_all=0.25, precision="split")
+    emax, fro = normalized_error(out, ref, 96)
+    assert emax <= SPLIT_TOL, emax
+
+
+def test_split_accumulates(ctx):
+    m, d, om = random_case(40, 50, 2, seed=5)
+    init = np.asfortranarray(np.random.default_rng(3).standard_normal((40 * 41 // 2, 2)) * 1e-3 + 0j)
+    ref = oracle.chi0(m, oracle.weights(d, om), accurate=True, susceph=init.copy(order="F"))
+    got = run_dev(ctx, m, d, om, init=init, precision="split")
+    assert np.max(np.abs(got - ref)) <= 1e-6 * np.max(np.abs(ref))
