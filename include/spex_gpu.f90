@@ -1,0 +1,71 @@
+! spex_gpu.f90 - ISO_C_BINDING interfaces of libspexgpu (include/spexgpu.h) for
+! the SPEX Fortran driver. Every routine returns an integer(c_int) status,
+! 0 on success; spx_last_error gives the message of the last failure.
+!
+! Arrays are passed exactly as SPEX holds them: cprod(npair, nbas) and
+! susceph(nbas*(nbas+1)/2, nfrqh) as complex(c_double_complex), column-major.
+!
+! This module is interface-only; it is not compiled in the build image (no
+! Fortran compiler is installed there).
+module spex_gpu
+  use, intrinsic :: iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: SPX_OK = 0, SPX_EINVAL = -1, SPX_ENOMEM = -2, &
+                               SPX_ECUDA = -3, SPX_ETIMEOUT = -4, SPX_ENOTSUP = -5, &
+                               SPX_ENODEV = -6
+  integer(c_int), parameter :: SPX_FP64 = 0, SPX_SPLIT = 1
+
+  type, bind(c) :: spx_options
+    integer(c_int32_t) :: struct_size = 32
+    integer(c_int32_t) :: verbose = 0
+    integer(c_int64_t) :: workspace_limit = 0
+    integer(c_int64_t) :: pinned_limit = 0
+    integer(c_int32_t) :: chunk_pairs = 0
+    integer(c_int32_t) :: timeout_ms = 0
+  end type
+
+  type, bind(c) :: spx_chi0_stats
+    real(c_double)     :: ms_total, ms_gram, ms_prep, flops
+    integer(c_int64_t) :: h2d_bytes, d2h_bytes
+    integer(c_int32_t) :: kernel_launches, precision
+  end type
+
+  interface
+    integer(c_int) function spx_ctx_create(device, opt, ctx) bind(c, name='spx_ctx_create')
+      import :: c_int, c_ptr, spx_options
+      integer(c_int), value :: device
+      type(spx_options), intent(in) :: opt
+      type(c_ptr), intent(out) :: ctx
+    end function
+
+    integer(c_int) function spx_ctx_destroy(ctx) bind(c, name='spx_ctx_destroy')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+
+    type(c_ptr) function spx_last_error(ctx) bind(c, name='spx_last_error')
+      import :: c_ptr
+      type(c_ptr), value :: ctx
+    end function
+
+    ! replaces src/susceptibility.f:950-975 (weights) and :1182-1240 (body loop)
+    integer(c_int) function spx_chi0_accumulate(ctx, cprod, ldc, npair, nbas, ediff, wscale, &
+                                                scale_all, nw, omega, precision, susceph, stats) &
+                                                bind(c, name='spx_chi0_accumulate')
+      import :: c_int, c_int32_t, c_int64_t, c_ptr, c_double, c_double_complex, spx_chi0_stats
+      type(c_ptr), value :: ctx
+      complex(c_double_complex), intent(in) :: cprod(*)
+      integer(c_int64_t), value :: ldc, npair
+      integer(c_int32_t), value :: nbas
+      real(c_double), intent(in) :: ediff(*)
+      type(c_ptr), value :: wscale                 ! c_loc(wscale) or c_null_ptr
+      real(c_double), value :: scale_all
+      integer(c_int32_t), value :: nw
+      real(c_double), intent(in) :: omega(*)
+      integer(c_int32_t), value :: precision
+      complex(c_double_complex), intent(inout) :: susceph(*)
+      type(spx_chi0_stats), intent(out) :: stats
+    end function
+  end interface
+end module spex_gpu
