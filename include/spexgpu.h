@@ -116,6 +116,20 @@ int spx_chi0_accumulate_dev(spx_ctx* ctx, const double* cprod, int64_t ldc,
                             int32_t nw, const double* omega, int32_t precision,
                             double* susceph, void* stream, spx_chi0_stats* stats);
 
+/* Allocation-free FP64 accumulation; no counterpart in the reference.
+ * For callers that cannot call cudaMalloc, such as a Fortran host whose device
+ * memory belongs to its OpenMP/OpenACC offload runtime or to a pool allocator.
+ * It takes no context and allocates nothing. Its scratch (the FP64 weights of
+ * one slab of pairs) is a static 32 MiB device array that every GPU loading
+ * the library keeps until exit. The first call on a device must come before any
+ * stream capture. Calls that overlap on the GPU race on the shared scratch.
+ * nw > 262144 is rejected with SPX_EINVAL. Device pointers, on the current
+ * device; returns after `stream` has finished the work. */
+int spx_chi0_accumulate_dev_noalloc(const double* cprod, int64_t ldc, int64_t npair,
+                                    int32_t nbas, const double* ediff, const double* wscale,
+                                    double scale_all, int32_t nw, const double* omega,
+                                    double* susceph, void* stream);
+
 /* Multiplies n complex elements of a device array by a real factor: the spin
  * factor 2 of src/susceptibility.f:1331-1343 for unpolarised, non-SOC runs. */
 int spx_scale_dev(spx_ctx* ctx, double* z, int64_t n, double factor, void* stream);

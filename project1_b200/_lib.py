@@ -68,6 +68,8 @@ SIGNATURES = {
         [_P, _P, _I64, _I64, _I32, _P, _P, C.c_double, _I32, _P, _I32, _P, _P, C.POINTER(spx_chi0_stats)],
     ),
     "spx_scale_dev": (C.c_int, [_P, _P, _I64, C.c_double, _P]),
+    "spx_chi0_accumulate_dev_noalloc": (
+        C.c_int, [_P, _I64, _I64, _I32, _P, _P, C.c_double, _I32, _P, _P, _P]),
     "spx_gen_normal_host": (None, [C.c_uint64, C.c_uint32, _I64, _I64, C.c_double, _P]),
     "spx_gen_normal_dev": (C.c_int, [_P, C.c_uint64, C.c_uint32, _I64, _I64, C.c_double, _P, _P]),
     "spx_gen_cmatrix_host": (None, [C.c_uint64, C.c_uint32, _I64, _I64, _I64, _I64, C.c_double, _P]),

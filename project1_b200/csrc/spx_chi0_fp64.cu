@@ -294,3 +294,38 @@ int launch_chi0_fp64(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int
 }
 
 }  // namespace spx
+
+namespace spx {
+
+// Launches K1 with explicit device resources instead of a context: used by the
+// allocation-free entry point, whose status word and weights live in static
+// device memory.
+int launch_chi0_fp64_noctx(int num_sms, int* status, uint64_t timeout_ns, const double2* M,
+                           int64_t ldc, int64_t P, int N, const double* W, int64_t ldw, int nw,
+                           double2* out, cudaStream_t stream) {
+  if (P <= 0 || N <= 0 || nw <= 0) return SPX_OK;
+  const int nblk = (N + F64_B - 1) / F64_B;
+  F64Params prm;
+  prm.M = M;
+  prm.ldc = ldc;
+  prm.P = P;
+  prm.N = N;
+  prm.W = W;
+  prm.ldw = ldw;
+  prm.nw = nw;
+  prm.out = out;
+  prm.npack = (int64_t)N * (N + 1) / 2;
+  prm.ntile = nblk * (nblk + 1) / 2;
+  prm.nitems = (int64_t)prm.ntile * nw;
+  prm.status = status;
+  prm.timeout_ns = timeout_ns;
+  const size_t smem = sizeof(F64Smem);
+  if (cudaFuncSetAttribute(chi0_fp64_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return SPX_ECUDA;
+  const int grid = (int)std::min<int64_t>(prm.nitems, (int64_t)2 * num_sms);
+  chi0_fp64_kernel<8><<<grid, F64_THREADS, smem, stream>>>(prm);
+  return cudaGetLastError() == cudaSuccess ? SPX_OK : SPX_ECUDA;
+}
+
+}  // namespace spx

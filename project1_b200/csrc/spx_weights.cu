@@ -115,3 +115,18 @@ extern "C" void spx_gen_cmatrix_host(uint64_t seed, uint32_t stream_id, int64_t 
       out[2 * (c * ld + p) + 1] = scale * z1;
     }
 }
+
+namespace spx {
+
+// Weights launch with explicit resources (no context): see launch_chi0_fp64_noctx.
+int launch_weights_noctx(int num_sms, int64_t P, int64_t ldw, const double* ediff,
+                         const double* wscale, double scale_all, int nw, const double* omega,
+                         double* w, cudaStream_t stream) {
+  const int64_t total = ldw * nw;
+  if (total <= 0) return SPX_OK;
+  const int grid = (int)std::min<int64_t>((total + 255) / 256, (int64_t)num_sms * 16);
+  weights_kernel<<<grid, 256, 0, stream>>>(P, ldw, ediff, wscale, scale_all, nw, omega, w);
+  return cudaGetLastError() == cudaSuccess ? SPX_OK : SPX_ECUDA;
+}
+
+}  // namespace spx
