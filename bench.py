@@ -337,7 +337,7 @@ def run_ours(args):
         res = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "bf16x3->f32->f64" if head == "split" else "f64",
+            "vs_baseline": None, "dtype": "int8x(3x4 digits)->int32->f64" if head == "split" else "f64",
             "data": "synthetic (seeded Philox4x32-10 normals, uniform energies, Gauss-Legendre frequencies)",
             "config": {"workload": workload_name(w), "nbas": N, "npair": P, "nw": nw,
                        "headline_precision": head, "parallelism": f"pairs sharded over {world} GPU(s)",

@@ -4,23 +4,26 @@
 // 1182-1240 with the HILBERT NONE weights of :950-975) is evaluated as an exact
 // integer contraction of 8-bit digit slices (an Ozaki-type error-free split):
 //
-//   x = s/127 * (d0 + d1/254 + d2/254^2 + d3/254^3 + r),  |d_t| <= 127, |r| <= 1/2,
+//   x = s/127 * (d0 + d1/256 + d2/256^2 + d3/256^3 + r/256^3),  |d0| <= 127,
+//   d1..d3 in [-128, 127], |r| <= 1/2,
 //
 // with s the largest |Re|, |Im| of the column over a slab of band pairs. The
+// digits are the balanced base-256 bytes of one integer, round(x*127/s * 2^24),
+// so a single FP64 -> int32 rounding per value produces all of them. The
 // unweighted operand A = M keeps 3 slices, the weighted operand B = w_f M keeps 4
 // (its column scale is s_j * max_p |w(p,f)|, so its relative resolution must
 // absorb the spread of the weights). Digit products with t + u <= 3 are summed on
 // tcgen05.mma kind::i8 into four int32 accumulators in tensor memory, one per
 // order g = t + u, which is exact: no rounding happens inside the contraction.
-// Once per slab of 32768 pairs (the int32 headroom) the epilogue forms
-// ((D0*254 + D1)*254 + D2)*254 + D3 exactly in int64 and adds
-// s_i s_j wmax_f / (127^2 254^3) times it to the FP64 output. The weights and
+// Once per slab of 32768 pairs (the int32 headroom: 3 * 128^2 * 32768 < 2^31) the
+// epilogue forms ((D0*256 + D1)*256 + D2)*256 + D3 exactly in int64 and adds
+// s_i s_j wmax_f / (127^2 2^24) times it to the FP64 output. The weights and
 // the scale factors stay FP64 throughout; near-degenerate pairs therefore keep
 // their FP64 weights.
 //
-// Error (per element, relative to sqrt|chi_ii chi_jj|): slicing of A <= 2^-24.9
-// times the column crest factor, slicing of B <= 2^-31.9 times the weighted crest
-// factor, dropped orders g >= 4 bounded by the same; see the accuracy tests.
+// Error (per element, relative to sqrt|chi_ii chi_jj|): slicing of A <= 2^-24/127
+// times the column crest factor, slicing of B <= 2^-32/127 times the weighted
+// crest factor, dropped orders g >= 4 bounded by the same; see the accuracy tests.
 //
 // Tile layout: a 64 x 64 complex tile is a 128 x 128 real-stacked product: A rows
 // are (Re M_i | Im M_i) for 64 mixed-basis functions, B rows likewise for the
@@ -48,7 +51,7 @@ constexpr int SP_SLAB = 32768;         // band pairs per exact int32 accumulatio
 constexpr int SP_THREADS = 192;        // warp 0 TMA, warp 1 MMA + TMEM, warps 2-5 epilogue
 constexpr int SP_PLANE = SP_ROWS * SP_KB;  // bytes of one slice of one stage
 constexpr int SP_TMEM_COLS = 512;      // 4 orders x 128 columns of int32
-constexpr double SP_RADIX = 254.0;
+
 
 // idesc for kind::i8: D s32 (bits 4-5 = 2), A/B signed int8 (bits 7-9, 10-12 = 1),
 // K-major A and B, N = 128 (bits 17-22 = N/8), M = 128 (bits 24-28 = M/16).
@@ -87,7 +90,7 @@ __device__ __forceinline__ void split_decode_tile(int t, int* bi, int* bj) {
   *bi = t - j * (j + 1) / 2;
 }
 
-// T = ((D0*254 + D1)*254 + D2)*254 + D3 for 32 columns starting at `taddr`, where
+// T = ((D0*256 + D1)*256 + D2)*256 + D3 for 32 columns starting at `taddr`, where
 // D_g sits 128 g columns further: the exact integer value of the slab's sum.
 __device__ __forceinline__ void load_orders(uint32_t taddr, long long (&T)[32]) {
   int32_t r[32];
@@ -100,7 +103,7 @@ __device__ __forceinline__ void load_orders(uint32_t taddr, long long (&T)[32]) 
     tmem_ld32(taddr + (uint32_t)(g * 128), r);
     tmem_wait_ld();
 #pragma unroll
-    for (int k = 0; k < 32; ++k) T[k] = T[k] * 254 + r[k];
+    for (int k = 0; k < 32; ++k) T[k] = T[k] * 256 + r[k];
   }
 }
 
@@ -226,7 +229,7 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       const int gi = bi * SP_TILE + ii;
       const double si = gi < prm.N ? prm.sA[gi] : 0.0;
       const double fac =
-          si * prm.wmax[f] / (127.0 * 127.0 * SP_RADIX * SP_RADIX * SP_RADIX);
+          si * prm.wmax[f] * (1.0 / (127.0 * 127.0 * 16777216.0));
       double* outf = prm.out + 2 * (int64_t)f * prm.npack;
       bool ok = true;
       for (int js = 0; js < 2 && ok; ++js, ++xseq) {
@@ -315,15 +318,17 @@ __global__ void split_wmax_kernel(const double* __restrict__ W, int64_t ldw, int
   }
 }
 
-// Digits of y, |y| <= 127: y = d0 + d1/254 + ... (round to nearest at every step).
+// Balanced base-256 digits of the integer Y = sum_t d_t 256^(S-1-t): low bytes
+// sign-extended, the rest carried up; |Y| <= 127 * 256^(S-1) keeps |d0| <= 127.
 template <int S>
-__device__ __forceinline__ void digits(double y, int (&d)[S]) {
+__device__ __forceinline__ void digits(int Y, int (&d)[S]) {
 #pragma unroll
-  for (int t = 0; t < S; ++t) {
-    const double r = rint(y);
-    d[t] = (int)r;
-    y = (y - r) * SP_RADIX;
+  for (int t = S - 1; t > 0; --t) {
+    const int lo = (int)(int8_t)(Y & 0xff);
+    d[t] = lo;
+    Y = (Y - lo) >> 8;
   }
+  d[0] = Y;
 }
 
 // One thread = one complex column i and 16 consecutive pairs of the slab. Writes
@@ -351,7 +356,7 @@ __global__ void split_quantize_kernel(const double2* __restrict__ M, int64_t ldc
     xi[k] = v.y;
   }
   const double s = col_ok ? sA[i] : 0.0;
-  const double inv = s > 0.0 ? 127.0 / s : 0.0;
+  const double inv = s > 0.0 ? 127.0 * 65536.0 / s : 0.0;  // 3 digits: scale 2^16
   // unweighted operand: 3 slices
   {
     uint32_t pr[SP_SA][4], pi[SP_SA][4];
@@ -362,8 +367,8 @@ __global__ void split_quantize_kernel(const double2* __restrict__ M, int64_t ldc
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
       int dr[SP_SA], di[SP_SA];
-      digits<SP_SA>(xr[k] * inv, dr);
-      digits<SP_SA>(xi[k] * inv, di);
+      digits<SP_SA>(__double2int_rn(xr[k] * inv), dr);
+      digits<SP_SA>(__double2int_rn(xi[k] * inv), di);
 #pragma unroll
       for (int t = 0; t < SP_SA; ++t) {
         pr[t][k >> 2] |= ((uint32_t)dr[t] & 0xffu) << (8 * (k & 3));
@@ -381,7 +386,7 @@ __global__ void split_quantize_kernel(const double2* __restrict__ M, int64_t ldc
   // weighted operand, one frequency at a time: 4 slices
   for (int f = 0; f < nw; ++f) {
     const double wm = wmax[f];
-    const double g = (s > 0.0 && wm > 0.0) ? 127.0 / (wm * s) : 0.0;
+    const double g = (s > 0.0 && wm > 0.0) ? 127.0 * 16777216.0 / (wm * s) : 0.0;  // 4 digits: 2^24
     const double* wf = W + (int64_t)f * ldw + p0 + p;
     uint32_t pr[SP_SB][4], pi[SP_SB][4];
 #pragma unroll
@@ -392,8 +397,8 @@ __global__ void split_quantize_kernel(const double2* __restrict__ M, int64_t ldc
     for (int k = 0; k < 16; ++k) {
       const double wk = (p + k < len) ? wf[k] * g : 0.0;
       int dr[SP_SB], di[SP_SB];
-      digits<SP_SB>(xr[k] * wk, dr);
-      digits<SP_SB>(xi[k] * wk, di);
+      digits<SP_SB>(__double2int_rn(xr[k] * wk), dr);
+      digits<SP_SB>(__double2int_rn(xi[k] * wk), di);
 #pragma unroll
       for (int u = 0; u < SP_SB; ++u) {
         pr[u][k >> 2] |= ((uint32_t)dr[u] & 0xffu) << (8 * (k & 3));
