@@ -197,20 +197,28 @@ __global__ void __launch_bounds__(F64_THREADS, 2) chi0_fp64_kernel(F64Params prm
             ar[2 * q + h] = valid[q] ? v.x : 0.0;
             ai[2 * q + h] = valid[q] ? v.y : 0.0;
           }
+        // two column slices at a time: the two MMAs that share an accumulator are
+        // three independent MMAs apart, hiding the DMMA latency
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-          double br[NQ], bim[NQ], bneg[NQ];
+        for (int np = 0; np < 2; ++np) {
+          double br[2][NQ], bim[2][NQ], bneg[2][NQ];
 #pragma unroll
-          for (int q = 0; q < NQ; ++q) {
-            const double2 v = sm.b[st][32 * wj + 8 * nt + g][ks * KI + t + 4 * q];
-            br[q] = wq[q] * v.x;
-            bim[q] = wq[q] * v.y;
-            bneg[q] = -bim[q];
-          }
-          dmma<KI>(accR[mt][nt], ar, br);
-          dmma<KI>(accR[mt][nt], ai, bim);
-          dmma<KI>(accI[mt][nt], ai, br);
-          dmma<KI>(accI[mt][nt], ar, bneg);
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+              const double2 v = sm.b[st][32 * wj + 8 * (2 * np + h) + g][ks * KI + t + 4 * q];
+              br[h][q] = wq[q] * v.x;
+              bim[h][q] = wq[q] * v.y;
+              bneg[h][q] = -bim[h][q];
+            }
+          dmma<KI>(accR[mt][2 * np], ar, br[0]);
+          dmma<KI>(accR[mt][2 * np + 1], ar, br[1]);
+          dmma<KI>(accI[mt][2 * np], ai, br[0]);
+          dmma<KI>(accI[mt][2 * np + 1], ai, br[1]);
+          dmma<KI>(accR[mt][2 * np], ai, bim[0]);
+          dmma<KI>(accR[mt][2 * np + 1], ai, bim[1]);
+          dmma<KI>(accI[mt][2 * np], ar, bneg[0]);
+          dmma<KI>(accI[mt][2 * np + 1], ar, bneg[1]);
         }
       }
     }

@@ -152,8 +152,8 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
             break;
           }
           mbar_arrive_expect_tx(&sm.full[st], (uint32_t)((SP_SA + SP_SB) * SP_PLANE));
-          tma_load_3d(&sm.a[st][0][0], &mapA, ks * SP_KB, bi * SP_ROWS, 0, &sm.full[st]);
-          tma_load_3d(&sm.b[st][0][0], &mapB, ks * SP_KB, bj * SP_ROWS, f * SP_SB, &sm.full[st]);
+          tma_load_4d(&sm.a[st][0][0], &mapA, 0, bi * SP_ROWS, ks, 0, &sm.full[st]);
+          tma_load_4d(&sm.b[st][0][0], &mapB, 0, bj * SP_ROWS, ks, f * SP_SB, &sm.full[st]);
           issued[st] = true;
           last_ph[st] = ph;
           if (++st == SP_ST) st = 0, ph ^= 1u;
@@ -256,8 +256,10 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
           const long long partner = sm.xchg[is_re ? 1 : 0][ii][k];
           const long long v = is_re ? tre[k] + partner : tre[k] - partner;
           if (gi <= gj && gj < prm.N) {
+            // one add per element per launch: launches are ordered, so the sum is
+            // deterministic, and the reduction needs no read round trip
             double* o = outf + 2 * ((int64_t)gj * (gj + 1) / 2 + gi) + (is_re ? 0 : 1);
-            *o += fac * prm.sA[gj] * (double)v;
+            atomicAdd(o, fac * prm.sA[gj] * (double)v);
           }
         }
         __syncwarp();
@@ -318,34 +320,67 @@ __global__ void split_wmax_kernel(const double* __restrict__ W, int64_t ldw, int
   }
 }
 
-// Balanced base-256 digits of the integer Y = sum_t d_t 256^(S-1-t): low bytes
-// sign-extended, the rest carried up; |Y| <= 127 * 256^(S-1) keeps |d0| <= 127.
-template <int S>
-__device__ __forceinline__ void digits(int Y, int (&d)[S]) {
-#pragma unroll
-  for (int t = S - 1; t > 0; --t) {
-    const int lo = (int)(int8_t)(Y & 0xff);
-    d[t] = lo;
-    Y = (Y - lo) >> 8;
-  }
-  d[0] = Y;
+// Round-to-nearest integer of a*b (|a*b| < 2^31) through the FP64 magic constant
+// 1.5*2^52: one fused multiply-add, the low word of the sum is the integer.
+__device__ __forceinline__ uint32_t round_mul(double a, double b) {
+  return (uint32_t)__double2loint(__fma_rn(a, b, 6755399441055744.0));
 }
 
-// One thread = one complex column i and 16 consecutive pairs of the slab. Writes
-// 16-byte runs of every digit plane: A planes [t][row][p], B planes [f][u][row][p],
-// rows real-stacked (block b of 64 columns -> rows 128 b + {0..63 Re, 64..127 Im}).
-__global__ void split_quantize_kernel(const double2* __restrict__ M, int64_t ldc, int64_t p0,
-                                      int len, int nchunk, int N, int npad, int64_t R, int64_t Ps,
-                                      const double* __restrict__ W, int64_t ldw, int nw,
-                                      const double* __restrict__ sA,
-                                      const double* __restrict__ wmax, int8_t* __restrict__ A,
-                                      int8_t* __restrict__ B) {
+// Four values Y (two's complement words) -> their balanced base-256 digit planes.
+// With U = Y + 0x808080, bytes 0..2 of U are the lower digits plus 128 and byte 3
+// is the top digit (|top| <= 127 because |Y| <= 127 * 2^24). out[t] holds digit t
+// (t = 0 most significant) of the four values, one per byte.
+template <int S>
+__device__ __forceinline__ void digit_planes(const uint32_t (&Y)[4], uint32_t (&out)[S]) {
+  const uint32_t bias = S == 4 ? 0x00808080u : 0x00008080u;
+  const uint32_t u0 = Y[0] + bias, u1 = Y[1] + bias, u2 = Y[2] + bias, u3 = Y[3] + bias;
+  const uint32_t lo01 = __byte_perm(u0, u1, 0x5140), lo23 = __byte_perm(u2, u3, 0x5140);
+  const uint32_t hi01 = __byte_perm(u0, u1, 0x7362), hi23 = __byte_perm(u2, u3, 0x7362);
+  const uint32_t b0 = __byte_perm(lo01, lo23, 0x5410) ^ 0x80808080u;  // byte 0 of each
+  const uint32_t b1 = __byte_perm(lo01, lo23, 0x7632) ^ 0x80808080u;  // byte 1
+  const uint32_t b2 = __byte_perm(hi01, hi23, 0x5410);                // byte 2
+  if constexpr (S == 4) {
+    out[0] = __byte_perm(hi01, hi23, 0x7632);  // byte 3: top digit
+    out[1] = b2 ^ 0x80808080u;
+    out[2] = b1;
+    out[3] = b0;
+  } else {
+    out[0] = b2;  // byte 2: top digit of a 3-digit value
+    out[1] = b1;
+    out[2] = b0;
+  }
+}
+
+// One thread = one complex column i and 16 consecutive pairs of the slab. Digit
+// planes are stored [plane][k-block of 32 pairs][row][32 bytes]; a warp holds 16
+// consecutive columns x the two halves of one k-block, so every store instruction
+// writes 16 adjacent rows x 32 bytes = 512 contiguous bytes, and the TMA box
+// (32 B, 128 rows, 1 k-block, planes) lands as [plane][row][32 B] in shared memory.
+// Rows are real-stacked: block b of 64 columns -> rows 128 b + {0..63 Re, 64..127 Im}.
+__global__ void __launch_bounds__(128)
+    split_quantize_kernel(const double2* __restrict__ M, int64_t ldc, int64_t p0, int len,
+                          int nchunk, int N, int npad, int64_t R, int64_t Ps,
+                          const double* __restrict__ W, int64_t ldw, int nw,
+                          const double* __restrict__ sA, const double* __restrict__ wmax,
+                          int8_t* __restrict__ A, int8_t* __restrict__ B) {
   const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (tid >= (int64_t)npad * nchunk) return;
-  const int i = (int)(tid / nchunk);
-  const int p = (int)(tid % nchunk) * 16;
+  // tid -> (k-block, column group of 16, half of the k-block, column in group)
+  const int ngroup = npad / 16;
+  const int lane16 = (int)(tid & 15), half = (int)((tid >> 4) & 1);
+  const int64_t rest = tid >> 5;
+  const int i = (int)(rest % ngroup) * 16 + lane16;
+  const int64_t kb = rest / ngroup;
+  const int p = (int)(kb * SP_KB) + half * 16;
   const int64_t r_re = (int64_t)(i / SP_TILE) * SP_ROWS + (i % SP_TILE);
   const int64_t r_im = r_re + SP_TILE;
+  const int64_t nkb = Ps / SP_KB;
+  // byte offsets of (plane 0, k-block, row) for this thread's 16 pairs; planes are
+  // nkb * R * 32 bytes apart
+  const int64_t pstride = nkb * R * SP_KB;
+  const int64_t a_re = (kb * R + r_re) * SP_KB + half * 16;
+  const int64_t a_im = (kb * R + r_im) * SP_KB + half * 16;
+  const int64_t b_re = a_re, b_im = a_im;
   double xr[16], xi[16];
   const bool col_ok = i < N;
 #pragma unroll
@@ -356,62 +391,59 @@ __global__ void split_quantize_kernel(const double2* __restrict__ M, int64_t ldc
     xi[k] = v.y;
   }
   const double s = col_ok ? sA[i] : 0.0;
-  const double inv = s > 0.0 ? 127.0 * 65536.0 / s : 0.0;  // 3 digits: scale 2^16
-  // unweighted operand: 3 slices
+  // unweighted operand: 3 digits of round(x * 127/s * 2^16)
   {
-    uint32_t pr[SP_SA][4], pi[SP_SA][4];
+    const double inv = s > 0.0 ? 127.0 * 65536.0 / s : 0.0;
+    uint32_t wr[SP_SA][4], wi[SP_SA][4];
 #pragma unroll
-    for (int t = 0; t < SP_SA; ++t)
+    for (int q = 0; q < 4; ++q) {
+      uint32_t yr[4], yi[4], pr[SP_SA], pi[SP_SA];
 #pragma unroll
-      for (int w = 0; w < 4; ++w) pr[t][w] = pi[t][w] = 0u;
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      int dr[SP_SA], di[SP_SA];
-      digits<SP_SA>(__double2int_rn(xr[k] * inv), dr);
-      digits<SP_SA>(__double2int_rn(xi[k] * inv), di);
-#pragma unroll
-      for (int t = 0; t < SP_SA; ++t) {
-        pr[t][k >> 2] |= ((uint32_t)dr[t] & 0xffu) << (8 * (k & 3));
-        pi[t][k >> 2] |= ((uint32_t)di[t] & 0xffu) << (8 * (k & 3));
+      for (int k = 0; k < 4; ++k) {
+        yr[k] = round_mul(xr[4 * q + k], inv);
+        yi[k] = round_mul(xi[4 * q + k], inv);
       }
+      digit_planes<SP_SA>(yr, pr);
+      digit_planes<SP_SA>(yi, pi);
+#pragma unroll
+      for (int t = 0; t < SP_SA; ++t) wr[t][q] = pr[t], wi[t][q] = pi[t];
     }
 #pragma unroll
     for (int t = 0; t < SP_SA; ++t) {
-      *reinterpret_cast<uint4*>(A + (t * R + r_re) * Ps + p) =
-          make_uint4(pr[t][0], pr[t][1], pr[t][2], pr[t][3]);
-      *reinterpret_cast<uint4*>(A + (t * R + r_im) * Ps + p) =
-          make_uint4(pi[t][0], pi[t][1], pi[t][2], pi[t][3]);
+      *reinterpret_cast<uint4*>(A + a_re + t * pstride) =
+          make_uint4(wr[t][0], wr[t][1], wr[t][2], wr[t][3]);
+      *reinterpret_cast<uint4*>(A + a_im + t * pstride) =
+          make_uint4(wi[t][0], wi[t][1], wi[t][2], wi[t][3]);
     }
   }
-  // weighted operand, one frequency at a time: 4 slices
+  // weighted operand, one frequency at a time: 4 digits of round(x w 127/(wmax s) 2^24)
   for (int f = 0; f < nw; ++f) {
     const double wm = wmax[f];
-    const double g = (s > 0.0 && wm > 0.0) ? 127.0 * 16777216.0 / (wm * s) : 0.0;  // 4 digits: 2^24
+    const double g = (s > 0.0 && wm > 0.0) ? 127.0 * 16777216.0 / (wm * s) : 0.0;
     const double* wf = W + (int64_t)f * ldw + p0 + p;
-    uint32_t pr[SP_SB][4], pi[SP_SB][4];
+    uint32_t wr[SP_SB][4], wi[SP_SB][4];
 #pragma unroll
-    for (int u = 0; u < SP_SB; ++u)
+    for (int q = 0; q < 4; ++q) {
+      uint32_t yr[4], yi[4], pr[SP_SB], pi[SP_SB];
 #pragma unroll
-      for (int w = 0; w < 4; ++w) pr[u][w] = pi[u][w] = 0u;
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      const double wk = (p + k < len) ? wf[k] * g : 0.0;
-      int dr[SP_SB], di[SP_SB];
-      digits<SP_SB>(__double2int_rn(xr[k] * wk), dr);
-      digits<SP_SB>(__double2int_rn(xi[k] * wk), di);
-#pragma unroll
-      for (int u = 0; u < SP_SB; ++u) {
-        pr[u][k >> 2] |= ((uint32_t)dr[u] & 0xffu) << (8 * (k & 3));
-        pi[u][k >> 2] |= ((uint32_t)di[u] & 0xffu) << (8 * (k & 3));
+      for (int k = 0; k < 4; ++k) {
+        const int kk = 4 * q + k;
+        const double wk = (p + kk < len) ? wf[kk] * g : 0.0;
+        yr[k] = round_mul(xr[kk], wk);
+        yi[k] = round_mul(xi[kk], wk);
       }
+      digit_planes<SP_SB>(yr, pr);
+      digit_planes<SP_SB>(yi, pi);
+#pragma unroll
+      for (int u = 0; u < SP_SB; ++u) wr[u][q] = pr[u], wi[u][q] = pi[u];
     }
 #pragma unroll
     for (int u = 0; u < SP_SB; ++u) {
       const int64_t plane = (int64_t)f * SP_SB + u;
-      *reinterpret_cast<uint4*>(B + (plane * R + r_re) * Ps + p) =
-          make_uint4(pr[u][0], pr[u][1], pr[u][2], pr[u][3]);
-      *reinterpret_cast<uint4*>(B + (plane * R + r_im) * Ps + p) =
-          make_uint4(pi[u][0], pi[u][1], pi[u][2], pi[u][3]);
+      *reinterpret_cast<uint4*>(B + b_re + plane * pstride) =
+          make_uint4(wr[u][0], wr[u][1], wr[u][2], wr[u][3]);
+      *reinterpret_cast<uint4*>(B + b_im + plane * pstride) =
+          make_uint4(wi[u][0], wi[u][1], wi[u][2], wi[u][3]);
     }
   }
 }
@@ -454,6 +486,22 @@ int make_tmap_u8_3d(spx_ctx* ctx, CUtensorMap* map, const void* base, uint64_t d
   return SPX_OK;
 }
 
+int make_tmap_u8_4d(spx_ctx* ctx, CUtensorMap* map, const void* base, const uint64_t dims[4],
+                    const uint64_t strides[3], const uint32_t box[4], CUtensorMapSwizzle swz) {
+  auto enc = get_encode();
+  if (!enc) return set_error(ctx, SPX_ECUDA, "cuTensorMapEncodeTiled unavailable");
+  cuuint64_t d[4] = {dims[0], dims[1], dims[2], dims[3]};
+  cuuint64_t st[3] = {strides[0], strides[1], strides[2]};
+  cuuint32_t b[4] = {box[0], box[1], box[2], box[3]};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<void*>(base), d, st, b, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return set_error(ctx, SPX_ECUDA, "cuTensorMapEncodeTiled (4-D) failed: " + std::to_string((int)r));
+  return SPX_OK;
+}
+
 struct SplitLayout {
   int64_t Ps, R;
   int nblk;
@@ -492,13 +540,25 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
   double* sA = (double*)(base + L.a_bytes + L.b_bytes);
   double* wmax = (double*)(base + L.a_bytes + L.b_bytes + L.s_bytes);
 
+  // planes in HBM: [plane][k-block][row][32 B]; TMA dims (32 B, row, k-block, plane)
+  // with increasing strides; a box (32, 128, 1, planes) lands as [plane][row][32 B]
   CUtensorMap mapA, mapB;
-  int rc = make_tmap_u8_3d(ctx, &mapA, A, L.Ps, L.R, SP_SA, L.Ps, L.R * L.Ps, SP_KB, SP_ROWS, SP_SA,
-                           CU_TENSOR_MAP_SWIZZLE_32B);
-  if (rc) return rc;
-  rc = make_tmap_u8_3d(ctx, &mapB, B, L.Ps, L.R, (uint64_t)SP_SB * nw, L.Ps, L.R * L.Ps, SP_KB,
-                       SP_ROWS, SP_SB, CU_TENSOR_MAP_SWIZZLE_32B);
-  if (rc) return rc;
+  const uint64_t nkb = (uint64_t)(L.Ps / SP_KB);
+  {
+    const uint64_t dims[4] = {SP_KB, (uint64_t)L.R, nkb, SP_SA};
+    const uint64_t strides[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};
+    const uint32_t box[4] = {SP_KB, SP_ROWS, 1, SP_SA};
+    int rc = make_tmap_u8_4d(ctx, &mapA, A, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_32B);
+    if (rc) return rc;
+  }
+  {
+    const uint64_t dims[4] = {SP_KB, (uint64_t)L.R, nkb, (uint64_t)SP_SB * nw};
+    const uint64_t strides[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};
+    const uint32_t box[4] = {SP_KB, SP_ROWS, 1, SP_SB};
+    int rc = make_tmap_u8_4d(ctx, &mapB, B, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_32B);
+    if (rc) return rc;
+  }
+  int rc = SPX_OK;
 
   const size_t smem = sizeof(SplitSmem) + 1024;
   static bool attr_set = false;
@@ -514,12 +574,12 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
   for (int64_t p0 = 0; p0 < P; p0 += L.Ps) {
     const int len = (int)std::min<int64_t>(L.Ps, P - p0);
     const int lenp = (int)align_up((size_t)len, SP_KB);
-    const int nchunk = lenp / 16;
+    const int nchunk = lenp / 16;  // 16-pair chunks; npad is a multiple of 64
     timing_mark(ctx, stream, 0);
     split_colmax_kernel<<<N, 256, 0, stream>>>(M, ldc, p0, len, sA);
     split_wmax_kernel<<<nw, 256, 0, stream>>>(W, ldw, p0, len, wmax);
     const int64_t nthr = (int64_t)npad * nchunk;
-    split_quantize_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, stream>>>(
+    split_quantize_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, stream>>>(
         M, ldc, p0, len, nchunk, N, npad, L.R, L.Ps, W, ldw, nw, sA, wmax, A, B);
     rc = check_cuda(ctx, cudaGetLastError(), "split operand preparation");
     if (rc) return rc;

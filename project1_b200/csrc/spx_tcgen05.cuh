@@ -102,6 +102,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
       : "memory");
 }
+// 4-D tiled TMA load into shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            int w, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z), "r"(w)
+      : "memory");
+}
 __device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
@@ -112,5 +121,9 @@ __device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
 int make_tmap_u8_3d(spx_ctx* ctx, CUtensorMap* map, const void* base, uint64_t d0, uint64_t d1,
                     uint64_t d2, uint64_t s1, uint64_t s2, uint32_t b0, uint32_t b1, uint32_t b2,
                     CUtensorMapSwizzle swz);
+// Host: 4-D uint8 tiled tensor map; dims[0] is contiguous, strides[] are the byte
+// strides of dims 1..3 (any order in memory).
+int make_tmap_u8_4d(spx_ctx* ctx, CUtensorMap* map, const void* base, const uint64_t dims[4],
+                    const uint64_t strides[3], const uint32_t box[4], CUtensorMapSwizzle swz);
 
 }  // namespace spx
