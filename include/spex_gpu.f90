@@ -17,12 +17,14 @@ module spex_gpu
   integer(c_int), parameter :: SPX_FP64 = 0, SPX_SPLIT = 1
 
   type, bind(c) :: spx_options
-    integer(c_int32_t) :: struct_size = 32
+    integer(c_int32_t) :: struct_size = 40
     integer(c_int32_t) :: verbose = 0
     integer(c_int64_t) :: workspace_limit = 0
     integer(c_int64_t) :: pinned_limit = 0
     integer(c_int32_t) :: chunk_pairs = 0
     integer(c_int32_t) :: timeout_ms = 0
+    integer(c_int32_t) :: split_variant = 0
+    integer(c_int32_t) :: reserved = 0
   end type
 
   type, bind(c) :: spx_chi0_stats

@@ -57,6 +57,9 @@ typedef struct spx_options {
   int64_t pinned_limit;     /* pinned host staging bytes, 0 = auto               */
   int32_t chunk_pairs;      /* band pairs per streamed chunk, 0 = auto           */
   int32_t timeout_ms;       /* bound on every device-side wait, 0 = 4000 ms      */
+  int32_t split_variant;    /* split-path kernel: 0 auto, 1 one CTA per tile,
+                               2 CTA pair (tcgen05 cta_group::2)                 */
+  int32_t reserved;
 } spx_options;
 
 /* Per-call statistics filled by the accumulation entry points (may be NULL). */

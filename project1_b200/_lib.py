@@ -29,6 +29,8 @@ class spx_options(C.Structure):
         ("pinned_limit", C.c_int64),
         ("chunk_pairs", C.c_int32),
         ("timeout_ms", C.c_int32),
+        ("split_variant", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

@@ -279,6 +279,234 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
 }
 
 // ---------------------------------------------------------------------------
+// CTA-pair form: one tcgen05.mma.cta_group::2 (M = 256) covers two 64 x 64 complex
+// tiles stacked in i. Each CTA of the cluster stages its own A tile (128 rows) and
+// half of the shared B tile (64 rows: CTA 0 the Re rows, CTA 1 the Im rows of the
+// 64 columns j); the leader CTA issues the MMAs, which read both CTAs' shared
+// memory and write each CTA's own TMEM. Per SM and stage this moves 20 KB instead
+// of 28 KB from L2 for the same tensor work. Every completion that crosses the
+// pair is an explicit remote arrive or commit (no multicast).
+
+constexpr int SP2_ST = 8;
+constexpr int SP2_BROWS = SP_ROWS / 2;          // B rows staged per CTA
+constexpr int SP2_BPLANE = SP2_BROWS * SP_KB;   // 2048 bytes
+constexpr uint32_t SP2_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(SP_ROWS / 8) << 17) |
+                               ((uint32_t)(2 * SP_ROWS / 16) << 24);   // M = 256, N = 128
+
+struct __align__(1024) Split2Smem {
+  uint8_t a[SP2_ST][SP_SA][SP_PLANE];
+  uint8_t b[SP2_ST][SP_SB][SP2_BPLANE];
+  long long xchg[2][SP_TILE][33];
+  uint64_t full[SP2_ST];   // leader: both CTAs' bytes of a stage have landed
+  uint64_t empty[SP2_ST];  // each CTA: the MMAs have read the stage
+  uint64_t tfull;          // each CTA: accumulators ready
+  uint64_t tempty;         // leader: both CTAs' epilogues have drained TMEM (8 warps)
+  uint64_t xfull, xfree, mdone;
+  uint32_t tmem_base;
+};
+
+// Pair tile t -> (bI, bJ): i-blocks of 128 (two 64-blocks), j-blocks of 64, with
+// 2 bI <= bJ; column-major over bJ.
+__device__ __forceinline__ void pair_decode_tile(int t, int* bI, int* bJ) {
+  int j = 0, c = 0;
+  while (c + j / 2 + 1 <= t) {
+    c += j / 2 + 1;
+    ++j;
+  }
+  *bJ = j;
+  *bI = t - c;
+}
+
+__global__ void __launch_bounds__(SP_THREADS, 1)
+    split_gram2_kernel(const __grid_constant__ CUtensorMap mapA,
+                       const __grid_constant__ CUtensorMap mapB, SplitParams prm) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  Split2Smem& sm = *reinterpret_cast<Split2Smem*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const int cid = (int)cluster_id_x(), ncl = (int)nclusters_x();
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < SP2_ST; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], 1);
+    }
+    mbar_init(&sm.tfull, 1);
+    mbar_init(&sm.tempty, 8);
+    mbar_init(&sm.xfull, 4);
+    mbar_init(&sm.xfree, 4);
+    mbar_init(&sm.mdone, 1);
+    fence_barrier_init();
+  }
+  if (warp == 1) tmem_alloc2(&sm.tmem_base, SP_TMEM_COLS);
+  tc_fence_before();
+  cluster_sync();  // both CTAs' barriers initialised and TMEM allocated
+  tc_fence_after();
+  const uint32_t tmem = sm.tmem_base;
+
+  if (warp == 0) {
+    // ---------------- TMA producer (both CTAs) ----------------
+    if (lane == 0) {
+      int st = 0;
+      uint32_t ph = 0;
+      bool issued[SP2_ST];
+      uint32_t last_ph[SP2_ST];
+      for (int q = 0; q < SP2_ST; ++q) issued[q] = false, last_ph[q] = 0;
+      bool ok = true;
+      for (int item = cid; item < prm.nitems && ok; item += ncl) {
+        const int f = item / prm.ntile;
+        int bI, bJ;
+        pair_decode_tile(item % prm.ntile, &bI, &bJ);
+        for (int ks = 0; ks < prm.nk; ++ks) {
+          if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) {
+            ok = false;
+            break;
+          }
+          const uint32_t lead_full = mapa_shared(smem_u32(&sm.full[st]), 0);
+          if (rank == 0)
+            mbar_arrive_expect_tx(&sm.full[st],
+                                  (uint32_t)(2 * (SP_SA * SP_PLANE + SP_SB * SP2_BPLANE)));
+          tma_load_4d_pair(&sm.a[st][0][0], &mapA, 0, (2 * bI + (int)rank) * SP_ROWS, ks, 0,
+                           lead_full);
+          tma_load_4d_pair(&sm.b[st][0][0], &mapB, 0, bJ * SP_ROWS + (int)rank * SP2_BROWS, ks,
+                           f * SP_SB, lead_full);
+          issued[st] = true;
+          last_ph[st] = ph;
+          if (++st == SP2_ST) st = 0, ph ^= 1u;
+        }
+      }
+      if (rank == 0) {
+        // the leader's stage barriers count both CTAs' bytes
+        for (int q = 0; q < SP2_ST; ++q)
+          if (issued[q]) mbar_drain(&sm.full[q], last_ph[q], prm.timeout_ns);
+      } else {
+        // the peer cannot poll the leader's barrier: give its last copies a bounded
+        // grace period to land (they complete in microseconds)
+        const uint64_t t0 = global_ns();
+        while (global_ns() - t0 < 200000ull) {
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer (leader CTA only) ----------------
+    if (rank == 0 && lane == 0) {
+      int st = 0;
+      uint32_t ph = 0;
+      int j = 0;
+      bool committed = false;
+      const uint32_t peer_tfull = mapa_shared(smem_u32(&sm.tfull), 1);
+      for (int item = cid; item < prm.nitems; item += ncl, ++j) {
+        if (!mbar_wait(&sm.tempty, (uint32_t)(j & 1) ^ 1u, prm.timeout_ns, prm.status)) break;
+        tc_fence_after();
+        bool ok = true;
+        for (int ks = 0; ks < prm.nk; ++ks) {
+          if (!mbar_wait(&sm.full[st], ph, prm.timeout_ns, prm.status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          uint64_t da[SP_SA], db[SP_SB];
+#pragma unroll
+          for (int t = 0; t < SP_SA; ++t) da[t] = desc_sw32(&sm.a[st][t][0]);
+#pragma unroll
+          for (int u = 0; u < SP_SB; ++u) db[u] = desc_sw32(&sm.b[st][u][0]);
+          const uint32_t k0 = ks > 0;
+          mma2_i8<1>(tmem + 0 * 128, da[0], db[0], SP2_IDESC, k0);
+          mma2_i8<2>(tmem + 1 * 128, da[0], db[1], SP2_IDESC, k0);
+          mma2_i8<2>(tmem + 2 * 128, da[0], db[2], SP2_IDESC, k0);
+          mma2_i8<3>(tmem + 3 * 128, da[0], db[3], SP2_IDESC, k0);
+          mma2_i8<1>(tmem + 1 * 128, da[1], db[0], SP2_IDESC, 1u);
+          mma2_i8<2>(tmem + 2 * 128, da[1], db[1], SP2_IDESC, 1u);
+          mma2_i8<3>(tmem + 3 * 128, da[1], db[2], SP2_IDESC, 1u);
+          mma2_i8<1>(tmem + 2 * 128, da[2], db[0], SP2_IDESC, 1u);
+          mma2_i8<3>(tmem + 3 * 128, da[2], db[1], SP2_IDESC, 1u);
+          // the stage is free in both CTAs once these MMAs have read it
+          tc_commit2(smem_u32(&sm.empty[st]));
+          tc_commit2(mapa_shared(smem_u32(&sm.empty[st]), 1));
+          committed = true;
+          if (++st == SP2_ST) st = 0, ph ^= 1u;
+        }
+        if (!ok) break;
+        tc_commit2(smem_u32(&sm.tfull));
+        tc_commit2(peer_tfull);
+      }
+      if (committed) {
+        tc_commit2(smem_u32(&sm.mdone));
+        mbar_drain(&sm.mdone, 0u, prm.timeout_ns);
+      }
+    }
+  } else {
+    // ---------------- epilogue (both CTAs): this CTA's 64 x 64 tile ----------------
+    const int q = warp & 3;
+    const bool is_re = q < 2;
+    const int ii = (q & 1) * 32 + lane;
+    const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16);
+    const uint32_t lead_tempty = mapa_shared(smem_u32(&sm.tempty), 0);
+    int j = 0;
+    uint32_t xseq = 0;
+    for (int item = cid; item < prm.nitems; item += ncl, ++j) {
+      if (!mbar_wait(&sm.tfull, (uint32_t)(j & 1), prm.timeout_ns, prm.status)) break;
+      tc_fence_after();
+      const int f = item / prm.ntile;
+      int bI, bJ;
+      pair_decode_tile(item % prm.ntile, &bI, &bJ);
+      const int bi = 2 * bI + (int)rank;
+      bool ok = true;
+      // a tile wholly below the diagonal or past N has nothing to store
+      if (bi <= bJ && bi * SP_TILE < prm.N) {
+        const int gi = bi * SP_TILE + ii;
+        const double si = gi < prm.N ? prm.sA[gi] : 0.0;
+        const double fac = si * prm.wmax[f] * (1.0 / (127.0 * 127.0 * 16777216.0));
+        double* outf = prm.out + 2 * (int64_t)f * prm.npack;
+        for (int js = 0; js < 2 && ok; ++js, ++xseq) {
+          long long tre[32], tim[32];
+          load_orders(tl + (uint32_t)(js * 32), tre);
+          load_orders(tl + (uint32_t)(64 + js * 32), tim);
+          if (!mbar_wait(&sm.xfree, (xseq & 1u) ^ 1u, prm.timeout_ns, prm.status)) {
+            ok = false;
+            break;
+          }
+#pragma unroll
+          for (int k = 0; k < 32; ++k) sm.xchg[is_re ? 0 : 1][ii][k] = tim[k];
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&sm.xfull);
+          if (!mbar_wait(&sm.xfull, xseq & 1u, prm.timeout_ns, prm.status)) {
+            ok = false;
+            break;
+          }
+#pragma unroll
+          for (int k = 0; k < 32; ++k) {
+            const int gj = bJ * SP_TILE + js * 32 + k;
+            const long long partner = sm.xchg[is_re ? 1 : 0][ii][k];
+            const long long v = is_re ? tre[k] + partner : tre[k] - partner;
+            if (gi <= gj && gj < prm.N) {
+              double* o = outf + 2 * ((int64_t)gj * (gj + 1) / 2 + gi) + (is_re ? 0 : 1);
+              atomicAdd(o, fac * prm.sA[gj] * (double)v);
+            }
+          }
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&sm.xfree);
+        }
+      }
+      if (!ok) break;
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        if (rank == 0) mbar_arrive(&sm.tempty);
+        else mbar_arrive_cluster(lead_tempty);
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // neither CTA leaves while the pair's MMAs may read its shared memory
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc2(tmem, SP_TMEM_COLS);
+}
+
+// ---------------------------------------------------------------------------
 // operand preparation
 
 // Column scales of one slab: sA[i] = max_p max(|Re M(p,i)|, |Im M(p,i)|).
@@ -512,7 +740,8 @@ static SplitLayout split_layout(int64_t P, int N, int nw) {
   SplitLayout L;
   L.Ps = std::min<int64_t>((int64_t)align_up((size_t)std::max<int64_t>(P, 1), SP_KB), SP_SLAB);
   L.nblk = (N + SP_TILE - 1) / SP_TILE;
-  L.R = (int64_t)L.nblk * SP_ROWS;
+  // an even number of 64-blocks, so a CTA pair's second A tile always exists
+  L.R = (int64_t)((L.nblk + 1) / 2 * 2) * SP_ROWS;
   L.a_bytes = align_up((size_t)SP_SA * L.R * L.Ps, 1024);
   L.b_bytes = align_up((size_t)SP_SB * nw * L.R * L.Ps, 1024);
   L.s_bytes = align_up(sizeof(double) * (size_t)std::max(N, 1), 256);
@@ -560,16 +789,53 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
   }
   int rc = SPX_OK;
 
+  const bool pair = ctx->opt.split_variant != 1;  // 0 (auto) and 2 select the CTA pair
+  CUtensorMap mapB2;
+  if (pair) {
+    const uint64_t dims[4] = {SP_KB, (uint64_t)L.R, nkb, (uint64_t)SP_SB * nw};
+    const uint64_t strides[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};
+    const uint32_t box[4] = {SP_KB, SP2_BROWS, 1, SP_SB};
+    int rc2 = make_tmap_u8_4d(ctx, &mapB2, B, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_32B);
+    if (rc2) return rc2;
+  }
   const size_t smem = sizeof(SplitSmem) + 1024;
+  const size_t smem2 = sizeof(Split2Smem) + 1024;
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(split_gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(split_gram2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem2);
     attr_set = true;
   }
   const int ntile = L.nblk * (L.nblk + 1) / 2;
-  const int nitems = ntile * nw;
+  int ntile2 = 0;
+  for (int bj = 0; bj < L.nblk; ++bj) ntile2 += bj / 2 + 1;
+  const int nitems = (pair ? ntile2 : ntile) * nw;
   const int grid = std::min(nitems, ctx->num_sms);
-  const int npad = L.nblk * SP_TILE;
+  const int npad = (int)(L.R / 2);  // columns covered by the stacked rows
+  // CTA-pair launch: as many clusters as can be resident at once (persistent)
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute cattr[1];
+  int nclusters = 0;
+  if (pair) {
+    cattr[0].id = cudaLaunchAttributeClusterDimension;
+    cattr[0].val.clusterDim.x = 2;
+    cattr[0].val.clusterDim.y = 1;
+    cattr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(SP_THREADS);
+    cfg.dynamicSmemBytes = smem2;
+    cfg.stream = stream;
+    cfg.attrs = cattr;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(2 * (ctx->num_sms / 2));
+    int maxc = 0;
+    rc = check_cuda(ctx, cudaOccupancyMaxActiveClusters(&maxc, split_gram2_kernel, &cfg),
+                    "cudaOccupancyMaxActiveClusters");
+    if (rc) return rc;
+    if (maxc <= 0) return set_error(ctx, SPX_ENOTSUP, "no CTA-pair cluster fits on this device");
+    nclusters = std::min(nitems, maxc);
+    cfg.gridDim = dim3(2 * nclusters);
+  }
 
   for (int64_t p0 = 0; p0 < P; p0 += L.Ps) {
     const int len = (int)std::min<int64_t>(L.Ps, P - p0);
@@ -586,7 +852,7 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
     timing_mark(ctx, stream, 1);
     SplitParams prm;
     prm.N = N;
-    prm.ntile = ntile;
+    prm.ntile = pair ? ntile2 : ntile;
     prm.nw = nw;
     prm.nitems = nitems;
     prm.nk = lenp / SP_KB;
@@ -597,8 +863,13 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
     prm.status = ctx->d_status;
     prm.timeout_ns =
         (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
-    split_gram_kernel<<<grid, SP_THREADS, smem, stream>>>(mapA, mapB, prm);
-    rc = check_cuda(ctx, cudaGetLastError(), "split_gram_kernel launch");
+    if (pair) {
+      rc = check_cuda(ctx, cudaLaunchKernelEx(&cfg, split_gram2_kernel, mapA, mapB2, prm),
+                      "split_gram2_kernel launch");
+    } else {
+      split_gram_kernel<<<grid, SP_THREADS, smem, stream>>>(mapA, mapB, prm);
+      rc = check_cuda(ctx, cudaGetLastError(), "split_gram_kernel launch");
+    }
     if (rc) return rc;
     *launches += 4;
   }

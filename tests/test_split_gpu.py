@@ -93,3 +93,18 @@ def test_split_accumulates(ctx):
     ref = oracle.chi0(m, oracle.weights(d, om), accurate=True, susceph=init.copy(order="F"))
     got = run_dev(ctx, m, d, om, init=init, precision="split")
     assert np.max(np.abs(got - ref)) <= 1e-6 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("nbas,npair,nw", [(65, 3000, 2), (200, 40000, 3), (130, 33, 1)])
+def test_split_cta_pair_equals_single_cta(nbas, npair, nw):
+    """The CTA-pair kernel (cta_group::2) and the one-CTA kernel sum the same exact
+    integers and add one FP64 term per element per launch: results are identical."""
+    m, d, om = random_case(nbas, npair, nw, seed=nbas + 3 * npair, degfrac=0.01)
+    outs = []
+    for variant in (1, 2):
+        with spx.Context(0, split_variant=variant) as c:
+            outs.append(run_dev(c, m, d, om, None, 0.5, precision="split"))
+    assert np.array_equal(outs[0], outs[1])
+    ref = oracle.chi0(m, oracle.weights(d, om, None, 0.5), accurate=True)
+    emax, fro = normalized_error(outs[1], ref, nbas)
+    assert emax <= SPLIT_TOL and fro <= SPLIT_FRO, (emax, fro)
