@@ -287,7 +287,8 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
 // of 28 KB from L2 for the same tensor work. Every completion that crosses the
 // pair is an explicit remote arrive or commit (no multicast).
 
-constexpr int SP2_ST = 8;
+constexpr int SP2_ST = 9;
+constexpr int SP2_XC = 16;                      // columns per epilogue exchange
 constexpr int SP2_BROWS = SP_ROWS / 2;          // B rows staged per CTA
 constexpr int SP2_BPLANE = SP2_BROWS * SP_KB;   // 2048 bytes
 constexpr uint32_t SP2_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(SP_ROWS / 8) << 17) |
@@ -296,7 +297,7 @@ constexpr uint32_t SP2_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(
 struct __align__(1024) Split2Smem {
   uint8_t a[SP2_ST][SP_SA][SP_PLANE];
   uint8_t b[SP2_ST][SP_SB][SP2_BPLANE];
-  long long xchg[2][SP_TILE][33];
+  long long xchg[2][SP_TILE][SP2_XC + 1];
   uint64_t full[SP2_ST];   // leader: both CTAs' bytes of a stage have landed
   uint64_t empty[SP2_ST];  // each CTA: the MMAs have read the stage
   uint64_t tfull;          // each CTA: accumulators ready
@@ -315,6 +316,22 @@ __device__ __forceinline__ void pair_decode_tile(int t, int* bI, int* bJ) {
   }
   *bJ = j;
   *bI = t - c;
+}
+
+// T = ((D0*256 + D1)*256 + D2)*256 + D3 for 16 columns starting at `taddr`.
+__device__ __forceinline__ void load_orders16(uint32_t taddr, long long (&T)[16]) {
+  int32_t r[16];
+  tmem_ld16(taddr, r);
+  tmem_wait_ld();
+#pragma unroll
+  for (int k = 0; k < 16; ++k) T[k] = r[k];
+#pragma unroll
+  for (int g = 1; g < 4; ++g) {
+    tmem_ld16(taddr + (uint32_t)(g * 128), r);
+    tmem_wait_ld();
+#pragma unroll
+    for (int k = 0; k < 16; ++k) T[k] = T[k] * 256 + r[k];
+  }
 }
 
 __global__ void __launch_bounds__(SP_THREADS, 1)
@@ -354,27 +371,42 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       uint32_t last_ph[SP2_ST];
       for (int q = 0; q < SP2_ST; ++q) issued[q] = false, last_ph[q] = 0;
       bool ok = true;
-      for (int item = cid; item < prm.nitems && ok; item += ncl) {
-        const int f = item / prm.ntile;
+      // Cursor over this cluster's (item, stage) sequence; it advances by increments
+      // and decodes a tile only when it enters a new item.
+      struct Cursor {
+        int item, ks, ya, yb, zf;
+      };
+      auto enter = [&](Cursor& u) {
         int bI, bJ;
-        pair_decode_tile(item % prm.ntile, &bI, &bJ);
-        for (int ks = 0; ks < prm.nk; ++ks) {
-          if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) {
-            ok = false;
-            break;
-          }
-          const uint32_t lead_full = mapa_shared(smem_u32(&sm.full[st]), 0);
-          if (rank == 0)
-            mbar_arrive_expect_tx(&sm.full[st],
-                                  (uint32_t)(2 * (SP_SA * SP_PLANE + SP_SB * SP2_BPLANE)));
-          tma_load_4d_pair(&sm.a[st][0][0], &mapA, 0, (2 * bI + (int)rank) * SP_ROWS, ks, 0,
-                           lead_full);
-          tma_load_4d_pair(&sm.b[st][0][0], &mapB, 0, bJ * SP_ROWS + (int)rank * SP2_BROWS, ks,
-                           f * SP_SB, lead_full);
-          issued[st] = true;
-          last_ph[st] = ph;
-          if (++st == SP2_ST) st = 0, ph ^= 1u;
+        pair_decode_tile(u.item % prm.ntile, &bI, &bJ);
+        u.ya = (2 * bI + (int)rank) * SP_ROWS;
+        u.yb = bJ * SP_ROWS + (int)rank * SP2_BROWS;
+        u.zf = (u.item / prm.ntile) * SP_SB;
+      };
+      auto advance = [&](Cursor& u) {
+        if (++u.ks == prm.nk) {
+          u.ks = 0;
+          u.item += ncl;
+          if (u.item < prm.nitems) enter(u);
         }
+      };
+      Cursor ld{cid, 0, 0, 0, 0};
+      if (cid < prm.nitems) enter(ld);
+      while (ld.item < prm.nitems) {
+        if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) {
+          ok = false;
+          break;
+        }
+        const uint32_t lead_full = mapa_shared(smem_u32(&sm.full[st]), 0);
+        if (rank == 0)
+          mbar_arrive_expect_tx(&sm.full[st],
+                                (uint32_t)(2 * (SP_SA * SP_PLANE + SP_SB * SP2_BPLANE)));
+        tma_load_4d_pair(&sm.a[st][0][0], &mapA, 0, ld.ya, ld.ks, 0, lead_full);
+        tma_load_4d_pair(&sm.b[st][0][0], &mapB, 0, ld.yb, ld.ks, ld.zf, lead_full);
+        advance(ld);
+        issued[st] = true;
+        last_ph[st] = ph;
+        if (++st == SP2_ST) st = 0, ph ^= 1u;
       }
       if (rank == 0) {
         // the leader's stage barriers count both CTAs' bytes
@@ -459,16 +491,16 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
         const double si = gi < prm.N ? prm.sA[gi] : 0.0;
         const double fac = si * prm.wmax[f] * (1.0 / (127.0 * 127.0 * 16777216.0));
         double* outf = prm.out + 2 * (int64_t)f * prm.npack;
-        for (int js = 0; js < 2 && ok; ++js, ++xseq) {
-          long long tre[32], tim[32];
-          load_orders(tl + (uint32_t)(js * 32), tre);
-          load_orders(tl + (uint32_t)(64 + js * 32), tim);
+        for (int js = 0; js < SP_TILE / SP2_XC && ok; ++js, ++xseq) {
+          long long tre[SP2_XC], tim[SP2_XC];
+          load_orders16(tl + (uint32_t)(js * SP2_XC), tre);
+          load_orders16(tl + (uint32_t)(64 + js * SP2_XC), tim);
           if (!mbar_wait(&sm.xfree, (xseq & 1u) ^ 1u, prm.timeout_ns, prm.status)) {
             ok = false;
             break;
           }
 #pragma unroll
-          for (int k = 0; k < 32; ++k) sm.xchg[is_re ? 0 : 1][ii][k] = tim[k];
+          for (int k = 0; k < SP2_XC; ++k) sm.xchg[is_re ? 0 : 1][ii][k] = tim[k];
           __syncwarp();
           if (lane == 0) mbar_arrive(&sm.xfull);
           if (!mbar_wait(&sm.xfull, xseq & 1u, prm.timeout_ns, prm.status)) {
@@ -476,8 +508,8 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
             break;
           }
 #pragma unroll
-          for (int k = 0; k < 32; ++k) {
-            const int gj = bJ * SP_TILE + js * 32 + k;
+          for (int k = 0; k < SP2_XC; ++k) {
+            const int gj = bJ * SP_TILE + js * SP2_XC + k;
             const long long partner = sm.xchg[is_re ? 1 : 0][ii][k];
             const long long v = is_re ? tre[k] + partner : tre[k] - partner;
             if (gi <= gj && gj < prm.N) {

@@ -149,6 +149,24 @@ __device__ __forceinline__ void tma_load_4d_pair(void* dst, const CUtensorMap* m
       : "memory");
 }
 
+// Pulls a 4-D tile into L2 ahead of its load (no shared memory, no completion).
+__device__ __forceinline__ void tma_prefetch_4d(const CUtensorMap* map, int x, int y, int z,
+                                                int w) {
+  asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(map),
+               "r"(x), "r"(y), "r"(z), "r"(w)
+               : "memory");
+}
+// 16 consecutive 32-bit TMEM columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+
 // 32 consecutive 32-bit TMEM columns of this thread's lane.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int32_t (&r)[32]) {
   asm volatile(
