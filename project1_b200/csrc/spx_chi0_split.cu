@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
     int j = 0;
     uint32_t xseq = 0;
     for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j) {
-      if (!mbar_wait(&sm.tfull, (uint32_t)(j & 1), prm.timeout_ns, prm.status)) break;
+      if (!mbar_wait_idle(&sm.tfull, (uint32_t)(j & 1), prm.timeout_ns, prm.status)) break;
       tc_fence_after();
       const int f = item / prm.ntile;
       int bi, bj;
@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
     int j = 0;
     uint32_t xseq = 0;
     for (int item = cid; item < prm.nitems; item += ncl, ++j) {
-      if (!mbar_wait(&sm.tfull, (uint32_t)(j & 1), prm.timeout_ns, prm.status)) break;
+      if (!mbar_wait_idle(&sm.tfull, (uint32_t)(j & 1), prm.timeout_ns, prm.status)) break;
       tc_fence_after();
       const int f = item / prm.ntile;
       int bI, bJ;

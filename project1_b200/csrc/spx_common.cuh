@@ -6,7 +6,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/spexgpu.h"
+#include "spexgpu.h"  // include/ is on the include path
 
 // ---------------------------------------------------------------------------
 // context
@@ -93,19 +93,49 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait: returns false (and records a timeout in *status) if the phase
-// with `parity` has not completed within `timeout_ns`.
+// with `parity` has not completed within `timeout_ns`. Polls with try_wait and
+// looks at the clock and at the other CTAs' status only every 64 polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t timeout_ns,
                                           int* status) {
   if (mbar_try_wait(bar, parity)) return true;
-  uint64_t t0 = global_ns();
-  while (!mbar_try_wait(bar, parity)) {
-    if (global_ns() - t0 > timeout_ns) {
-      atomicCAS(status, 0, (int)kStatusTimeout);
-      return false;
+  const uint64_t t0 = global_ns();
+  for (uint32_t n = 1;; ++n) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((n & 63) == 0) {
+      if (global_ns() - t0 > timeout_ns) {
+        atomicCAS(status, 0, (int)kStatusTimeout);
+        return false;
+      }
+      if (*((volatile int*)status) != 0) return false;  // another CTA gave up
     }
-    if (*((volatile int*)status) != 0) return false;  // another CTA gave up
   }
-  return true;
+}
+// The same bounded wait for warps that idle for long stretches (an epilogue waiting
+// for a whole tile): the thread sleeps inside try_wait between polls.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(2000u)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_idle(uint64_t* bar, uint32_t parity,
+                                               uint64_t timeout_ns, int* status) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t n = 1;; ++n) {
+    if (mbar_try_wait_sleep(bar, parity)) return true;
+    if ((n & 15) == 0) {
+      if (global_ns() - t0 > timeout_ns) {
+        atomicCAS(status, 0, (int)kStatusTimeout);
+        return false;
+      }
+      if (*((volatile int*)status) != 0) return false;
+    }
+  }
 }
 // Bounded wait used only on the way out after a failure: waits for copies
 // already issued to land, ignoring the status word, for at most timeout_ns.
