@@ -244,12 +244,15 @@ extern "C" int spx_ctx_create(int device, const spx_options* opt, spx_ctx** out)
                        "stream")) ||
       (rc = check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking),
                        "stream")) ||
+      (rc = check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->prep_stream, cudaStreamNonBlocking),
+                       "stream")) ||
       (rc = check_cuda(ctx, cudaMalloc(&ctx->d_status, sizeof(int)), "status word")) ||
       (rc = check_cuda(ctx, cudaMemset(ctx->d_status, 0, sizeof(int)), "status word"))) {
     spx_ctx_destroy(ctx);
     return rc;
   }
   for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+  for (auto& ev : ctx->sev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
   *out = ctx;
   return SPX_OK;
 }
@@ -259,7 +262,10 @@ extern "C" int spx_ctx_destroy(spx_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  if (ctx->prep_stream) cudaStreamSynchronize(ctx->prep_stream);
   for (auto& ev : ctx->ev)
+    if (ev) cudaEventDestroy(ev);
+  for (auto& ev : ctx->sev)
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : ctx->mark_pool) cudaEventDestroy(ev);
   if (ctx->ws) cudaFree(ctx->ws);
@@ -267,6 +273,7 @@ extern "C" int spx_ctx_destroy(spx_ctx* ctx) {
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->prep_stream) cudaStreamDestroy(ctx->prep_stream);
   delete ctx;
   return SPX_OK;
 }

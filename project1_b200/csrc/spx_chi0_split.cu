@@ -43,10 +43,12 @@ namespace spx {
 
 constexpr int SP_TILE = 64;            // complex rows / columns per tile
 constexpr int SP_ROWS = 128;           // real-stacked rows per tile (re | im)
-constexpr int SP_KB = 32;              // band pairs per pipeline stage = one int8 MMA K step
+constexpr int SP_KB = 64;              // band pairs (bytes) per pipeline stage: two MMA K steps
+constexpr int SP_KSTEP = 32;           // int8 MMA K
+constexpr int SP_NKS = SP_KB / SP_KSTEP;
 constexpr int SP_SA = 3;               // digit slices of the unweighted operand
 constexpr int SP_SB = 4;               // digit slices of the weighted operand
-constexpr int SP_ST = 6;               // pipeline stages
+constexpr int SP_ST = 3;               // pipeline stages
 constexpr int SP_SLAB = 32768;         // band pairs per exact int32 accumulation
 constexpr int SP_THREADS = 192;        // warp 0 TMA, warp 1 MMA + TMEM, warps 2-5 epilogue
 constexpr int SP_PLANE = SP_ROWS * SP_KB;  // bytes of one slice of one stage
@@ -181,23 +183,26 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
             break;
           }
           tc_fence_after();
-          uint64_t da[SP_SA], db[SP_SB];
-#pragma unroll
-          for (int t = 0; t < SP_SA; ++t) da[t] = desc_sw32(&sm.a[st][t][0]);
-#pragma unroll
-          for (int u = 0; u < SP_SB; ++u) db[u] = desc_sw32(&sm.b[st][u][0]);
           // order g = t + u lives at TMEM columns [128 g, 128 g + 128); the first
-          // product of every order in a slab (t == 0, ks == 0) overwrites it
-          const uint32_t k0 = ks > 0;
-          mma_i8<1>(tmem + 0 * 128, da[0], db[0], SP_IDESC, k0);
-          mma_i8<2>(tmem + 1 * 128, da[0], db[1], SP_IDESC, k0);
-          mma_i8<2>(tmem + 2 * 128, da[0], db[2], SP_IDESC, k0);
-          mma_i8<3>(tmem + 3 * 128, da[0], db[3], SP_IDESC, k0);
-          mma_i8<1>(tmem + 1 * 128, da[1], db[0], SP_IDESC, 1u);
-          mma_i8<2>(tmem + 2 * 128, da[1], db[1], SP_IDESC, 1u);
-          mma_i8<3>(tmem + 3 * 128, da[1], db[2], SP_IDESC, 1u);
-          mma_i8<1>(tmem + 2 * 128, da[2], db[0], SP_IDESC, 1u);
-          mma_i8<3>(tmem + 3 * 128, da[2], db[1], SP_IDESC, 1u);
+          // product of every order in a slab (t == 0, first K step) overwrites it
+#pragma unroll
+          for (int kk = 0; kk < SP_NKS; ++kk) {
+            uint64_t da[SP_SA], db[SP_SB];
+#pragma unroll
+            for (int t = 0; t < SP_SA; ++t) da[t] = desc_sw64(&sm.a[st][t][0]) + (uint64_t)(kk * 2);
+#pragma unroll
+            for (int u = 0; u < SP_SB; ++u) db[u] = desc_sw64(&sm.b[st][u][0]) + (uint64_t)(kk * 2);
+            const uint32_t k0 = (ks > 0 || kk > 0);
+            mma_i8<1>(tmem + 0 * 128, da[0], db[0], SP_IDESC, k0);
+            mma_i8<2>(tmem + 1 * 128, da[0], db[1], SP_IDESC, k0);
+            mma_i8<2>(tmem + 2 * 128, da[0], db[2], SP_IDESC, k0);
+            mma_i8<3>(tmem + 3 * 128, da[0], db[3], SP_IDESC, k0);
+            mma_i8<1>(tmem + 1 * 128, da[1], db[0], SP_IDESC, 1u);
+            mma_i8<2>(tmem + 2 * 128, da[1], db[1], SP_IDESC, 1u);
+            mma_i8<3>(tmem + 3 * 128, da[1], db[2], SP_IDESC, 1u);
+            mma_i8<1>(tmem + 2 * 128, da[2], db[0], SP_IDESC, 1u);
+            mma_i8<3>(tmem + 3 * 128, da[2], db[1], SP_IDESC, 1u);
+          }
           tc_commit(&sm.empty[st]);  // stage free once these MMAs have read it
           committed = true;
           if (++st == SP_ST) st = 0, ph ^= 1u;
@@ -287,7 +292,7 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
 // of 28 KB from L2 for the same tensor work. Every completion that crosses the
 // pair is an explicit remote arrive or commit (no multicast).
 
-constexpr int SP2_ST = 9;
+constexpr int SP2_ST = 5;
 constexpr int SP2_XC = 16;                      // columns per epilogue exchange
 constexpr int SP2_BROWS = SP_ROWS / 2;          // B rows staged per CTA
 constexpr int SP2_BPLANE = SP2_BROWS * SP_KB;   // 2048 bytes
@@ -438,21 +443,24 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
             break;
           }
           tc_fence_after();
-          uint64_t da[SP_SA], db[SP_SB];
 #pragma unroll
-          for (int t = 0; t < SP_SA; ++t) da[t] = desc_sw32(&sm.a[st][t][0]);
+          for (int kk = 0; kk < SP_NKS; ++kk) {
+            uint64_t da[SP_SA], db[SP_SB];
 #pragma unroll
-          for (int u = 0; u < SP_SB; ++u) db[u] = desc_sw32(&sm.b[st][u][0]);
-          const uint32_t k0 = ks > 0;
-          mma2_i8<1>(tmem + 0 * 128, da[0], db[0], SP2_IDESC, k0);
-          mma2_i8<2>(tmem + 1 * 128, da[0], db[1], SP2_IDESC, k0);
-          mma2_i8<2>(tmem + 2 * 128, da[0], db[2], SP2_IDESC, k0);
-          mma2_i8<3>(tmem + 3 * 128, da[0], db[3], SP2_IDESC, k0);
-          mma2_i8<1>(tmem + 1 * 128, da[1], db[0], SP2_IDESC, 1u);
-          mma2_i8<2>(tmem + 2 * 128, da[1], db[1], SP2_IDESC, 1u);
-          mma2_i8<3>(tmem + 3 * 128, da[1], db[2], SP2_IDESC, 1u);
-          mma2_i8<1>(tmem + 2 * 128, da[2], db[0], SP2_IDESC, 1u);
-          mma2_i8<3>(tmem + 3 * 128, da[2], db[1], SP2_IDESC, 1u);
+            for (int t = 0; t < SP_SA; ++t) da[t] = desc_sw64(&sm.a[st][t][0]) + (uint64_t)(kk * 2);
+#pragma unroll
+            for (int u = 0; u < SP_SB; ++u) db[u] = desc_sw64(&sm.b[st][u][0]) + (uint64_t)(kk * 2);
+            const uint32_t k0 = (ks > 0 || kk > 0);
+            mma2_i8<1>(tmem + 0 * 128, da[0], db[0], SP2_IDESC, k0);
+            mma2_i8<2>(tmem + 1 * 128, da[0], db[1], SP2_IDESC, k0);
+            mma2_i8<2>(tmem + 2 * 128, da[0], db[2], SP2_IDESC, k0);
+            mma2_i8<3>(tmem + 3 * 128, da[0], db[3], SP2_IDESC, k0);
+            mma2_i8<1>(tmem + 1 * 128, da[1], db[0], SP2_IDESC, 1u);
+            mma2_i8<2>(tmem + 2 * 128, da[1], db[1], SP2_IDESC, 1u);
+            mma2_i8<3>(tmem + 3 * 128, da[1], db[2], SP2_IDESC, 1u);
+            mma2_i8<1>(tmem + 2 * 128, da[2], db[0], SP2_IDESC, 1u);
+            mma2_i8<3>(tmem + 3 * 128, da[2], db[1], SP2_IDESC, 1u);
+          }
           // the stage is free in both CTAs once these MMAs have read it
           tc_commit2(smem_u32(&sm.empty[st]));
           tc_commit2(mapa_shared(smem_u32(&sm.empty[st]), 1));
@@ -612,10 +620,10 @@ __device__ __forceinline__ void digit_planes(const uint32_t (&Y)[4], uint32_t (&
 }
 
 // One thread = one complex column i and 16 consecutive pairs of the slab. Digit
-// planes are stored [plane][k-block of 32 pairs][row][32 bytes]; a warp holds 16
-// consecutive columns x the two halves of one k-block, so every store instruction
-// writes 16 adjacent rows x 32 bytes = 512 contiguous bytes, and the TMA box
-// (32 B, 128 rows, 1 k-block, planes) lands as [plane][row][32 B] in shared memory.
+// planes are stored [plane][k-block of 64 pairs][row][64 bytes]; a warp holds 8
+// consecutive columns x the four quarters of one k-block, so every store
+// instruction writes 8 adjacent rows x 64 bytes = 512 contiguous bytes, and the TMA
+// box (64 B, rows, 1 k-block, planes) lands as [plane][row][64 B] in shared memory.
 // Rows are real-stacked: block b of 64 columns -> rows 128 b + {0..63 Re, 64..127 Im}.
 __global__ void __launch_bounds__(128)
     split_quantize_kernel(const double2* __restrict__ M, int64_t ldc, int64_t p0, int len,
@@ -625,21 +633,21 @@ __global__ void __launch_bounds__(128)
                           int8_t* __restrict__ A, int8_t* __restrict__ B) {
   const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (tid >= (int64_t)npad * nchunk) return;
-  // tid -> (k-block, column group of 16, half of the k-block, column in group)
-  const int ngroup = npad / 16;
-  const int lane16 = (int)(tid & 15), half = (int)((tid >> 4) & 1);
+  // tid -> (k-block, column group of 8, quarter of the k-block, column in group)
+  const int ngroup = npad / 8;
+  const int lane8 = (int)(tid & 7), quarter = (int)((tid >> 3) & 3);
   const int64_t rest = tid >> 5;
-  const int i = (int)(rest % ngroup) * 16 + lane16;
+  const int i = (int)(rest % ngroup) * 8 + lane8;
   const int64_t kb = rest / ngroup;
-  const int p = (int)(kb * SP_KB) + half * 16;
+  const int p = (int)(kb * SP_KB) + quarter * 16;
   const int64_t r_re = (int64_t)(i / SP_TILE) * SP_ROWS + (i % SP_TILE);
   const int64_t r_im = r_re + SP_TILE;
   const int64_t nkb = Ps / SP_KB;
   // byte offsets of (plane 0, k-block, row) for this thread's 16 pairs; planes are
   // nkb * R * 32 bytes apart
   const int64_t pstride = nkb * R * SP_KB;
-  const int64_t a_re = (kb * R + r_re) * SP_KB + half * 16;
-  const int64_t a_im = (kb * R + r_im) * SP_KB + half * 16;
+  const int64_t a_re = (kb * R + r_re) * SP_KB + quarter * 16;
+  const int64_t a_im = (kb * R + r_im) * SP_KB + quarter * 16;
   const int64_t b_re = a_re, b_im = a_im;
   double xr[16], xi[16];
   const bool col_ok = i < N;
@@ -781,9 +789,13 @@ static SplitLayout split_layout(int64_t P, int N, int nw) {
   return L;
 }
 
+// Two operand buffers when there is more than one slab: slab s+1 is quantized
+// while slab s accumulates.
+static int split_nbuf(int64_t P) { return P > SP_SLAB ? 2 : 1; }
+
 size_t split_workspace_bytes(int64_t P, int N, int nw) {
   SplitLayout L = split_layout(P, N, nw);
-  return L.a_bytes + L.b_bytes + L.s_bytes + L.w_bytes + 1024;
+  return split_nbuf(P) * (L.a_bytes + L.b_bytes + L.s_bytes + L.w_bytes) + 1024;
 }
 
 void timing_mark(spx_ctx* ctx, cudaStream_t s, int kind);
@@ -796,40 +808,38 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
   if (!ws || ws_bytes < split_workspace_bytes(P, N, nw))
     return set_error(ctx, SPX_EINVAL, "split workspace too small");
   uint8_t* base = (uint8_t*)align_up((size_t)ws, 1024);
-  int8_t* A = (int8_t*)base;
-  int8_t* B = (int8_t*)(base + L.a_bytes);
-  double* sA = (double*)(base + L.a_bytes + L.b_bytes);
-  double* wmax = (double*)(base + L.a_bytes + L.b_bytes + L.s_bytes);
-
-  // planes in HBM: [plane][k-block][row][32 B]; TMA dims (32 B, row, k-block, plane)
-  // with increasing strides; a box (32, 128, 1, planes) lands as [plane][row][32 B]
-  CUtensorMap mapA, mapB;
-  const uint64_t nkb = (uint64_t)(L.Ps / SP_KB);
-  {
-    const uint64_t dims[4] = {SP_KB, (uint64_t)L.R, nkb, SP_SA};
-    const uint64_t strides[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};
-    const uint32_t box[4] = {SP_KB, SP_ROWS, 1, SP_SA};
-    int rc = make_tmap_u8_4d(ctx, &mapA, A, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_32B);
-    if (rc) return rc;
+  const int nbuf = split_nbuf(P);
+  const size_t set_bytes = L.a_bytes + L.b_bytes + L.s_bytes + L.w_bytes;
+  int8_t* A[2];
+  int8_t* B[2];
+  double* sA[2];
+  double* wmax[2];
+  for (int b = 0; b < 2; ++b) {
+    uint8_t* s0 = base + (size_t)(b < nbuf ? b : 0) * set_bytes;
+    A[b] = (int8_t*)s0;
+    B[b] = (int8_t*)(s0 + L.a_bytes);
+    sA[b] = (double*)(s0 + L.a_bytes + L.b_bytes);
+    wmax[b] = (double*)(s0 + L.a_bytes + L.b_bytes + L.s_bytes);
   }
-  {
-    const uint64_t dims[4] = {SP_KB, (uint64_t)L.R, nkb, (uint64_t)SP_SB * nw};
-    const uint64_t strides[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};
-    const uint32_t box[4] = {SP_KB, SP_ROWS, 1, SP_SB};
-    int rc = make_tmap_u8_4d(ctx, &mapB, B, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_32B);
-    if (rc) return rc;
+
+  // planes in HBM: [plane][k-block][row][K bytes]; TMA dims (K, row, k-block, plane)
+  // with increasing strides; a box (K, rows, 1, planes) lands as [plane][row][K]
+  const uint64_t nkb = (uint64_t)(L.Ps / SP_KB);
+  const bool pair = ctx->opt.split_variant != 1;  // 0 (auto) and 2 select the CTA pair
+  CUtensorMap mapA[2], mapB[2];
+  for (int b = 0; b < nbuf; ++b) {
+    const uint64_t sta[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};
+    const uint64_t da[4] = {SP_KB, (uint64_t)L.R, nkb, SP_SA};
+    const uint32_t ba[4] = {SP_KB, SP_ROWS, 1, SP_SA};
+    int rc0 = make_tmap_u8_4d(ctx, &mapA[b], A[b], da, sta, ba, CU_TENSOR_MAP_SWIZZLE_64B);
+    if (rc0) return rc0;
+    const uint64_t db[4] = {SP_KB, (uint64_t)L.R, nkb, (uint64_t)SP_SB * nw};
+    const uint32_t bb[4] = {SP_KB, (uint32_t)(pair ? SP2_BROWS : SP_ROWS), 1, SP_SB};
+    rc0 = make_tmap_u8_4d(ctx, &mapB[b], B[b], db, sta, bb, CU_TENSOR_MAP_SWIZZLE_64B);
+    if (rc0) return rc0;
   }
   int rc = SPX_OK;
 
-  const bool pair = ctx->opt.split_variant != 1;  // 0 (auto) and 2 select the CTA pair
-  CUtensorMap mapB2;
-  if (pair) {
-    const uint64_t dims[4] = {SP_KB, (uint64_t)L.R, nkb, (uint64_t)SP_SB * nw};
-    const uint64_t strides[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};
-    const uint32_t box[4] = {SP_KB, SP2_BROWS, 1, SP_SB};
-    int rc2 = make_tmap_u8_4d(ctx, &mapB2, B, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_32B);
-    if (rc2) return rc2;
-  }
   const size_t smem = sizeof(SplitSmem) + 1024;
   const size_t smem2 = sizeof(Split2Smem) + 1024;
   static bool attr_set = false;
@@ -869,18 +879,45 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
     cfg.gridDim = dim3(2 * nclusters);
   }
 
-  for (int64_t p0 = 0; p0 < P; p0 += L.Ps) {
+  // Preparation (column scales, weight maxima, digit planes) of slab s+1 runs on
+  // the preparation stream while slab s accumulates on `stream`; buffer b = s % 2.
+  const int64_t nslab = (P + L.Ps - 1) / L.Ps;
+  cudaStream_t ps = ctx->prep_stream;
+  cudaEvent_t ev_start = ctx->sev[0];
+  cudaEvent_t prep_done[2] = {ctx->sev[1], ctx->sev[2]};
+  cudaEvent_t gram_done[2] = {ctx->sev[3], ctx->sev[4]};
+  auto prep = [&](int64_t s) -> int {
+    const int b = (int)(s % nbuf);
+    const int64_t p0 = s * L.Ps;
     const int len = (int)std::min<int64_t>(L.Ps, P - p0);
     const int lenp = (int)align_up((size_t)len, SP_KB);
     const int nchunk = lenp / 16;  // 16-pair chunks; npad is a multiple of 64
-    timing_mark(ctx, stream, 0);
-    split_colmax_kernel<<<N, 256, 0, stream>>>(M, ldc, p0, len, sA);
-    split_wmax_kernel<<<nw, 256, 0, stream>>>(W, ldw, p0, len, wmax);
+    split_colmax_kernel<<<N, 256, 0, ps>>>(M, ldc, p0, len, sA[b]);
+    split_wmax_kernel<<<nw, 256, 0, ps>>>(W, ldw, p0, len, wmax[b]);
     const int64_t nthr = (int64_t)npad * nchunk;
-    split_quantize_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, stream>>>(
-        M, ldc, p0, len, nchunk, N, npad, L.R, L.Ps, W, ldw, nw, sA, wmax, A, B);
-    rc = check_cuda(ctx, cudaGetLastError(), "split operand preparation");
-    if (rc) return rc;
+    split_quantize_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, ps>>>(
+        M, ldc, p0, len, nchunk, N, npad, L.R, L.Ps, W, ldw, nw, sA[b], wmax[b], A[b], B[b]);
+    int r = check_cuda(ctx, cudaGetLastError(), "split operand preparation");
+    if (r) return r;
+    *launches += 3;
+    return check_cuda(ctx, cudaEventRecord(prep_done[b], ps), "event");
+  };
+  // the preparation stream starts after everything already queued on `stream`
+  // (the weights, and whatever produced cprod)
+  if ((rc = check_cuda(ctx, cudaEventRecord(ev_start, stream), "event")) ||
+      (rc = check_cuda(ctx, cudaStreamWaitEvent(ps, ev_start, 0), "event")))
+    return rc;
+  timing_mark(ctx, stream, 0);
+  if ((rc = prep(0))) return rc;
+  for (int64_t s = 0; s < nslab; ++s) {
+    const int b = (int)(s % nbuf);
+    const int len = (int)std::min<int64_t>(L.Ps, P - s * L.Ps);
+    const int lenp = (int)align_up((size_t)len, SP_KB);
+    if ((rc = check_cuda(ctx, cudaStreamWaitEvent(stream, prep_done[b], 0), "event"))) return rc;
+    // with two buffers, slab s+1 goes into the buffer that slab s-1 accumulated from
+    if (nbuf == 2 && s >= 1 && s + 1 < nslab &&
+        (rc = check_cuda(ctx, cudaStreamWaitEvent(ps, gram_done[(s + 1) % 2], 0), "event")))
+      return rc;
     timing_mark(ctx, stream, 1);
     SplitParams prm;
     prm.N = N;
@@ -888,22 +925,30 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
     prm.nw = nw;
     prm.nitems = nitems;
     prm.nk = lenp / SP_KB;
-    prm.sA = sA;
-    prm.wmax = wmax;
+    prm.sA = sA[b];
+    prm.wmax = wmax[b];
     prm.out = reinterpret_cast<double*>(out);
     prm.npack = (int64_t)N * (N + 1) / 2;
     prm.status = ctx->d_status;
     prm.timeout_ns =
         (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
     if (pair) {
-      rc = check_cuda(ctx, cudaLaunchKernelEx(&cfg, split_gram2_kernel, mapA, mapB2, prm),
+      rc = check_cuda(ctx, cudaLaunchKernelEx(&cfg, split_gram2_kernel, mapA[b], mapB[b], prm),
                       "split_gram2_kernel launch");
     } else {
-      split_gram_kernel<<<grid, SP_THREADS, smem, stream>>>(mapA, mapB, prm);
+      split_gram_kernel<<<grid, SP_THREADS, smem, stream>>>(mapA[b], mapB[b], prm);
       rc = check_cuda(ctx, cudaGetLastError(), "split_gram_kernel launch");
     }
     if (rc) return rc;
-    *launches += 4;
+    *launches += 1;
+    if ((rc = check_cuda(ctx, cudaEventRecord(gram_done[b], stream), "event"))) return rc;
+    if (s + 1 < nslab) {
+      // with one buffer, the next preparation waits for this accumulation
+      if (nbuf == 1 &&
+          (rc = check_cuda(ctx, cudaStreamWaitEvent(ps, gram_done[0], 0), "event")))
+        return rc;
+      if ((rc = prep(s + 1))) return rc;
+    }
   }
   return SPX_OK;
 }

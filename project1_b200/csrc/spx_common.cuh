@@ -17,6 +17,8 @@ struct spx_ctx {
   int cc_major = 0, cc_minor = 0;
   cudaStream_t stream = nullptr;   // main compute stream
   cudaStream_t copy_stream = nullptr;
+  cudaStream_t prep_stream = nullptr;  // split-path operand preparation, overlapped
+  cudaEvent_t sev[5] = {};             // split path: start, prep done x2, accumulation done x2
   spx_options opt{};
   std::string err;
   int* d_status = nullptr;         // device error word (0 = ok), see spx_status_*

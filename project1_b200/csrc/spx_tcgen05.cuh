@@ -197,6 +197,20 @@ __device__ __forceinline__ uint64_t desc_sw32(const void* smem_tile) {
   return d;
 }
 
+// K-major operand descriptor for a SWIZZLE_64B tile of 64-byte rows: 8-row atoms
+// of 512 B (SBO), version 1, layout type 4. The second 32-byte K step of a row is
+// addressed by advancing the start address by 32 bytes inside the atom.
+__device__ __forceinline__ uint64_t desc_sw64(const void* smem_tile) {
+  const uint32_t a = smem_u32(smem_tile);
+  uint64_t d = 0;
+  d |= (uint64_t)((a >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;                  // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;         // stride byte offset: next 8-row group
+  d |= (uint64_t)1 << 46;                  // descriptor version for sm_100
+  d |= (uint64_t)4 << 61;                  // SWIZZLE_64B
+  return d;
+}
+
 // 3-D tiled TMA load into shared memory, completing on `bar`.
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
                                             uint64_t* bar) {
