@@ -197,11 +197,11 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
+    from project1_b200.parallel import pair_shard, reduce_partial
     w = workload_from_args(args)
-    # shard the pair axis: rank r owns a contiguous block of k points (Mblocks over k)
+    # shard the pair axis: rank r owns a contiguous block of whole k points (Mblocks)
     P = w.npair
-    p_lo = rank * P // world
-    p_hi = (rank + 1) * P // world
+    p_lo, p_hi = pair_shard(P, world, rank, block=w.nocc * w.nunocc)
     Pr = p_hi - p_lo
     N, nw = w.nbas, w.nw
     npk = spx.npack(N)
@@ -232,8 +232,7 @@ def run_ours(args):
         out.zero_()
         st = ctx.chi0_accumulate_dev(M, ediff, omega, out, scale_all=1.0 / w.nk, precision=precision,
                                      stream=stream.cuda_stream, stats=True)
-        if world > 1:
-            dist.reduce(out, 0)
+        reduce_partial(out, dst=0)
         return st
 
     def timed(precision, warmup, steps, sampler=None):
