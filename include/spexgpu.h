@@ -138,6 +138,69 @@ int spx_chi0_accumulate_dev_noalloc(const double* cprod, int64_t ldc, int64_t np
  * factor 2 of src/susceptibility.f:1331-1343 for unpolarised, non-SOC runs. */
 int spx_scale_dev(spx_ctx* ctx, double* z, int64_t n, double factor, void* stream);
 
+/* ---- mixed-product-basis projections (K4) -----------------------------------
+ * Muffin-tin part, replaces wavefproducts2_mt (src/wavefproducts.f:95-431, the
+ * non-INV, no-SOC branch): for every atom a, k point k, occupied band n and
+ * unoccupied band n',
+ *   cprod(p, a*maxllm + I) += cexp_a * sum_lm1 cmt_unocc(lm1, n') * conj(mat_n(lm1, I)),
+ *   mat_n(lm1, I) = sum_lm cmt_occ(lm, n) * integral(ln, ln1, lln) * gaunt1(l1, l, LL, m, MM),
+ * p = n' + nunocc*(n + nocc*k), with the index nest of :299-337. All atoms share
+ * gaunt1 and integral (one atom type); maxlm = (lcut+1)^2 nrad,
+ * maxllm = (lcutm+1)^2 nradm. The descriptor arrays are host memory. */
+typedef struct spx_mt_desc {
+  int32_t natom, lcut, nrad, lcutm, nradm;
+  int32_t ld1;              /* second dimension of integral (>= (lcut+1)*nrad)       */
+  const double* gaunt;      /* gaunt1(0:lcut, 0:lcut, 0:lcutm, -lcut:lcut, -lcutm:lcutm),
+                               column-major                                          */
+  const double* integral;   /* integral((lcut+1)*nrad, ld1, (lcutm+1)*nradm), col-major */
+  const double* cexp;       /* complex (natom): exp(-2 pi i q.R_a)                    */
+} spx_mt_desc;
+
+/* Interstitial part, replaces the explicit-convolution branch of
+ * wavefproducts2_pw (src/wavefproducts.f:760-997) with the step function:
+ *   cpw0(G0) = sum_G1 cstep(G0 - G1) cpw_occ(G1),
+ *   cprod(p, col0 + ig) += 1/sqrt(vol) * sum_ig2 cpw_unocc(ig2, n') * conj(cpw0(G2(ig2) - GM(ig) + g)).
+ * gpt1 lists the G vectors of the occupied states (at k), gpt2 those of the
+ * unoccupied states (at k+q), gptm the mixed-basis plane waves; one set is used
+ * for every k of a call (call once per k when the sets differ). Host arrays. */
+typedef struct spx_pw_desc {
+  int32_t ngpt1, ngpt2, ngptm;
+  int32_t step_radius;      /* cstep is given on [-sr, sr]^3, sr <= 4                 */
+  const int32_t* gpt1;      /* (3, ngpt1) integer G vectors                           */
+  const int32_t* gpt2;      /* (3, ngpt2)                                             */
+  const int32_t* gptm;      /* (3, ngptm)                                             */
+  int32_t gshift[3];        /* backfolding vector g (src/wavefproducts.f:549-551)     */
+  int32_t reserved;
+  const double* cstep;      /* complex (2sr+1)^3, x fastest                            */
+  double vol;               /* unit-cell volume                                        */
+} spx_pw_desc;
+
+/* Coefficient layouts (complex, C order, device memory):
+ *   cmt_occ (nk, nocc, natom, maxlm), cmt_unocc (nk, nunocc, natom, maxlm),
+ *   cpw_occ (nk, nocc, ngpt1), cpw_unocc (nk, nunocc, ngpt2);
+ * cprod is the column-major (ldc, ncol) complex matrix of spx_chi0_accumulate,
+ * ldc >= nk*nocc*nunocc. Both calls ADD into cprod. Ordered on `stream`. */
+int spx_wfprod_mt_dev(spx_ctx* ctx, const spx_mt_desc* mt, int32_t nk, int32_t nocc,
+                      int32_t nunocc, const double* cmt_occ, const double* cmt_unocc,
+                      double* cprod, int64_t ldc, void* stream);
+int spx_wfprod_pw_dev(spx_ctx* ctx, const spx_pw_desc* pw, int32_t nk, int32_t nocc,
+                      int32_t nunocc, const double* cpw_occ, const double* cpw_unocc,
+                      double* cprod, int64_t ldc, int32_t col0, void* stream);
+
+/* Products and polarisation in one call, with M kept on the device: the packet
+ * loop of src/susceptibility.f:751-1276 from the wave-function coefficients
+ * (products :778,790, weights :950-975, accumulation :1182-1240). The mixed
+ * basis is the natom*maxllm MT functions followed by the ngptm plane waves;
+ * pairs p = n' + nunocc*(n + nocc*k). ediff, wscale (may be NULL), omega and
+ * susceph as in spx_chi0_accumulate_dev; all arrays device memory. */
+int spx_chi0_from_coeffs_dev(spx_ctx* ctx, const spx_mt_desc* mt, const spx_pw_desc* pw,
+                             int32_t nk, int32_t nocc, int32_t nunocc,
+                             const double* cmt_occ, const double* cmt_unocc,
+                             const double* cpw_occ, const double* cpw_unocc,
+                             const double* ediff, const double* wscale, double scale_all,
+                             int32_t nw, const double* omega, int32_t precision,
+                             double* susceph, void* stream, spx_chi0_stats* stats);
+
 /* ---- seeded synthetic inputs (K8) -------------------------------------------
  * Philox4x32-10 (Salmon et al., SC'11) with a Box-Muller transform written from
  * basic IEEE operations only, so host and device produce identical bits.

@@ -88,3 +88,85 @@ def chi0_element(a, b, w) -> np.ndarray:
 
 def max_threads() -> int:
     return load().oracle_max_threads()
+
+
+def _bind_wfprod(lib):
+    P, I64, D = C.c_void_p, C.c_int64, C.c_double
+    ci = C.c_int
+    lib.oracle_wfprod_mt.argtypes = [ci, ci, ci, ci, ci, P, P, ci, P, ci, ci, ci, P, P, P, I64]
+    lib.oracle_wfprod_mt.restype = None
+    lib.oracle_wfprod_pw.argtypes = [ci, P, ci, P, ci, P, P, ci, P, D, ci, ci, ci, P, P, P, I64, ci]
+    lib.oracle_wfprod_pw.restype = None
+
+
+def wfprod_mt(mt, nk, nocc, nunocc, cmt_occ, cmt_unocc, cprod, ldc=None):
+    """cprod(:, :nbasp) += wavefproducts2_mt (src/wavefproducts.f:95-431). `mt` is the
+    dict of project1_b200.inputs.mt_basis; cprod is Fortran (npair, nbas) complex."""
+    lib = load()
+    _bind_wfprod(lib)
+    g = np.asfortranarray(mt["gaunt"], dtype=np.float64)
+    integ = np.asfortranarray(mt["integral"], dtype=np.float64)
+    ce = np.ascontiguousarray(mt["cexp"], dtype=np.complex128)
+    c1 = np.ascontiguousarray(cmt_occ, dtype=np.complex128)
+    c2 = np.ascontiguousarray(cmt_unocc, dtype=np.complex128)
+    lib.oracle_wfprod_mt(mt["natom"], mt["lcut"], mt["nrad"], mt["lcutm"], mt["nradm"], _p(g), _p(integ),
+                         integ.shape[1], _p(ce), nk, nocc, nunocc, _p(c1), _p(c2), _p(cprod),
+                         cprod.shape[0] if ldc is None else ldc)
+    return cprod
+
+
+def wfprod_pw(pw, nk, nocc, nunocc, cpw_occ, cpw_unocc, cprod, col0, ldc=None):
+    """cprod(:, col0:col0+ngptm) += explicit-convolution wavefproducts2_pw with the step
+    function (src/wavefproducts.f:760-997)."""
+    lib = load()
+    _bind_wfprod(lib)
+    gpt1 = np.ascontiguousarray(pw["gpt1"], dtype=np.int32)
+    gpt2 = np.ascontiguousarray(pw["gpt2"], dtype=np.int32)
+    gptm = np.ascontiguousarray(pw["gptm"], dtype=np.int32)
+    gsh = np.ascontiguousarray(pw["gshift"], dtype=np.int32)
+    cs = np.ascontiguousarray(pw["cstep"], dtype=np.complex128)
+    c1 = np.ascontiguousarray(cpw_occ, dtype=np.complex128)
+    c2 = np.ascontiguousarray(cpw_unocc, dtype=np.complex128)
+    lib.oracle_wfprod_pw(gpt1.shape[0], _p(gpt1), gpt2.shape[0], _p(gpt2), gptm.shape[0], _p(gptm), _p(gsh), pw["step_radius"], _p(cs),
+                         pw["vol"], nk, nocc, nunocc, _p(c1), _p(c2), _p(cprod),
+                         cprod.shape[0] if ldc is None else ldc, col0)
+    return cprod
+
+
+def wfprod_pw_fft(pw, nk, nocc, nunocc, cpw_occ, cpw_unocc, nfft):
+    """The FFT branch of wavefproducts2_pw (src/wavefproducts.f:576-758) in numpy:
+    scatter to the grid, FFTW_BACKWARD (G -> r), conj(.)/sqrt(vol) times the step
+    function, times FFT(phi_n')/nnfft, FFTW_FORWARD (r -> G), gather G_M - g.
+    Returns cprod_pw (npair, ngptm). Used only to cross-check the explicit path."""
+    gpt1, gpt2, gptm, gsh = pw["gpt1"], pw["gpt2"], pw["gptm"], np.asarray(pw["gshift"])
+    sr = pw["step_radius"]
+    ns = 2 * sr + 1
+    nn = nfft ** 3
+    cs = np.asarray(pw["cstep"]).reshape(ns, ns, ns, order="F")
+    grid_step = np.zeros((nfft,) * 3, complex)
+    for d0 in range(-sr, sr + 1):
+        for d1 in range(-sr, sr + 1):
+            for d2 in range(-sr, sr + 1):
+                grid_step[d0 % nfft, d1 % nfft, d2 % nfft] = cs[d0 + sr, d1 + sr, d2 + sr]
+    theta = np.fft.ifftn(grid_step) * nn          # FFTW_BACKWARD is unnormalised
+    idx1 = tuple((gpt1 % nfft).T)
+    idx2 = tuple((gpt2 % nfft).T)
+    out_idx = tuple(((gptm - gsh) % nfft).T)
+    c1 = np.asarray(cpw_occ).reshape(nk, nocc, gpt1.shape[0])
+    c2 = np.asarray(cpw_unocc).reshape(nk, nunocc, gpt2.shape[0])
+    res = np.zeros((nk, nocc, nunocc, gptm.shape[0]), complex)
+    for k in range(nk):
+        r1 = []
+        for n in range(nocc):
+            g = np.zeros((nfft,) * 3, complex)
+            g[idx1] = c1[k, n]
+            r1.append(np.conj(np.fft.ifftn(g) * nn / np.sqrt(pw["vol"])) * theta)
+        for npr in range(nunocc):
+            g = np.zeros((nfft,) * 3, complex)
+            g[idx2] = c2[k, npr]
+            r2 = np.fft.ifftn(g) * nn / nn
+            for n in range(nocc):
+                prod = np.fft.fftn(r1[n] * r2)
+                res[k, n, npr] = prod[out_idx]
+    # layout p = n' + nu*(n + no*k)
+    return res.reshape(nk * nocc * nunocc, -1)

@@ -47,6 +47,24 @@ class spx_chi0_stats(C.Structure):
     ]
 
 
+class spx_mt_desc(C.Structure):
+    _fields_ = [
+        ("natom", C.c_int32), ("lcut", C.c_int32), ("nrad", C.c_int32),
+        ("lcutm", C.c_int32), ("nradm", C.c_int32), ("ld1", C.c_int32),
+        ("gaunt", C.c_void_p), ("integral", C.c_void_p), ("cexp", C.c_void_p),
+    ]
+
+
+class spx_pw_desc(C.Structure):
+    _fields_ = [
+        ("ngpt1", C.c_int32), ("ngpt2", C.c_int32), ("ngptm", C.c_int32),
+        ("step_radius", C.c_int32),
+        ("gpt1", C.c_void_p), ("gpt2", C.c_void_p), ("gptm", C.c_void_p),
+        ("gshift", C.c_int32 * 3), ("reserved", C.c_int32),
+        ("cstep", C.c_void_p), ("vol", C.c_double),
+    ]
+
+
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
 _I64 = C.c_int64
@@ -72,6 +90,15 @@ SIGNATURES = {
     "spx_scale_dev": (C.c_int, [_P, _P, _I64, C.c_double, _P]),
     "spx_chi0_accumulate_dev_noalloc": (
         C.c_int, [_P, _I64, _I64, _I32, _P, _P, C.c_double, _I32, _P, _P, _P]),
+    "spx_wfprod_mt_dev": (
+        C.c_int, [_P, C.POINTER(spx_mt_desc), _I32, _I32, _I32, _P, _P, _P, _I64, _P]),
+    "spx_wfprod_pw_dev": (
+        C.c_int, [_P, C.POINTER(spx_pw_desc), _I32, _I32, _I32, _P, _P, _P, _I64, _I32, _P]),
+    "spx_chi0_from_coeffs_dev": (
+        C.c_int,
+        [_P, C.POINTER(spx_mt_desc), C.POINTER(spx_pw_desc), _I32, _I32, _I32, _P, _P, _P, _P,
+         _P, _P, C.c_double, _I32, _P, _I32, _P, _P, C.POINTER(spx_chi0_stats)],
+    ),
     "spx_gen_normal_host": (None, [C.c_uint64, C.c_uint32, _I64, _I64, C.c_double, _P]),
     "spx_gen_normal_dev": (C.c_int, [_P, C.c_uint64, C.c_uint32, _I64, _I64, C.c_double, _P, _P]),
     "spx_gen_cmatrix_host": (None, [C.c_uint64, C.c_uint32, _I64, _I64, _I64, _I64, C.c_double, _P]),
