@@ -201,6 +201,68 @@ int spx_chi0_from_coeffs_dev(spx_ctx* ctx, const spx_mt_desc* mt, const spx_pw_d
                              int32_t nw, const double* omega, int32_t precision,
                              double* susceph, void* stream, spx_chi0_stats* stats);
 
+/* ---- many q points in one launch (K7) ---------------------------------------
+ * The q loop of the reference driver (src/correlation.f:293-339 calls
+ * `susceptibility` once per q point) as one call: every q has its own N_MB,
+ * band window and output. Each q is accumulated exactly as by
+ * spx_chi0_accumulate_dev (same slabs and kernels, so the same bits). Its M is
+ * a device array, or is generated on the device slab by slab from the seeded
+ * Philox stream (cprod = NULL), so that no q's M is ever held whole.
+ * Unless SPX_BATCH_NOGRAPH is given, the whole schedule (generation, weights,
+ * operand preparation, accumulation of every slab of every q) is captured once
+ * into a CUDA graph, cached in the context under the batch's signature, and
+ * replayed with a single launch. */
+typedef struct spx_q_desc {
+  int32_t nbas;             /* N_MB of this q                                         */
+  int32_t variant;          /* split kernel: 0 tuned / context default, 1 one CTA per
+                               tile, 2 CTA pair                                       */
+  int64_t npair;
+  int32_t slab_pairs;       /* pairs per exact int32 slab, multiple of 64 and
+                               <= 32768; 0 tuned / 32768                              */
+  int32_t reserved0;
+  const double* cprod;      /* device (ldc, nbas) complex, or NULL = generated        */
+  int64_t ldc;
+  uint64_t seed;            /* generated M: element (p, c) of stream (seed, stream_id) */
+  uint32_t stream_id;       /* laid out as spx_gen_cmatrix_*, times m_scale           */
+  int32_t reserved1;
+  double m_scale;
+  const double* ediff;      /* device (npair)                                         */
+  const double* wscale;     /* device (npair) or NULL                                 */
+  double scale_all;
+  double* susceph;          /* device packed (nbas(nbas+1)/2, nw), accumulated        */
+} spx_q_desc;
+
+#define SPX_BATCH_AUTOTUNE 1  /* measure (N, P) buckets missing from the table first  */
+#define SPX_BATCH_NOGRAPH  2  /* enqueue the schedule directly, without a graph       */
+
+/* omega: device (nw). Ordered on `stream`; returns once enqueued unless stats. */
+int spx_chi0_batched(spx_ctx* ctx, int32_t nq, const spx_q_desc* q, int32_t nw,
+                     const double* omega, int32_t precision, int32_t flags, void* stream,
+                     spx_chi0_stats* stats);
+
+/* Split-path tuning table of a context: per (N_MB bucket, pair bucket, nw) the
+ * kernel variant and slab size that measured fastest on a probe of that shape. */
+typedef struct spx_tune_entry {
+  int32_t nbas_bucket;      /* ceil(nbas / 128)                                        */
+  int32_t npair_bucket;     /* 0: npair <= 16384, 1: <= 32768, 2: more                 */
+  int32_t nw;
+  int32_t variant;          /* 1 one CTA per tile, 2 CTA pair                          */
+  int32_t slab_pairs;
+  int32_t reserved;
+  double  tflops;           /* measured throughput of the chosen configuration        */
+} spx_tune_entry;
+
+/* Measures the candidates on a seeded probe of (nbas, min(npair, 65536), nw),
+ * stores the best in the table and returns it in *out (may be NULL). */
+int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
+                       spx_tune_entry* out);
+/* SPX_OK and *out if the bucket of (nbas, npair, nw) is in the table, else SPX_ENOTSUP. */
+int spx_tune_lookup(const spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
+                    spx_tune_entry* out);
+/* The table as a JSON file, and back (entries are merged into the table). */
+int spx_tune_save(const spx_ctx* ctx, const char* path);
+int spx_tune_load(spx_ctx* ctx, const char* path);
+
 /* ---- seeded synthetic inputs (K8) -------------------------------------------
  * Philox4x32-10 (Salmon et al., SC'11) with a Box-Muller transform written from
  * basic IEEE operations only, so host and device produce identical bits.

@@ -65,6 +65,27 @@ class spx_pw_desc(C.Structure):
     ]
 
 
+class spx_q_desc(C.Structure):
+    _fields_ = [
+        ("nbas", C.c_int32), ("variant", C.c_int32), ("npair", C.c_int64),
+        ("slab_pairs", C.c_int32), ("reserved0", C.c_int32),
+        ("cprod", C.c_void_p), ("ldc", C.c_int64),
+        ("seed", C.c_uint64), ("stream_id", C.c_uint32), ("reserved1", C.c_int32),
+        ("m_scale", C.c_double), ("ediff", C.c_void_p), ("wscale", C.c_void_p),
+        ("scale_all", C.c_double), ("susceph", C.c_void_p),
+    ]
+
+
+class spx_tune_entry(C.Structure):
+    _fields_ = [
+        ("nbas_bucket", C.c_int32), ("npair_bucket", C.c_int32), ("nw", C.c_int32),
+        ("variant", C.c_int32), ("slab_pairs", C.c_int32), ("reserved", C.c_int32),
+        ("tflops", C.c_double),
+    ]
+
+
+SPX_BATCH_AUTOTUNE, SPX_BATCH_NOGRAPH = 1, 2
+
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
 _I64 = C.c_int64
@@ -99,6 +120,12 @@ SIGNATURES = {
         [_P, C.POINTER(spx_mt_desc), C.POINTER(spx_pw_desc), _I32, _I32, _I32, _P, _P, _P, _P,
          _P, _P, C.c_double, _I32, _P, _I32, _P, _P, C.POINTER(spx_chi0_stats)],
     ),
+    "spx_chi0_batched": (
+        C.c_int, [_P, _I32, C.POINTER(spx_q_desc), _I32, _P, _I32, _I32, _P, C.POINTER(spx_chi0_stats)]),
+    "spx_autotune_split": (C.c_int, [_P, _I32, _I64, _I32, C.POINTER(spx_tune_entry)]),
+    "spx_tune_lookup": (C.c_int, [_P, _I32, _I64, _I32, C.POINTER(spx_tune_entry)]),
+    "spx_tune_save": (C.c_int, [_P, C.c_char_p]),
+    "spx_tune_load": (C.c_int, [_P, C.c_char_p]),
     "spx_gen_normal_host": (None, [C.c_uint64, C.c_uint32, _I64, _I64, C.c_double, _P]),
     "spx_gen_normal_dev": (C.c_int, [_P, C.c_uint64, C.c_uint32, _I64, _I64, C.c_double, _P, _P]),
     "spx_gen_cmatrix_host": (None, [C.c_uint64, C.c_uint32, _I64, _I64, _I64, _I64, C.c_double, _P]),

@@ -33,7 +33,7 @@ int launch_gen_cmatrix(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, int64_t, 
 int launch_chi0_fp64(spx_ctx*, const double2*, int64_t, int64_t, int, const double*, int64_t,
                      int, double2*, cudaStream_t, int);
 int split_chi0_slab(spx_ctx*, const double2*, int64_t, int64_t, int, const double*, int64_t,
-                    int, double2*, void*, size_t, cudaStream_t, int*, cudaEvent_t);
+                    int, double2*, void*, size_t, cudaStream_t, int*, int variant, int slab);
 size_t split_workspace_bytes(int64_t P, int N, int nw);
 
 void timing_mark(spx_ctx* ctx, cudaStream_t s, int kind) {
@@ -182,7 +182,7 @@ static int chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int
   } else {
     // the split path marks its own preparation / accumulation phases
     rc = split_chi0_slab(ctx, M, ldc, P, N, W, ldw, nw, out, split_ws, split_ws_bytes, s,
-                         launches, nullptr);
+                         launches, 0, 0);
   }
   timing_mark(ctx, s, 2);
   return rc;
@@ -268,6 +268,10 @@ extern "C" int spx_ctx_destroy(spx_ctx* ctx) {
   for (auto& ev : ctx->sev)
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : ctx->mark_pool) cudaEventDestroy(ev);
+  for (auto& g : ctx->graphs) {
+    cudaGraphExecDestroy(g.exec);
+    cudaGraphDestroy(g.graph);
+  }
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->d_status) cudaFree(ctx->d_status);

@@ -1,0 +1,440 @@
+// K7: the polarisation of many q points in one launch, and the split-path autotuner.
+//
+// The reference computes one q point per call of `susceptibility`
+// (src/correlation.f:293-339), each with its own mixed basis and band window.
+// spx_chi0_batched takes the whole list: the schedule of every q (optional
+// on-device generation of M, FP64 weights, digit planes, int8 tensor-core
+// accumulation, slab by slab) is captured once into a CUDA graph and replayed
+// with one launch; the graph is cached in the context under a hash of the
+// batch (shapes, pointers, workspace), so a repeated batch costs one
+// cudaGraphLaunch. Per q the slabs and kernels are exactly those of
+// spx_chi0_accumulate_dev, so results are bit-identical to per-q calls.
+//
+// The autotuner times the split-kernel variants (one CTA per tile, CTA pair)
+// and slab sizes on a seeded probe of each (N bucket, pair bucket, nw) and keeps
+// the fastest in the context's table, which the batched call consults for
+// every q whose descriptor leaves the choice open. The table persists as JSON.
+#include <cuda_runtime.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "spx_common.cuh"
+
+namespace spx {
+
+int launch_weights(spx_ctx*, int64_t, int64_t, const double*, const double*, double, int,
+                   const double*, double*, cudaStream_t);
+int launch_chi0_fp64(spx_ctx*, const double2*, int64_t, int64_t, int, const double*, int64_t,
+                     int, double2*, cudaStream_t, int);
+int split_chi0_slab(spx_ctx*, const double2*, int64_t, int64_t, int, const double*, int64_t,
+                    int, double2*, void*, size_t, cudaStream_t, int*, int, int);
+size_t split_workspace_bytes(int64_t P, int N, int nw, int slab);
+int launch_gen_cmatrix_rows(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, int64_t, int64_t,
+                            int64_t, double, double2*, cudaStream_t);
+int launch_gen_normal(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, double, double*,
+                      cudaStream_t);
+
+constexpr int kDefaultVariant = 2;
+constexpr int kDefaultSlab = 32768;
+constexpr int64_t kChunkSlabs = 8;   // pairs per generated / weighted chunk, in slabs
+constexpr size_t kMaxGraphs = 8;
+
+static int nbas_bucket(int N) { return (N + 127) / 128; }
+static int npair_bucket(int64_t P) { return P <= 16384 ? 0 : (P <= 32768 ? 1 : 2); }
+
+static const spx_tune_entry* find_tune(const spx_ctx* ctx, int N, int64_t P, int nw) {
+  const int nb = nbas_bucket(N), pb = npair_bucket(P);
+  for (const auto& e : ctx->tune)
+    if (e.nbas_bucket == nb && e.npair_bucket == pb && e.nw == nw) return &e;
+  return nullptr;
+}
+
+static void store_tune(spx_ctx* ctx, const spx_tune_entry& t) {
+  for (auto& e : ctx->tune)
+    if (e.nbas_bucket == t.nbas_bucket && e.npair_bucket == t.npair_bucket && e.nw == t.nw) {
+      e = t;
+      return;
+    }
+  ctx->tune.push_back(t);
+}
+
+struct QPlan {
+  int variant, slab;
+  int64_t chunk;     // pairs per chunk (a multiple of the slab, so slabs match per-q calls)
+  size_t w_bytes, g_bytes, s_bytes;
+};
+
+static QPlan plan_q(const spx_ctx* ctx, const spx_q_desc& q, int nw, int precision) {
+  QPlan p;
+  p.variant = q.variant;
+  p.slab = q.slab_pairs;
+  if (precision == SPX_SPLIT && (p.variant == 0 || p.slab == 0)) {
+    const spx_tune_entry* t = find_tune(ctx, q.nbas, q.npair, nw);
+    if (p.variant == 0)
+      p.variant = t ? t->variant
+                    : (ctx->opt.split_variant ? ctx->opt.split_variant : kDefaultVariant);
+    if (p.slab == 0) p.slab = t ? t->slab_pairs : kDefaultSlab;
+  }
+  if (p.slab <= 0) p.slab = kDefaultSlab;
+  p.slab = std::max(64, std::min(kDefaultSlab, p.slab / 64 * 64));
+  p.chunk = std::min<int64_t>(q.npair, kChunkSlabs * p.slab);
+  p.chunk = std::max<int64_t>(p.chunk, 1);
+  const int64_t ld = (int64_t)align_up((size_t)p.chunk, 16);
+  p.w_bytes = align_up(sizeof(double) * (size_t)ld * nw, 256);
+  p.g_bytes = q.cprod ? 0 : align_up(sizeof(double2) * (size_t)ld * q.nbas, 256);
+  p.s_bytes = precision == SPX_SPLIT ? split_workspace_bytes(p.chunk, q.nbas, nw, p.slab) : 0;
+  return p;
+}
+
+// FNV-1a over the bytes that define a batch schedule
+static uint64_t fnv(uint64_t h, const void* p, size_t n) {
+  const unsigned char* b = (const unsigned char*)p;
+  for (size_t i = 0; i < n; ++i) {
+    h ^= b[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+// Enqueues the whole schedule on `s`.
+static int enqueue_batch(spx_ctx* ctx, int nq, const spx_q_desc* q, const QPlan* pl, int nw,
+                         const double* omega, int precision, char* ws, cudaStream_t s,
+                         int* launches) {
+  for (int i = 0; i < nq; ++i) {
+    const spx_q_desc& d = q[i];
+    const QPlan& p = pl[i];
+    if (d.npair == 0 || d.nbas == 0) continue;
+    double* W = (double*)ws;
+    double2* G = (double2*)(ws + p.w_bytes);
+    void* sws = p.s_bytes ? (void*)(ws + p.w_bytes + p.g_bytes) : nullptr;
+    for (int64_t p0 = 0; p0 < d.npair; p0 += p.chunk) {
+      const int64_t len = std::min<int64_t>(p.chunk, d.npair - p0);
+      const int64_t ldw = (int64_t)align_up((size_t)len, 16);
+      const double2* M;
+      int64_t ldc;
+      int rc;
+      if (d.cprod) {
+        M = reinterpret_cast<const double2*>(d.cprod) + p0;
+        ldc = d.ldc;
+      } else {
+        ldc = ldw;
+        if ((rc = launch_gen_cmatrix_rows(ctx, d.seed, d.stream_id, d.npair, p0, len, d.nbas, ldc,
+                                          d.m_scale, G, s)))
+          return rc;
+        ++*launches;
+        M = G;
+      }
+      if ((rc = launch_weights(ctx, len, ldw, d.ediff + p0, d.wscale ? d.wscale + p0 : nullptr,
+                               d.scale_all, nw, omega, W, s)))
+        return rc;
+      ++*launches;
+      if (precision == SPX_SPLIT) {
+        rc = split_chi0_slab(ctx, M, ldc, len, d.nbas, W, ldw, nw,
+                             reinterpret_cast<double2*>(d.susceph), sws, p.s_bytes, s, launches,
+                             p.variant, p.slab);
+      } else {
+        rc = launch_chi0_fp64(ctx, M, ldc, len, d.nbas, W, ldw, nw,
+                              reinterpret_cast<double2*>(d.susceph), s, 8);
+        ++*launches;
+      }
+      if (rc) return rc;
+    }
+  }
+  return SPX_OK;
+}
+
+}  // namespace spx
+
+using namespace spx;
+
+extern "C" int spx_chi0_batched(spx_ctx* ctx, int32_t nq, const spx_q_desc* q, int32_t nw,
+                                const double* omega, int32_t precision, int32_t flags,
+                                void* stream, spx_chi0_stats* stats) {
+  if (!ctx) return SPX_EINVAL;
+  if (nq < 0 || nw < 0) return set_error(ctx, SPX_EINVAL, "negative size");
+  if (nq > 0 && !q) return set_error(ctx, SPX_EINVAL, "null q list");
+  if (precision != SPX_FP64 && precision != SPX_SPLIT)
+    return set_error(ctx, SPX_EINVAL, "unknown precision");
+  double flops = 0;
+  for (int i = 0; i < nq; ++i) {
+    const spx_q_desc& d = q[i];
+    const std::string at = " in q " + std::to_string(i);
+    if (d.nbas < 0 || d.npair < 0) return set_error(ctx, SPX_EINVAL, "negative size" + at);
+    if (d.nbas > 46340) return set_error(ctx, SPX_EINVAL, "nbas too large" + at);
+    if (d.slab_pairs < 0 || d.variant < 0 || d.variant > 2)
+      return set_error(ctx, SPX_EINVAL, "bad variant or slab" + at);
+    if (d.npair > 0 && d.nbas > 0 && nw > 0) {
+      if (!d.ediff || !d.susceph || !omega) return set_error(ctx, SPX_EINVAL, "null array" + at);
+      if (d.cprod && d.ldc < d.npair) return set_error(ctx, SPX_EINVAL, "ldc < npair" + at);
+    }
+    flops += 8.0 * (double)d.nbas * d.nbas * (double)d.npair * nw;
+  }
+  cudaSetDevice(ctx->device);
+  auto t0 = std::chrono::steady_clock::now();
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->precision = precision;
+    stats->flops = flops;
+  }
+  if (nq == 0 || nw == 0) return SPX_OK;
+  int rc;
+  // tune the buckets the table lacks, before anything is captured
+  if ((flags & SPX_BATCH_AUTOTUNE) && precision == SPX_SPLIT) {
+    for (int i = 0; i < nq; ++i)
+      if (q[i].npair > 0 && q[i].nbas > 0 && (q[i].variant == 0 || q[i].slab_pairs == 0) &&
+          !find_tune(ctx, q[i].nbas, q[i].npair, nw))
+        if ((rc = spx_autotune_split(ctx, q[i].nbas, q[i].npair, nw, nullptr))) return rc;
+  }
+  std::vector<QPlan> pl(nq);
+  size_t need = 0;
+  for (int i = 0; i < nq; ++i) {
+    pl[i] = plan_q(ctx, q[i], nw, precision);
+    need = std::max(need, pl[i].w_bytes + pl[i].g_bytes + pl[i].s_bytes);
+  }
+  if ((rc = ensure_workspace(ctx, need + 1024))) return rc;
+  cudaStream_t s = pick_stream(ctx, stream);
+  int launches = 0;
+  cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+  if (stats) cudaEventRecord(e0, s);
+  const bool timing = ctx->timing;
+  ctx->timing = false;
+  if (flags & SPX_BATCH_NOGRAPH) {
+    rc = enqueue_batch(ctx, nq, q, pl.data(), nw, omega, precision, (char*)ctx->ws, s, &launches);
+  } else {
+    uint64_t key = 1469598103934665603ull;
+    key = fnv(key, &nq, sizeof(nq));
+    key = fnv(key, q, sizeof(spx_q_desc) * nq);
+    key = fnv(key, &nw, sizeof(nw));
+    key = fnv(key, &omega, sizeof(omega));
+    key = fnv(key, &precision, sizeof(precision));
+    key = fnv(key, &ctx->ws, sizeof(ctx->ws));
+    key = fnv(key, &ctx->ws_bytes, sizeof(ctx->ws_bytes));
+    for (const QPlan& p : pl) key = fnv(key, &p, sizeof(p));
+    spx_ctx::BatchGraph* hit = nullptr;
+    for (auto& g : ctx->graphs)
+      if (g.key == key) hit = &g;
+    if (!hit) {
+      // capture on the context stream; the preparation stream joins through events
+      cudaStream_t cs = ctx->stream;
+      cudaGraph_t graph = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      if ((rc = check_cuda(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed),
+                           "begin capture"))) {
+        ctx->timing = timing;
+        return rc;
+      }
+      int cap_launches = 0;
+      rc = enqueue_batch(ctx, nq, q, pl.data(), nw, omega, precision, (char*)ctx->ws, cs,
+                         &cap_launches);
+      cudaError_t ee = cudaStreamEndCapture(cs, &graph);
+      if (!rc) rc = check_cuda(ctx, ee, "end capture");
+      if (!rc) rc = check_cuda(ctx, cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+      if (rc) {
+        cudaGetLastError();
+        if (graph) cudaGraphDestroy(graph);
+        ctx->timing = timing;
+        return rc;
+      }
+      if (ctx->graphs.size() >= kMaxGraphs) {
+        auto old = std::min_element(ctx->graphs.begin(), ctx->graphs.end(),
+                                    [](const spx_ctx::BatchGraph& a, const spx_ctx::BatchGraph& b) {
+                                      return a.last_use < b.last_use;
+                                    });
+        cudaGraphExecDestroy(old->exec);
+        cudaGraphDestroy(old->graph);
+        ctx->graphs.erase(old);
+      }
+      ctx->graphs.push_back({key, graph, exec, 0});
+      hit = &ctx->graphs.back();
+      launches = cap_launches;
+    }
+    hit->last_use = ++ctx->graph_clock;
+    rc = check_cuda(ctx, cudaGraphLaunch(hit->exec, s), "graph launch");
+    if (!launches) {
+      // a replay: count the kernel nodes of the graph
+      size_t n = 0;
+      cudaGraphGetNodes(hit->graph, nullptr, &n);
+      std::vector<cudaGraphNode_t> nodes(n);
+      if (n) cudaGraphGetNodes(hit->graph, nodes.data(), &n);
+      for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++launches;
+      }
+    }
+  }
+  ctx->timing = timing;
+  if (rc) return rc;
+  if (stats) {
+    cudaEventRecord(e1, s);
+    rc = collect_status(ctx, s, "chi0_batched");
+    if (rc) return rc;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    stats->ms_gram = ms;  // device time of the whole batch
+    stats->kernel_launches = launches;
+    stats->ms_total =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return SPX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// autotuner
+
+extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
+                                  spx_tune_entry* out) {
+  if (!ctx) return SPX_EINVAL;
+  if (nbas <= 0 || npair <= 0 || nw <= 0) return set_error(ctx, SPX_EINVAL, "empty probe");
+  if (nbas > 46340) return set_error(ctx, SPX_EINVAL, "nbas too large");
+  cudaSetDevice(ctx->device);
+  const int64_t P = std::min<int64_t>(npair, 2 * (int64_t)kDefaultSlab);
+  const int64_t ld = (int64_t)align_up((size_t)P, 16);
+  const int64_t npack = (int64_t)nbas * (nbas + 1) / 2;
+  const int slabs[2] = {16384, 32768};
+  size_t sws = 0;
+  for (int sl : slabs) sws = std::max(sws, split_workspace_bytes(P, nbas, nw, sl));
+  const size_t m_bytes = align_up(sizeof(double2) * (size_t)ld * nbas, 256);
+  const size_t o_bytes = align_up(sizeof(double2) * (size_t)npack * nw, 256);
+  const size_t e_bytes = align_up(sizeof(double) * (size_t)ld, 256);
+  const size_t w_bytes = align_up(sizeof(double) * (size_t)ld * nw, 256);
+  const size_t om_bytes = align_up(sizeof(double) * (size_t)nw, 256);
+  int rc = ensure_workspace(ctx, m_bytes + o_bytes + e_bytes + w_bytes + om_bytes + sws + 1024);
+  if (rc) return rc;
+  char* b = (char*)ctx->ws;
+  double2* M = (double2*)b;
+  double2* O = (double2*)(b += m_bytes);
+  double* E = (double*)(b += o_bytes);
+  double* W = (double*)(b += e_bytes);
+  double* OM = (double*)(b += w_bytes);
+  void* S = (void*)(b += om_bytes);
+  cudaStream_t s = ctx->stream;
+  // seeded probe: M ~ N(0,1)/sqrt(N), energy differences 3 N(0,1), frequencies 1..nw
+  if ((rc = launch_gen_cmatrix_rows(ctx, 0x5eed, 77, P, 0, P, nbas, ld,
+                                    1.0 / std::sqrt((double)nbas), M, s)) ||
+      (rc = launch_gen_normal(ctx, 0x5eed, 78, 0, P, 3.0, E, s)))
+    return rc;
+  std::vector<double> om(nw);
+  for (int f = 0; f < nw; ++f) om[f] = 1.0 + f;
+  if ((rc = check_cuda(ctx, cudaMemcpyAsync(OM, om.data(), sizeof(double) * nw,
+                                            cudaMemcpyHostToDevice, s), "probe")) ||
+      (rc = check_cuda(ctx, cudaStreamSynchronize(s), "probe")))
+    return rc;
+  if ((rc = launch_weights(ctx, P, ld, E, nullptr, 1.0, nw, OM, W, s))) return rc;
+  spx_tune_entry best{};
+  best.nbas_bucket = nbas_bucket(nbas);
+  best.npair_bucket = npair_bucket(npair);
+  best.nw = nw;
+  best.tflops = -1;
+  const double flops = 8.0 * (double)nbas * nbas * (double)P * nw;
+  cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+  for (int variant = 1; variant <= 2; ++variant)
+    for (int sl : slabs) {
+      if (sl == 32768 && npair <= 16384) continue;  // one slab either way
+      int launches = 0;
+      float best_ms = 1e30f;
+      for (int rep = 0; rep < 2; ++rep) {  // the first run warms up
+        cudaEventRecord(e0, s);
+        rc = split_chi0_slab(ctx, M, ld, P, nbas, W, ld, nw, O, S, sws, s, &launches, variant, sl);
+        if (rc) return rc;
+        cudaEventRecord(e1, s);
+        if ((rc = collect_status(ctx, s, "autotune"))) return rc;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep) best_ms = std::min(best_ms, ms);
+      }
+      const double tf = flops / (best_ms * 1e-3) / 1e12;
+      if (tf > best.tflops) {
+        best.tflops = tf;
+        best.variant = variant;
+        best.slab_pairs = sl;
+      }
+    }
+  store_tune(ctx, best);
+  if (out) *out = best;
+  return SPX_OK;
+}
+
+extern "C" int spx_tune_lookup(const spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
+                               spx_tune_entry* out) {
+  if (!ctx) return SPX_EINVAL;
+  const spx_tune_entry* t = find_tune(ctx, nbas, npair, nw);
+  if (!t) return SPX_ENOTSUP;
+  if (out) *out = *t;
+  return SPX_OK;
+}
+
+extern "C" int spx_tune_save(const spx_ctx* ctx, const char* path) {
+  if (!ctx || !path) return SPX_EINVAL;
+  FILE* f = fopen(path, "w");
+  if (!f) return SPX_EINVAL;
+  cudaDeviceProp prop;
+  const bool have = cudaGetDeviceProperties(&prop, ctx->device) == cudaSuccess;
+  fprintf(f,
+          "{\n  \"format\": \"spexgpu-tune-1\",\n  \"device\": \"%s\",\n  \"sms\": %d,\n"
+          "  \"entries\": [",
+          have ? prop.name : "unknown", ctx->num_sms);
+  for (size_t i = 0; i < ctx->tune.size(); ++i) {
+    const spx_tune_entry& e = ctx->tune[i];
+    fprintf(f,
+            "%s\n    {\"nbas_bucket\": %d, \"npair_bucket\": %d, \"nw\": %d, \"variant\": %d, "
+            "\"slab_pairs\": %d, \"tflops\": %.3f}",
+            i ? "," : "", e.nbas_bucket, e.npair_bucket, e.nw, e.variant, e.slab_pairs, e.tflops);
+  }
+  fprintf(f, "\n  ]\n}\n");
+  return fclose(f) == 0 ? SPX_OK : SPX_EINVAL;
+}
+
+static bool json_field(const std::string& obj, const char* key, double* v) {
+  const std::string k = std::string("\"") + key + "\"";
+  size_t p = obj.find(k);
+  if (p == std::string::npos) return false;
+  p = obj.find(':', p + k.size());
+  if (p == std::string::npos) return false;
+  return sscanf(obj.c_str() + p + 1, " %lf", v) == 1;
+}
+
+extern "C" int spx_tune_load(spx_ctx* ctx, const char* path) {
+  if (!ctx || !path) return SPX_EINVAL;
+  FILE* f = fopen(path, "r");
+  if (!f) return set_error(ctx, SPX_EINVAL, std::string("cannot open ") + path);
+  std::string txt;
+  char buf[4096];
+  size_t n;
+  while ((n = fread(buf, 1, sizeof(buf), f)) > 0) txt.append(buf, n);
+  fclose(f);
+  if (txt.find("\"spexgpu-tune-1\"") == std::string::npos)
+    return set_error(ctx, SPX_EINVAL, "not a tuning table");
+  size_t p = txt.find("\"entries\"");
+  if (p == std::string::npos) return set_error(ctx, SPX_EINVAL, "tuning table without entries");
+  std::vector<spx_tune_entry> got;
+  while ((p = txt.find('{', p + 1)) != std::string::npos) {
+    const size_t e = txt.find('}', p);
+    if (e == std::string::npos) break;
+    const std::string obj = txt.substr(p, e - p + 1);
+    double nb, pb, nw, var, sl, tf = 0;
+    if (!json_field(obj, "nbas_bucket", &nb) || !json_field(obj, "npair_bucket", &pb) ||
+        !json_field(obj, "nw", &nw) || !json_field(obj, "variant", &var) ||
+        !json_field(obj, "slab_pairs", &sl))
+      return set_error(ctx, SPX_EINVAL, "malformed tuning entry");
+    json_field(obj, "tflops", &tf);
+    if (var < 1 || var > 2 || sl < 64 || sl > 32768 || nb < 1 || nw < 1 || pb < 0 || pb > 2)
+      return set_error(ctx, SPX_EINVAL, "tuning entry out of range");
+    spx_tune_entry t{};
+    t.nbas_bucket = (int)nb;
+    t.npair_bucket = (int)pb;
+    t.nw = (int)nw;
+    t.variant = (int)var;
+    t.slab_pairs = (int)sl;
+    t.tflops = tf;
+    got.push_back(t);
+    p = e;
+  }
+  for (const auto& t : got) store_tune(ctx, t);  // all or nothing
+  return SPX_OK;
+}

@@ -776,9 +776,10 @@ struct SplitLayout {
   size_t a_bytes, b_bytes, s_bytes, w_bytes;
 };
 
-static SplitLayout split_layout(int64_t P, int N, int nw) {
+// slab: band pairs per exact int32 slab, a multiple of SP_KB in [SP_KB, SP_SLAB]
+static SplitLayout split_layout(int64_t P, int N, int nw, int slab = SP_SLAB) {
   SplitLayout L;
-  L.Ps = std::min<int64_t>((int64_t)align_up((size_t)std::max<int64_t>(P, 1), SP_KB), SP_SLAB);
+  L.Ps = std::min<int64_t>((int64_t)align_up((size_t)std::max<int64_t>(P, 1), SP_KB), slab);
   L.nblk = (N + SP_TILE - 1) / SP_TILE;
   // an even number of 64-blocks, so a CTA pair's second A tile always exists
   L.R = (int64_t)((L.nblk + 1) / 2 * 2) * SP_ROWS;
@@ -791,24 +792,36 @@ static SplitLayout split_layout(int64_t P, int N, int nw) {
 
 // Two operand buffers when there is more than one slab: slab s+1 is quantized
 // while slab s accumulates.
-static int split_nbuf(int64_t P) { return P > SP_SLAB ? 2 : 1; }
+static int split_nbuf(int64_t P, int slab = SP_SLAB) { return P > slab ? 2 : 1; }
 
+static int clamp_slab(int slab) {
+  if (slab <= 0) return SP_SLAB;
+  return (int)std::min<int64_t>(SP_SLAB, std::max<int64_t>(SP_KB, slab / SP_KB * SP_KB));
+}
+
+size_t split_workspace_bytes(int64_t P, int N, int nw, int slab) {
+  slab = clamp_slab(slab);
+  SplitLayout L = split_layout(P, N, nw, slab);
+  return split_nbuf(P, slab) * (L.a_bytes + L.b_bytes + L.s_bytes + L.w_bytes) + 1024;
+}
 size_t split_workspace_bytes(int64_t P, int N, int nw) {
-  SplitLayout L = split_layout(P, N, nw);
-  return split_nbuf(P) * (L.a_bytes + L.b_bytes + L.s_bytes + L.w_bytes) + 1024;
+  return split_workspace_bytes(P, N, nw, SP_SLAB);
 }
 
 void timing_mark(spx_ctx* ctx, cudaStream_t s, int kind);
 
+// variant: 1 one CTA per tile, 2 CTA pair, 0 the context's choice; slab: pairs per
+// exact int32 slab (0 = 32768).
 int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N, const double* W,
                     int64_t ldw, int nw, double2* out, void* ws, size_t ws_bytes,
-                    cudaStream_t stream, int* launches, cudaEvent_t /*prep_done*/) {
+                    cudaStream_t stream, int* launches, int variant, int slab) {
   if (P <= 0 || N <= 0 || nw <= 0) return SPX_OK;
-  SplitLayout L = split_layout(P, N, nw);
-  if (!ws || ws_bytes < split_workspace_bytes(P, N, nw))
+  slab = clamp_slab(slab);
+  SplitLayout L = split_layout(P, N, nw, slab);
+  if (!ws || ws_bytes < split_workspace_bytes(P, N, nw, slab))
     return set_error(ctx, SPX_EINVAL, "split workspace too small");
   uint8_t* base = (uint8_t*)align_up((size_t)ws, 1024);
-  const int nbuf = split_nbuf(P);
+  const int nbuf = split_nbuf(P, slab);
   const size_t set_bytes = L.a_bytes + L.b_bytes + L.s_bytes + L.w_bytes;
   int8_t* A[2];
   int8_t* B[2];
@@ -825,7 +838,8 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
   // planes in HBM: [plane][k-block][row][K bytes]; TMA dims (K, row, k-block, plane)
   // with increasing strides; a box (K, rows, 1, planes) lands as [plane][row][K]
   const uint64_t nkb = (uint64_t)(L.Ps / SP_KB);
-  const bool pair = ctx->opt.split_variant != 1;  // 0 (auto) and 2 select the CTA pair
+  if (variant == 0) variant = ctx->opt.split_variant;
+  const bool pair = variant != 1;  // 0 (auto) and 2 select the CTA pair
   CUtensorMap mapA[2], mapB[2];
   for (int b = 0; b < nbuf; ++b) {
     const uint64_t sta[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};

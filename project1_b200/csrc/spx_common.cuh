@@ -34,6 +34,17 @@ struct spx_ctx {
   std::vector<cudaEvent_t> mark_pool;
   std::vector<int> mark_kind;
   size_t nmarks = 0;
+  // split-path tuning table, one entry per (N bucket, pair bucket, nw)
+  std::vector<spx_tune_entry> tune;
+  // captured batched schedules, keyed by the batch signature (least recently used first out)
+  struct BatchGraph {
+    uint64_t key;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    uint64_t last_use;
+  };
+  std::vector<BatchGraph> graphs;
+  uint64_t graph_clock = 0;
 };
 
 namespace spx {

@@ -64,13 +64,16 @@ __global__ void gen_normal_kernel(uint64_t seed, uint32_t sid, int64_t offset, i
 
 // Complex matrix: element (p, c) re/im = stream elements 2*rows*(col0+c) + 2p + {0,1}.
 // One thread per complex element; a Philox block yields exactly that pair.
-__global__ void gen_cmatrix_kernel(uint64_t seed, uint32_t sid, int64_t rows, int64_t cols,
-                                   int64_t ld, int64_t col0, double scale, double2* out) {
+// out[c*ld + p] = element (p0 + p, col0 + c) of a (rows_total x ...) stream matrix,
+// p < rows: rows [p0, p0+rows) of its columns [col0, col0+cols).
+__global__ void gen_cmatrix_kernel(uint64_t seed, uint32_t sid, int64_t rows_total, int64_t p0,
+                                   int64_t rows, int64_t cols, int64_t ld, int64_t col0,
+                                   double scale, double2* out) {
   const int64_t total = rows * cols;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t c = t / rows, p = t - c * rows;
-    const uint64_t e = (uint64_t)(2 * rows * (col0 + c) + 2 * p);
+    const uint64_t e = (uint64_t)(2 * rows_total * (col0 + c) + 2 * (p0 + p));
     double z0, z1;
     normal_pair(seed, sid, e >> 1, &z0, &z1);  // e is even: (z0, z1) = elements e, e+1
     out[c * ld + p] = make_double2(__dmul_rn(scale, z0), __dmul_rn(scale, z1));
@@ -90,8 +93,19 @@ int launch_gen_cmatrix(spx_ctx* ctx, uint64_t seed, uint32_t sid, int64_t rows, 
                        cudaStream_t stream) {
   if (rows <= 0 || cols <= 0) return SPX_OK;
   int grid = (int)std::min<int64_t>((rows * cols + 255) / 256, (int64_t)ctx->num_sms * 32);
-  gen_cmatrix_kernel<<<grid, 256, 0, stream>>>(seed, sid, rows, cols, ld, col0, scale,
+  gen_cmatrix_kernel<<<grid, 256, 0, stream>>>(seed, sid, rows, 0, rows, cols, ld, col0, scale,
                                                reinterpret_cast<double2*>(out));
+  return check_cuda(ctx, cudaGetLastError(), "gen_cmatrix_kernel launch");
+}
+
+// Rows [p0, p0+rows) of the generated (rows_total x cols) matrix, into out (ld >= rows).
+int launch_gen_cmatrix_rows(spx_ctx* ctx, uint64_t seed, uint32_t sid, int64_t rows_total,
+                            int64_t p0, int64_t rows, int64_t cols, int64_t ld, double scale,
+                            double2* out, cudaStream_t stream) {
+  if (rows <= 0 || cols <= 0) return SPX_OK;
+  int grid = (int)std::min<int64_t>((rows * cols + 255) / 256, (int64_t)ctx->num_sms * 32);
+  gen_cmatrix_kernel<<<grid, 256, 0, stream>>>(seed, sid, rows_total, p0, rows, cols, ld, 0,
+                                               scale, out);
   return check_cuda(ctx, cudaGetLastError(), "gen_cmatrix_kernel launch");
 }
 

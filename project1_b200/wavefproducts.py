@@ -12,7 +12,8 @@ src/trafo.f:514-569); here they are explicit device arrays:
   cprod     complex128 (ncol, ldc) row-major == Fortran (ldc, ncol); rows
             p = n' + nunocc*(n + nocc*k), as src/susceptibility.f:861-865 orders them.
 
-Both calls ADD into cprod. Descriptors are dicts as built by
+Both calls ADD into cprod. Calls on torch tensors are ordered on torch's current
+stream unless a stream is given. Descriptors are dicts as built by
 project1_b200.inputs.mt_basis / pw_basis.
 """
 from __future__ import annotations
@@ -58,7 +59,14 @@ class PwDesc:
                                   self.cstep.ctypes.data, float(pw["vol"]))
 
 
-def _stream(stream):
+def _stream(stream, like=None):
+    """The stream a call is ordered on: the given one, else torch's current stream of
+    the tensor `like` (so the call is ordered after the torch work that made its inputs)."""
+    if stream is None and like is not None and hasattr(like, "is_cuda") and like.is_cuda:
+        import torch
+        # torch's default stream has handle 0, which the C ABI reads as "the context
+        # stream": name it as cudaStreamLegacy (handle 1) instead
+        stream = torch.cuda.current_stream(like.device).cuda_stream or 1
     return None if stream is None else C.c_void_p(int(stream))
 
 
@@ -70,7 +78,7 @@ def wavefproducts2_mt(ctx: Context, mt, cmt_occ, cmt_unocc, cprod, stream=None) 
     if cmt_occ.shape[2:] != (d.natom, d.maxlm) or cmt_unocc.shape[2:] != (d.natom, d.maxlm):
         raise ValueError("coefficient arrays must be (nk, nb, natom, maxlm)")
     rc = ctx.lib.spx_wfprod_mt_dev(ctx.handle, C.byref(d.c), nk, nocc, nunocc, _ptr(cmt_occ),
-                                   _ptr(cmt_unocc), _ptr(cprod), cprod.shape[1], _stream(stream))
+                                   _ptr(cmt_unocc), _ptr(cprod), cprod.shape[1], _stream(stream, cprod))
     ctx._check(rc, "spx_wfprod_mt_dev")
 
 
@@ -82,7 +90,7 @@ def wavefproducts2_pw(ctx: Context, pw, cpw_occ, cpw_unocc, cprod, col0: int,
     nunocc = cpw_unocc.shape[1]
     rc = ctx.lib.spx_wfprod_pw_dev(ctx.handle, C.byref(d.c), nk, nocc, nunocc, _ptr(cpw_occ),
                                    _ptr(cpw_unocc), _ptr(cprod), cprod.shape[1], col0,
-                                   _stream(stream))
+                                   _stream(stream, cprod))
     ctx._check(rc, "spx_wfprod_pw_dev")
 
 
@@ -98,7 +106,7 @@ def chi0_from_coeffs(ctx: Context, mt, pw, cmt_occ, cmt_unocc, cpw_occ, cpw_unoc
     rc = ctx.lib.spx_chi0_from_coeffs_dev(
         ctx.handle, C.byref(dm.c), C.byref(dp.c), nk, nocc, nunocc, _ptr(cmt_occ),
         _ptr(cmt_unocc), _ptr(cpw_occ), _ptr(cpw_unocc), _ptr(ediff), _ptr(wscale), scale_all,
-        omega.shape[0], _ptr(omega), PRECISIONS[precision], _ptr(susceph), _stream(stream),
+        omega.shape[0], _ptr(omega), PRECISIONS[precision], _ptr(susceph), _stream(stream, susceph),
         C.byref(st) if st is not None else None)
     ctx._check(rc, "spx_chi0_from_coeffs_dev")
     return _stats(st) if st is not None else None

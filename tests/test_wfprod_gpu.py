@@ -166,7 +166,8 @@ def test_chi0_from_coeffs_equals_products_then_accumulate(ctx):
     wavefproducts2_mt(ctx, mt, _dev(m1), _dev(m2), cp)
     wavefproducts2_pw(ctx, pw, _dev(p1), _dev(p2), cp, w.nbasp)
     a = torch.zeros((len(omega), npack(w.nbas)), dtype=torch.complex128, device=DEV)
-    ctx.chi0_accumulate_dev(cp, _dev(ediff), _dev(omega), a, precision="split", npair=w.npair)
+    ctx.chi0_accumulate_dev(cp, _dev(ediff), _dev(omega), a, precision="split", npair=w.npair,
+                            stream=torch.cuda.current_stream().cuda_stream or 1)
     b = torch.zeros_like(a)
     chi0_from_coeffs(ctx, mt, pw, _dev(m1), _dev(m2), _dev(p1), _dev(p2), _dev(ediff),
                      _dev(omega), b, precision="split")
