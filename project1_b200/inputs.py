@@ -216,3 +216,36 @@ def pw_coeffs(w: WfprodWorkload, pw: dict):
     c1 = (rng.standard_normal((w.nk, w.nocc, n1)) + 1j * rng.standard_normal((w.nk, w.nocc, n1))) * d1
     c2 = (rng.standard_normal((w.nk, w.nunocc, n2)) + 1j * rng.standard_normal((w.nk, w.nunocc, n2))) * d2
     return c1, c2
+
+
+# ---------------------------------------------------------------------------
+# batched uneven q points: 32 q with N_MB ~ U{600..1800}, band windows
+# occ ~ U{20..60} x unocc ~ U{150..500}, 64 k points, 24 frequencies, M generated
+# per q from its own Philox stream.
+
+@dataclass
+class BatchedWorkload:
+    name: str
+    nq: int = 32
+    nk: int = 64
+    nw: int = 24
+    nbas_range: tuple = (600, 1800)
+    occ_range: tuple = (20, 60)
+    unocc_range: tuple = (150, 500)
+    seed: int = SEED + 3
+
+
+BATCHED_CONFIGS = {"c3": BatchedWorkload("c3")}
+
+
+def batched_qs(w: BatchedWorkload) -> list:
+    """The per-q workloads, drawn once from the batch seed (inclusive ranges)."""
+    rng = np.random.default_rng([w.seed, 31])
+    out = []
+    for q in range(w.nq):
+        nbas = int(rng.integers(w.nbas_range[0], w.nbas_range[1] + 1))
+        nocc = int(rng.integers(w.occ_range[0], w.occ_range[1] + 1))
+        nunocc = int(rng.integers(w.unocc_range[0], w.unocc_range[1] + 1))
+        out.append(Chi0Workload(f"{w.name}q{q}", nbas, w.nk, nocc, nunocc, w.nw,
+                                seed=w.seed * 1000 + q, stream_id=1))
+    return out

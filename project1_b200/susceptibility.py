@@ -164,6 +164,55 @@ class Context:
                                     None if stream is None else C.c_void_p(int(stream)))
         self._check(rc, "spx_scale_dev")
 
+    # ---- many q points in one launch ---------------------------------------------
+
+    def chi0_batched(self, qs, omega, precision: str = "split", flags: int = 0, stream=None,
+                     stats: bool = False) -> Optional[dict]:
+        """Accumulates every q of `qs` (dicts, see below) in one launch of a cached graph.
+
+        Each dict: nbas, npair, ediff (device float64), susceph (device complex128
+        (nw, npack)), optionally cprod (device (nbas, ldc)) or seed/stream_id/m_scale
+        for on-device generation, wscale, scale_all, variant, slab_pairs.
+        Ordered on torch's current stream unless `stream` is given."""
+        arr = (_lib.spx_q_desc * max(len(qs), 1))()
+        for i, q in enumerate(qs):
+            d = arr[i]
+            d.nbas, d.npair = int(q["nbas"]), int(q["npair"])
+            d.variant, d.slab_pairs = int(q.get("variant", 0)), int(q.get("slab_pairs", 0))
+            cp = q.get("cprod")
+            d.cprod = None if cp is None else int(cp.data_ptr())
+            d.ldc = 0 if cp is None else int(cp.shape[1])
+            d.seed, d.stream_id = int(q.get("seed", 0)), int(q.get("stream_id", 0))
+            d.m_scale = float(q.get("m_scale", 1.0))
+            d.ediff = int(q["ediff"].data_ptr())
+            ws = q.get("wscale")
+            d.wscale = None if ws is None else int(ws.data_ptr())
+            d.scale_all = float(q.get("scale_all", 1.0))
+            d.susceph = int(q["susceph"].data_ptr())
+        st = _lib.spx_chi0_stats() if stats else None
+        rc = self.lib.spx_chi0_batched(self.handle, len(qs), arr, omega.shape[0], _ptr(omega),
+                                       PRECISIONS[precision], flags, torch_stream(stream, omega),
+                                       C.byref(st) if st is not None else None)
+        self._check(rc, "spx_chi0_batched")
+        return _stats(st) if st is not None else None
+
+    def autotune_split(self, nbas: int, npair: int, nw: int) -> dict:
+        e = _lib.spx_tune_entry()
+        self._check(self.lib.spx_autotune_split(self.handle, nbas, npair, nw, C.byref(e)),
+                    "spx_autotune_split")
+        return _stats(e)
+
+    def tune_lookup(self, nbas: int, npair: int, nw: int) -> Optional[dict]:
+        e = _lib.spx_tune_entry()
+        rc = self.lib.spx_tune_lookup(self.handle, nbas, npair, nw, C.byref(e))
+        return _stats(e) if rc == 0 else None
+
+    def tune_save(self, path: str) -> None:
+        self._check(self.lib.spx_tune_save(self.handle, str(path).encode()), "spx_tune_save")
+
+    def tune_load(self, path: str) -> None:
+        self._check(self.lib.spx_tune_load(self.handle, str(path).encode()), "spx_tune_load")
+
     def gen_cmatrix_dev(self, seed: int, stream_id: int, out, rows: int, col0: int = 0,
                         scale: float = 1.0, stream=None) -> None:
         """Fills torch complex128 (cols, ld) with the seeded normal matrix (see spx_gen_cmatrix_host)."""
@@ -171,6 +220,17 @@ class Context:
         rc = self.lib.spx_gen_cmatrix_dev(self.handle, seed, stream_id, rows, cols, ld, col0, scale,
                                           _ptr(out), None if stream is None else C.c_void_p(int(stream)))
         self._check(rc, "spx_gen_cmatrix_dev")
+
+
+def torch_stream(stream, like=None):
+    """The stream a call is ordered on: the given one, else torch's current stream of
+    the tensor `like` (so the call is ordered after the torch work that made its inputs)."""
+    if stream is None and like is not None and hasattr(like, "is_cuda") and like.is_cuda:
+        import torch
+        # torch's default stream has handle 0, which the C ABI reads as "the context
+        # stream": name it as cudaStreamLegacy (handle 1) instead
+        stream = torch.cuda.current_stream(like.device).cuda_stream or 1
+    return None if stream is None else C.c_void_p(int(stream))
 
 
 def _stats(st) -> dict:

@@ -24,7 +24,7 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from .susceptibility import PRECISIONS, Context, _ptr, _stats
+from .susceptibility import PRECISIONS, Context, _ptr, _stats, torch_stream
 
 
 class MtDesc:
@@ -59,15 +59,7 @@ class PwDesc:
                                   self.cstep.ctypes.data, float(pw["vol"]))
 
 
-def _stream(stream, like=None):
-    """The stream a call is ordered on: the given one, else torch's current stream of
-    the tensor `like` (so the call is ordered after the torch work that made its inputs)."""
-    if stream is None and like is not None and hasattr(like, "is_cuda") and like.is_cuda:
-        import torch
-        # torch's default stream has handle 0, which the C ABI reads as "the context
-        # stream": name it as cudaStreamLegacy (handle 1) instead
-        stream = torch.cuda.current_stream(like.device).cuda_stream or 1
-    return None if stream is None else C.c_void_p(int(stream))
+_stream = torch_stream
 
 
 def wavefproducts2_mt(ctx: Context, mt, cmt_occ, cmt_unocc, cprod, stream=None) -> None:

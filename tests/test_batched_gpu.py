@@ -1,0 +1,165 @@
+"""Many q points in one graph launch (K7) and the split-path autotuner."""
+import json
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+import oracle
+import project1_b200 as spx
+from project1_b200 import _lib, inputs
+from project1_b200.susceptibility import SpexGpuError, npack
+from chi0_util import normalized_error
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+SPLIT_TOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = spx.Context(0)
+    yield c
+    c.close()
+
+
+def _q(nbas, npair, nw, seed, generated, variant=2, slab=32768):
+    rng = np.random.default_rng(seed)
+    ed = rng.uniform(0.5, 40.0, npair)
+    ed[rng.choice(npair, max(1, npair // 100), replace=False)] = 2e-7
+    q = dict(nbas=nbas, npair=npair, variant=variant, slab_pairs=slab,
+             ediff=torch.from_numpy(ed).to(DEV), scale_all=0.25,
+             susceph=torch.zeros((nw, npack(nbas)), dtype=torch.complex128, device=DEV))
+    if generated:
+        q.update(seed=1000 + seed, stream_id=3, m_scale=1.0 / np.sqrt(nbas))
+    else:
+        m = spx.gen_cmatrix_host(1000 + seed, 3, npair, nbas, scale=1.0 / np.sqrt(nbas))
+        ldc = npair + 5
+        cp = torch.zeros((nbas, ldc), dtype=torch.complex128, device=DEV)
+        cp[:, :npair] = torch.from_numpy(np.ascontiguousarray(m.T)).to(DEV)
+        q.update(cprod=cp)
+    return q
+
+
+SHAPES = [(40, 300), (129, 5000), (200, 40000), (1, 7), (257, 33000)]
+
+
+def _per_q_reference(ctx, q, omega, precision):
+    """The same q through the single-q entry point on an explicit M."""
+    nbas, npair = q["nbas"], q["npair"]
+    if "cprod" in q:
+        cp = q["cprod"]
+    else:
+        cp = torch.empty((nbas, npair), dtype=torch.complex128, device=DEV)
+        ctx.gen_cmatrix_dev(q["seed"], q["stream_id"], cp, npair, scale=q["m_scale"])
+        ctx.synchronize()
+    out = torch.zeros_like(q["susceph"])
+    torch.cuda.synchronize()   # the context stream does not wait for torch's
+    ctx.chi0_accumulate_dev(cp, q["ediff"], omega, out, scale_all=q["scale_all"],
+                            precision=precision, npair=npair, stats=True)
+    return out
+
+
+@pytest.mark.parametrize("generated", [False, True])
+@pytest.mark.parametrize("precision", ["split", "fp64"])
+def test_batched_equals_per_q_calls(ctx, generated, precision):
+    omega = torch.from_numpy(inputs.frequencies(3)).to(DEV)
+    qs = [_q(n, p, 3, i, generated) for i, (n, p) in enumerate(SHAPES)]
+    st = ctx.chi0_batched(qs, omega, precision=precision, stats=True)
+    assert st["kernel_launches"] > len(qs)
+    for q in qs:
+        ref = _per_q_reference(ctx, q, omega, precision)
+        assert torch.equal(q["susceph"], ref), (q["nbas"], q["npair"])
+
+
+def test_batched_matches_oracle(ctx):
+    omega_h = inputs.frequencies(2)
+    omega = torch.from_numpy(omega_h).to(DEV)
+    qs = [_q(n, p, 2, 7 + i, True) for i, (n, p) in enumerate([(70, 900), (33, 2000), (150, 400)])]
+    ctx.chi0_batched(qs, omega, stats=True)
+    for q in qs:
+        m = spx.gen_cmatrix_host(q["seed"], q["stream_id"], q["npair"], q["nbas"], scale=q["m_scale"])
+        ref = oracle.chi0(m, oracle.weights(q["ediff"].cpu().numpy(), omega_h, None, q["scale_all"]),
+                          accurate=True)
+        emax, fro = normalized_error(q["susceph"].cpu().numpy().T, ref, q["nbas"])
+        assert emax <= SPLIT_TOL, (emax, fro)
+
+
+def test_graph_replay_repeats_the_result(ctx):
+    omega = torch.from_numpy(inputs.frequencies(3)).to(DEV)
+    qs = [_q(n, p, 3, 20 + i, True) for i, (n, p) in enumerate([(96, 3000), (300, 70000)])]
+    ctx.chi0_batched(qs, omega, stats=True)           # captures the graph
+    first = [q["susceph"].clone() for q in qs]
+    for q in qs:
+        q["susceph"].zero_()
+    st = ctx.chi0_batched(qs, omega, stats=True)      # replays it
+    assert st["kernel_launches"] > 0
+    for q, a in zip(qs, first):
+        assert torch.equal(q["susceph"], a)
+    # without a graph: the same bits again
+    for q in qs:
+        q["susceph"].zero_()
+    ctx.chi0_batched(qs, omega, flags=_lib.SPX_BATCH_NOGRAPH, stats=True)
+    for q, a in zip(qs, first):
+        assert torch.equal(q["susceph"], a)
+
+
+def test_variants_and_slabs_agree(ctx):
+    """Every tuning choice computes the same chi within the split bound."""
+    omega_h = inputs.frequencies(2)
+    omega = torch.from_numpy(omega_h).to(DEV)
+    outs = []
+    for variant, slab in [(1, 16384), (2, 16384), (1, 32768), (2, 4096)]:
+        q = _q(180, 50000, 2, 99, True, variant=variant, slab=slab)
+        ctx.chi0_batched([q], omega, stats=True)
+        outs.append(q["susceph"].cpu().numpy().T)
+    m = spx.gen_cmatrix_host(1099, 3, 50000, 180, scale=1 / np.sqrt(180))
+    ref = oracle.chi0(m, oracle.weights(q["ediff"].cpu().numpy(), omega_h, None, 0.25), accurate=True)
+    for o in outs:
+        emax, _ = normalized_error(o, ref, 180)
+        assert emax <= SPLIT_TOL
+
+
+def test_autotune_table_roundtrip(ctx, tmp_path):
+    e = ctx.autotune_split(200, 40000, 3)
+    assert e["variant"] in (1, 2) and e["slab_pairs"] in (16384, 32768) and e["tflops"] > 0
+    assert ctx.tune_lookup(200, 40000, 3) == e
+    assert ctx.tune_lookup(200, 40000, 4) is None
+    path = tmp_path / "tune.json"
+    ctx.tune_save(path)
+    doc = json.loads(path.read_text())
+    assert doc["format"] == "spexgpu-tune-1" and len(doc["entries"]) >= 1
+    other = spx.Context(0)
+    try:
+        assert other.tune_lookup(200, 40000, 3) is None
+        other.tune_load(path)
+        got = other.tune_lookup(200, 40000, 3)
+        assert got["variant"] == e["variant"] and got["slab_pairs"] == e["slab_pairs"]
+        bad = tmp_path / "bad.json"
+        bad.write_text('{"format": "spexgpu-tune-1", "entries": [{"nbas_bucket": 2, "variant": 9}]}')
+        with pytest.raises(SpexGpuError):
+            other.tune_load(bad)
+    finally:
+        other.close()
+
+
+def test_autotuned_batch(ctx):
+    omega = torch.from_numpy(inputs.frequencies(2)).to(DEV)
+    qs = [_q(n, p, 2, 40 + i, True, variant=0, slab=0) for i, (n, p) in enumerate([(260, 20000), (520, 9000)])]
+    ctx.chi0_batched(qs, omega, flags=_lib.SPX_BATCH_AUTOTUNE, stats=True)
+    for q in qs:
+        assert ctx.tune_lookup(q["nbas"], q["npair"], 2) is not None
+        assert torch.isfinite(torch.view_as_real(q["susceph"])).all()
+        assert q["susceph"].abs().max() > 0
+
+
+def test_batched_rejects_bad_descriptors(ctx):
+    omega = torch.from_numpy(inputs.frequencies(2)).to(DEV)
+    q = _q(40, 100, 2, 1, False)
+    with pytest.raises(SpexGpuError):
+        ctx.chi0_batched([dict(q, variant=3)], omega)
+    with pytest.raises(SpexGpuError):
+        ctx.chi0_batched([dict(q, npair=200)], omega)       # ldc 105 < npair
+    with pytest.raises(SpexGpuError):
+        ctx.chi0_batched([dict(q, nbas=50000)], omega)

@@ -94,3 +94,14 @@ def test_gaunt_table_density():
                         valid += abs(m + MM) <= l1
     frac = np.count_nonzero(g) / valid
     assert 0.04 < frac < 0.06, frac
+
+
+def test_batched_workload_draws():
+    w = inputs.BATCHED_CONFIGS["c3"]
+    qs = inputs.batched_qs(w)
+    assert len(qs) == 32
+    assert all(600 <= q.nbas <= 1800 and 20 <= q.nocc <= 60 and 150 <= q.nunocc <= 500 for q in qs)
+    assert all(q.nk == 64 and q.nw == 24 for q in qs)
+    assert len({q.seed for q in qs}) == 32
+    assert qs == inputs.batched_qs(w)        # reproducible
+    assert 5e15 < sum(q.flops for q in qs) < 1.2e16
