@@ -350,10 +350,130 @@ def run_ours(args):
             res["speedup_vs_fp64"] = value / fp64["value"]
         if world == 1 and args.cpu_budget > 0:
             res["cpu_baseline"] = cpu_baseline(w, budget_s=args.cpu_budget)
-        print(json.dumps(res))
     ctx.close()
+    del M
+    if rank == 0 and world == 1:
+        torch.cuda.empty_cache()
+        if args.products_steps > 0:
+            res["c4_products_chi0"] = bench_products(args, dev, stream)
+            torch.cuda.empty_cache()
+        if args.batched_steps > 0:
+            res["c3_batched"] = bench_batched(args, dev, stream)
+    if rank == 0:
+        print(json.dumps(res))
     if world > 1:
         dist.destroy_process_group()
+
+
+def bench_batched(args, dev, stream):
+    """32 uneven q points, M generated on the device slab by slab, all q in
+    one replayed CUDA graph per step (autotuned per (N, P) bucket in the warm-up)."""
+    import torch
+    import project1_b200 as spx
+    from project1_b200 import _lib, inputs
+    bw = inputs.BATCHED_CONFIGS["c3"]
+    qws = inputs.batched_qs(bw)
+    omega = torch.from_numpy(inputs.frequencies(bw.nw)).to(dev)
+    ctx = spx.Context(dev.index or 0)
+    qs = []
+    for qw in qws:
+        qs.append(dict(nbas=qw.nbas, npair=qw.npair, seed=qw.seed, stream_id=qw.stream_id,
+                       m_scale=qw.m_scale, ediff=torch.from_numpy(inputs.pair_ediff(qw)).to(dev),
+                       scale_all=1.0 / qw.nk,
+                       susceph=torch.zeros((bw.nw, spx.npack(qw.nbas)), dtype=torch.complex128,
+                                           device=dev)))
+    flops = sum(q.flops for q in qws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(args.batched_warmup):
+        for q in qs:
+            q["susceph"].zero_()
+        ctx.chi0_batched(qs, omega, flags=_lib.SPX_BATCH_AUTOTUNE if i == 0 else 0,
+                         stream=stream.cuda_stream, stats=True)
+    warm_s = time.perf_counter() - t0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kernels = 0
+    e0.record(stream)
+    for _ in range(args.batched_steps):
+        for q in qs:
+            q["susceph"].zero_()
+        st = ctx.chi0_batched(qs, omega, stream=stream.cuda_stream, stats=True)
+        kernels = st["kernel_launches"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.batched_steps
+    tune = [ctx.tune_lookup(q["nbas"], q["npair"], bw.nw) for q in qs]
+    res = {"workload": f"c3: {bw.nq} q, N_MB U{{{bw.nbas_range[0]}..{bw.nbas_range[1]}}}, "
+                       f"occ U{{{bw.occ_range[0]}..{bw.occ_range[1]}}} x unocc "
+                       f"U{{{bw.unocc_range[0]}..{bw.unocc_range[1]}}}, {bw.nk} k, {bw.nw} freqs, split",
+           "value": flops / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms,
+           "steps": args.batched_steps, "warmup": args.batched_warmup,
+           "warmup_s_incl_autotune_and_capture": warm_s, "flops_per_step": flops,
+           "npair_total": sum(q.npair for q in qws), "graph_launches_per_step": 1,
+           "kernels_per_step": kernels,
+           "tuned_choices": sorted({(t["nbas_bucket"], t["npair_bucket"], t["variant"], t["slab_pairs"])
+                                    for t in tune if t}),
+           "m_generated_on_device": True}
+    ctx.close()
+    return res
+
+
+def bench_products(args, dev, stream):
+    """wave-function products (MT Gaunt contraction + interstitial
+    convolution) and split chi0 in one call, M never leaving the device."""
+    import torch
+    import project1_b200 as spx
+    from project1_b200 import inputs
+    from project1_b200.wavefproducts import (MtDesc, PwDesc, chi0_from_coeffs, wavefproducts2_mt,
+                                             wavefproducts2_pw)
+    w = inputs.WFPROD_CONFIGS["c4"]
+    mt, pw = MtDesc(inputs.mt_basis(w)), PwDesc(inputs.pw_basis(w))
+    m1, m2 = inputs.mt_coeffs(w)
+    p1, p2 = inputs.pw_coeffs(w, {"gpt1": pw.gpt1, "gpt2": pw.gpt2})
+    D = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    m1, m2, p1, p2 = D(m1), D(m2), D(p1), D(p2)
+    ew = inputs.Chi0Workload("c4", w.nbas, w.nk, w.nocc, w.nunocc, w.nw, seed=w.seed)
+    ediff = D(inputs.pair_ediff(ew))
+    omega = D(inputs.frequencies(w.nw))
+    out = torch.zeros((w.nw, spx.npack(w.nbas)), dtype=torch.complex128, device=dev)
+    ctx = spx.Context(dev.index or 0)
+    sc = stream.cuda_stream
+
+    def timed(fn, warmup, steps):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def fused():
+        out.zero_()
+        chi0_from_coeffs(ctx, mt, pw, m1, m2, p1, p2, ediff, omega, out, scale_all=1.0 / w.nk,
+                         precision="split", stream=sc)
+    ms = timed(fused, args.products_warmup, args.products_steps)
+    st = chi0_from_coeffs(ctx, mt, pw, m1, m2, p1, p2, ediff, omega, out, scale_all=1.0 / w.nk,
+                          precision="split", stream=sc, stats=True)
+    cp = torch.zeros((w.nbas, w.npair), dtype=torch.complex128, device=dev)
+    mt_ms = timed(lambda: wavefproducts2_mt(ctx, mt, m1, m2, cp, stream=sc), 1, 2)
+    pw_ms = timed(lambda: wavefproducts2_pw(ctx, pw, p1, p2, cp, w.nbasp, stream=sc), 1, 2)
+    fl_mt = 8.0 * w.nunocc * w.maxlm * w.nocc * w.maxllm * w.nk * w.natom
+    fl_pw = 8.0 * w.nunocc * w.ngpt * w.nocc * w.ngptm * w.nk
+    res = {"workload": f"c4: {w.natom} atoms lmax {w.lcut} x {w.nrad} radial (maxlm {w.maxlm}), "
+                       f"{w.ngpt} PW, {w.ngptm} MPB PW, N_MB {w.nbas}, {w.nk} k, {w.nocc} x {w.nunocc} "
+                       f"bands, {w.nw} freqs; products FP64, chi0 split",
+           "value": w.flops / (ms * 1e-3) / 1e12, "unit": UNIT + " (chi0 flops over products + chi0 time)",
+           "ms_per_step": ms, "steps": args.products_steps, "warmup": args.products_warmup,
+           "chi0_kernel_ms": st["ms_gram"], "products_and_prep_ms": st["ms_prep"],
+           "mt_ms": mt_ms, "mt_tflops_fp64": fl_mt / (mt_ms * 1e-3) / 1e12,
+           "pw_ms": pw_ms, "pw_tflops_fp64": fl_pw / (pw_ms * 1e-3) / 1e12,
+           "kernels_per_step": st["kernel_launches"], "m_bytes_on_device": 16 * w.nbas * w.npair}
+    ctx.close()
+    return res
 
 
 def accuracy_check(ctx, w, M, ediff, omega, stream, ediff_h, omega_h, nsample=24):
@@ -420,6 +540,10 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=10.0)
     ap.add_argument("--no-check", dest="check", action="store_false")
+    ap.add_argument("--products-steps", type=int, default=3, help="configs[4] timed steps (0: skip)")
+    ap.add_argument("--products-warmup", type=int, default=3)
+    ap.add_argument("--batched-steps", type=int, default=1, help="configs[3] timed batches (0: skip)")
+    ap.add_argument("--batched-warmup", type=int, default=1)
     ap.add_argument("--precision", choices=["split", "fp64"], default=None,
                     help="force the measured path (profiling captures)")
     ap.add_argument("--kpts", type=int, default=0, help="override the k-point count (profiling)")

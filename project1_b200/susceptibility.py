@@ -137,7 +137,8 @@ class Context:
     def chi0_accumulate_dev(self, cprod, ediff, omega, susceph, wscale=None, scale_all: float = 1.0,
                             precision: str = "fp64", stream=None, npair: Optional[int] = None,
                             stats: bool = False) -> Optional[dict]:
-        """Device form on torch CUDA tensors.
+        """Device form on torch CUDA tensors, ordered on torch's current stream unless
+        `stream` is given.
 
         cprod: complex128 (nbas, ldc) row-major == Fortran (ldc, nbas); npair <= ldc.
         susceph: complex128 (nw, npack) row-major == Fortran (npack, nw).
@@ -148,20 +149,19 @@ class Context:
         st = _lib.spx_chi0_stats() if stats else None
         rc = self.lib.spx_chi0_accumulate_dev(
             self.handle, _ptr(cprod), ldc, npair, nbas, _ptr(ediff), _ptr(wscale), scale_all, nw,
-            _ptr(omega), PRECISIONS[precision], _ptr(susceph),
-            None if stream is None else C.c_void_p(int(stream)), C.byref(st) if st is not None else None)
+            _ptr(omega), PRECISIONS[precision], _ptr(susceph), torch_stream(stream, susceph),
+            C.byref(st) if st is not None else None)
         self._check(rc, "spx_chi0_accumulate_dev")
         return _stats(st) if st is not None else None
 
     def weights_dev(self, ediff, omega, w, wscale=None, scale_all: float = 1.0, stream=None) -> None:
         rc = self.lib.spx_weights_dev(self.handle, ediff.shape[0], _ptr(ediff), _ptr(wscale), scale_all,
                                       omega.shape[0], _ptr(omega), _ptr(w),
-                                      None if stream is None else C.c_void_p(int(stream)))
+                                      torch_stream(stream, w))
         self._check(rc, "spx_weights_dev")
 
     def scale_dev(self, z, factor: float, stream=None) -> None:
-        rc = self.lib.spx_scale_dev(self.handle, _ptr(z), z.numel(), factor,
-                                    None if stream is None else C.c_void_p(int(stream)))
+        rc = self.lib.spx_scale_dev(self.handle, _ptr(z), z.numel(), factor, torch_stream(stream, z))
         self._check(rc, "spx_scale_dev")
 
     # ---- many q points in one launch ---------------------------------------------
@@ -218,7 +218,7 @@ class Context:
         """Fills torch complex128 (cols, ld) with the seeded normal matrix (see spx_gen_cmatrix_host)."""
         cols, ld = out.shape
         rc = self.lib.spx_gen_cmatrix_dev(self.handle, seed, stream_id, rows, cols, ld, col0, scale,
-                                          _ptr(out), None if stream is None else C.c_void_p(int(stream)))
+                                          _ptr(out), torch_stream(stream, out))
         self._check(rc, "spx_gen_cmatrix_dev")
 
 
@@ -227,10 +227,12 @@ def torch_stream(stream, like=None):
     the tensor `like` (so the call is ordered after the torch work that made its inputs)."""
     if stream is None and like is not None and hasattr(like, "is_cuda") and like.is_cuda:
         import torch
-        # torch's default stream has handle 0, which the C ABI reads as "the context
-        # stream": name it as cudaStreamLegacy (handle 1) instead
-        stream = torch.cuda.current_stream(like.device).cuda_stream or 1
-    return None if stream is None else C.c_void_p(int(stream))
+        stream = torch.cuda.current_stream(like.device).cuda_stream
+    if stream is None:
+        return None
+    # handle 0 is the legacy default stream (torch's default stream), which the C ABI
+    # would read as "the context stream": name it as cudaStreamLegacy (handle 1)
+    return C.c_void_p(int(stream) or 1)
 
 
 def _stats(st) -> dict:
