@@ -33,6 +33,39 @@ module spex_gpu
     integer(c_int32_t) :: kernel_launches, precision
   end type
 
+  ! spx_mt_desc / spx_pw_desc: host descriptors of the product basis (c_loc of
+  ! Fortran arrays); the coefficient and cprod pointers of the _dev calls are
+  ! device addresses (e.g. from an OpenACC host_data or CUDA Fortran device array)
+  type, bind(c) :: spx_mt_desc
+    integer(c_int32_t) :: natom, lcut, nrad, lcutm, nradm, ld1
+    type(c_ptr) :: gaunt, integral, cexp
+  end type
+
+  type, bind(c) :: spx_pw_desc
+    integer(c_int32_t) :: ngpt1, ngpt2, ngptm, step_radius
+    type(c_ptr) :: gpt1, gpt2, gptm
+    integer(c_int32_t) :: gshift(3)
+    integer(c_int32_t) :: reserved = 0
+    type(c_ptr) :: cstep
+    real(c_double) :: vol
+  end type
+
+  type, bind(c) :: spx_q_desc
+    integer(c_int32_t) :: nbas, variant = 0
+    integer(c_int64_t) :: npair
+    integer(c_int32_t) :: slab_pairs = 0, reserved0 = 0
+    type(c_ptr) :: cprod                         ! device, or c_null_ptr = generated
+    integer(c_int64_t) :: ldc
+    integer(c_int64_t) :: seed                   ! uint64 in C
+    integer(c_int32_t) :: stream_id, reserved1 = 0
+    real(c_double) :: m_scale
+    type(c_ptr) :: ediff, wscale
+    real(c_double) :: scale_all
+    type(c_ptr) :: susceph
+  end type
+
+  integer(c_int), parameter :: SPX_BATCH_AUTOTUNE = 1, SPX_BATCH_NOGRAPH = 2
+
   interface
     integer(c_int) function spx_ctx_create(device, opt, ctx) bind(c, name='spx_ctx_create')
       import :: c_int, c_ptr, spx_options
@@ -67,6 +100,54 @@ module spex_gpu
       real(c_double), intent(in) :: omega(*)
       integer(c_int32_t), value :: precision
       complex(c_double_complex), intent(inout) :: susceph(*)
+      type(spx_chi0_stats), intent(out) :: stats
+    end function
+
+    ! replaces wavefproducts2_mt, src/wavefproducts.f:95-431 (device arrays)
+    integer(c_int) function spx_wfprod_mt_dev(ctx, mt, nk, nocc, nunocc, cmt_occ, cmt_unocc, &
+                                              cprod, ldc, stream) bind(c, name='spx_wfprod_mt_dev')
+      import :: c_int, c_int32_t, c_int64_t, c_ptr, spx_mt_desc
+      type(c_ptr), value :: ctx
+      type(spx_mt_desc), intent(in) :: mt
+      integer(c_int32_t), value :: nk, nocc, nunocc
+      type(c_ptr), value :: cmt_occ, cmt_unocc, cprod, stream
+      integer(c_int64_t), value :: ldc
+    end function
+
+    ! replaces the explicit-convolution wavefproducts2_pw, src/wavefproducts.f:760-997
+    integer(c_int) function spx_wfprod_pw_dev(ctx, pw, nk, nocc, nunocc, cpw_occ, cpw_unocc, &
+                                              cprod, ldc, col0, stream) bind(c, name='spx_wfprod_pw_dev')
+      import :: c_int, c_int32_t, c_int64_t, c_ptr, spx_pw_desc
+      type(c_ptr), value :: ctx
+      type(spx_pw_desc), intent(in) :: pw
+      integer(c_int32_t), value :: nk, nocc, nunocc, col0
+      type(c_ptr), value :: cpw_occ, cpw_unocc, cprod, stream
+      integer(c_int64_t), value :: ldc
+    end function
+
+    ! the packet loop src/susceptibility.f:751-1276 from coefficients to chi0
+    integer(c_int) function spx_chi0_from_coeffs_dev(ctx, mt, pw, nk, nocc, nunocc, cmt_occ, &
+        cmt_unocc, cpw_occ, cpw_unocc, ediff, wscale, scale_all, nw, omega, precision, susceph, &
+        stream, stats) bind(c, name='spx_chi0_from_coeffs_dev')
+      import :: c_int, c_int32_t, c_ptr, c_double, spx_mt_desc, spx_pw_desc, spx_chi0_stats
+      type(c_ptr), value :: ctx
+      type(spx_mt_desc), intent(in) :: mt
+      type(spx_pw_desc), intent(in) :: pw
+      integer(c_int32_t), value :: nk, nocc, nunocc, nw, precision
+      type(c_ptr), value :: cmt_occ, cmt_unocc, cpw_occ, cpw_unocc, ediff, wscale, omega, susceph
+      real(c_double), value :: scale_all
+      type(c_ptr), value :: stream
+      type(spx_chi0_stats), intent(out) :: stats
+    end function
+
+    ! the q loop around susceptibility, src/correlation.f:293-339
+    integer(c_int) function spx_chi0_batched(ctx, nq, q, nw, omega, precision, flags, stream, &
+                                             stats) bind(c, name='spx_chi0_batched')
+      import :: c_int, c_int32_t, c_ptr, spx_q_desc, spx_chi0_stats
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: nq, nw, precision, flags
+      type(spx_q_desc), intent(in) :: q(*)
+      type(c_ptr), value :: omega, stream
       type(spx_chi0_stats), intent(out) :: stats
     end function
   end interface
