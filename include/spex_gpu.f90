@@ -45,7 +45,7 @@ module spex_gpu
     integer(c_int32_t) :: ngpt1, ngpt2, ngptm, step_radius
     type(c_ptr) :: gpt1, gpt2, gptm
     integer(c_int32_t) :: gshift(3)
-    integer(c_int32_t) :: reserved = 0
+    integer(c_int32_t) :: nfft = 0               ! 0 explicit convolution, n: FFT branch
     type(c_ptr) :: cstep
     real(c_double) :: vol
   end type

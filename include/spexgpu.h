@@ -156,8 +156,9 @@ typedef struct spx_mt_desc {
   const double* cexp;       /* complex (natom): exp(-2 pi i q.R_a)                    */
 } spx_mt_desc;
 
-/* Interstitial part, replaces the explicit-convolution branch of
- * wavefproducts2_pw (src/wavefproducts.f:760-997) with the step function:
+/* Interstitial part, replaces wavefproducts2_pw with the step function: the
+ * explicit-convolution branch (src/wavefproducts.f:760-997) or, with nfft > 0,
+ * the FFT branch (:576-758), which computes the same sum on a grid:
  *   cpw0(G0) = sum_G1 cstep(G0 - G1) cpw_occ(G1),
  *   cprod(p, col0 + ig) += 1/sqrt(vol) * sum_ig2 cpw_unocc(ig2, n') * conj(cpw0(G2(ig2) - GM(ig) + g)).
  * gpt1 lists the G vectors of the occupied states (at k), gpt2 those of the
@@ -170,7 +171,9 @@ typedef struct spx_pw_desc {
   const int32_t* gpt2;      /* (3, ngpt2)                                             */
   const int32_t* gptm;      /* (3, ngptm)                                             */
   int32_t gshift[3];        /* backfolding vector g (src/wavefproducts.f:549-551)     */
-  int32_t reserved;
+  int32_t nfft;             /* 0: explicit convolution (:760-997); n > 0: the FFT
+                               branch (:576-758) on an n^3 grid, 2 <= n <= 64, at most
+                               16 distinct (G_M - g) mod n per axis, ngptm <= 4096   */
   const double* cstep;      /* complex (2sr+1)^3, x fastest                            */
   double vol;               /* unit-cell volume                                        */
 } spx_pw_desc;

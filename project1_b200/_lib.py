@@ -60,7 +60,7 @@ class spx_pw_desc(C.Structure):
         ("ngpt1", C.c_int32), ("ngpt2", C.c_int32), ("ngptm", C.c_int32),
         ("step_radius", C.c_int32),
         ("gpt1", C.c_void_p), ("gpt2", C.c_void_p), ("gptm", C.c_void_p),
-        ("gshift", C.c_int32 * 3), ("reserved", C.c_int32),
+        ("gshift", C.c_int32 * 3), ("nfft", C.c_int32),
         ("cstep", C.c_void_p), ("vol", C.c_double),
     ]
 

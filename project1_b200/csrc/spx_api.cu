@@ -530,7 +530,7 @@ int wfprod_mt_run(spx_ctx*, const spx_mt_desc*, int, int, int, const double2*, c
 int wfprod_pw_run(spx_ctx*, const spx_pw_desc*, int, int, int, const double2*, const double2*,
                   double2*, int64_t, int, void*, size_t, cudaStream_t, int*);
 size_t wfprod_mt_workspace(const spx_mt_desc*, int, int);
-size_t wfprod_pw_workspace(const spx_pw_desc*, int, int);
+size_t wfprod_pw_workspace(const spx_pw_desc*, int, int, int);
 }  // namespace spx
 
 extern "C" int spx_chi0_from_coeffs_dev(spx_ctx* ctx, const spx_mt_desc* mt,
@@ -566,7 +566,7 @@ extern "C" int spx_chi0_from_coeffs_dev(spx_ctx* ctx, const spx_mt_desc* mt,
   cudaStream_t s = pick_stream(ctx, stream);
   const int64_t ldc = (int64_t)align_up((size_t)npair, 16);
   const size_t m_bytes = align_up(sizeof(double2) * (size_t)ldc * nbas, 256);
-  const size_t prod_bytes = std::max(wfprod_mt_workspace(mt, nk, nocc), wfprod_pw_workspace(pw, nk, nocc));
+  const size_t prod_bytes = std::max(wfprod_mt_workspace(mt, nk, nocc), wfprod_pw_workspace(pw, nk, nocc, nunocc));
   const int64_t ldw = ldc;
   const size_t w_bytes = align_up(sizeof(double) * (size_t)ldw * nw, 256);
   const size_t s_bytes = precision == SPX_SPLIT ? split_workspace_bytes(npair, nbas, nw) : 0;

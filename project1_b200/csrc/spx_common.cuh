@@ -65,6 +65,24 @@ void timing_mark(spx_ctx* ctx, cudaStream_t s, int kind);
 // Sums the intervals between consecutive marks per kind (after a sync) and clears them.
 void timing_collect(spx_ctx* ctx, double* ms_prep, double* ms_gram);
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+// Carves 256-byte aligned pieces off a scratch range; ok turns false when it runs out.
+struct Carve {
+  char* p;
+  size_t left;
+  bool ok = true;
+  template <class T>
+  T* take(size_t n) {
+    const size_t bytes = align_up(sizeof(T) * std::max<size_t>(n, 1), 256);
+    if (bytes > left) {
+      ok = false;
+      return nullptr;
+    }
+    T* r = reinterpret_cast<T*>(p);
+    p += bytes;
+    left -= bytes;
+    return r;
+  }
+};
 inline cudaStream_t pick_stream(spx_ctx* ctx, void* s) {
   return s ? (cudaStream_t)s : ctx->stream;
 }

@@ -417,23 +417,7 @@ static GBox bounding_box(const int* g, int n) {
 // ---------------------------------------------------------------------------
 // workspace planning shared by the entry points
 
-struct Carve {
-  char* p;
-  size_t left;
-  bool ok = true;
-  template <class T>
-  T* take(size_t n) {
-    const size_t bytes = align_up(sizeof(T) * std::max<size_t>(n, 1), 256);
-    if (bytes > left) {
-      ok = false;
-      return nullptr;
-    }
-    T* r = reinterpret_cast<T*>(p);
-    p += bytes;
-    left -= bytes;
-    return r;
-  }
-};
+
 
 static size_t mt_fixed_bytes(const MtMap& mp) {
   return align_up(sizeof(int) * mp.rp.size(), 256) + align_up(sizeof(int) * std::max<size_t>(mp.ci.size(), 1), 256) +
@@ -564,7 +548,13 @@ static int plan_pw(spx_ctx* ctx, const spx_pw_desc* d, PwPlan* pl) {
   return SPX_OK;
 }
 
-size_t wfprod_pw_workspace(const spx_pw_desc* d, int nk, int nocc) {
+size_t wfprod_pw_fft_workspace(const spx_pw_desc* d, int nk, int nocc, int nunocc);
+int wfprod_pw_fft_run(spx_ctx* ctx, const spx_pw_desc* d, int nk, int nocc, int nunocc,
+                      const double2* c1, const double2* c2, double2* cprod, int64_t ldc, int col0,
+                      void* ws, size_t ws_bytes, cudaStream_t s, int* launches);
+
+size_t wfprod_pw_workspace(const spx_pw_desc* d, int nk, int nocc, int nunocc) {
+  if (d->nfft > 0) return wfprod_pw_fft_workspace(d, nk, nocc, nunocc);
   spx_ctx dummy;
   PwPlan pl;
   if (plan_pw(&dummy, d, &pl)) return 0;
@@ -581,6 +571,9 @@ size_t wfprod_pw_workspace(const spx_pw_desc* d, int nk, int nocc) {
 int wfprod_pw_run(spx_ctx* ctx, const spx_pw_desc* d, int nk, int nocc, int nunocc,
                   const double2* c1, const double2* c2, double2* cprod, int64_t ldc, int col0,
                   void* ws, size_t ws_bytes, cudaStream_t s, int* launches) {
+  if (d->nfft > 0)
+    return wfprod_pw_fft_run(ctx, d, nk, nocc, nunocc, c1, c2, cprod, ldc, col0, ws, ws_bytes, s,
+                             launches);
   PwPlan pl;
   int rc = plan_pw(ctx, d, &pl);
   if (rc) return rc;
@@ -699,8 +692,12 @@ extern "C" int spx_wfprod_pw_dev(spx_ctx* ctx, const spx_pw_desc* pw, int32_t nk
   if (col0 < 0) return set_error(ctx, SPX_EINVAL, "negative col0");
   if ((int64_t)nk * nocc * nunocc == 0) return SPX_OK;
   cudaSetDevice(ctx->device);
-  const size_t need = wfprod_pw_workspace(pw, nk, nocc);
+  const size_t need = wfprod_pw_workspace(pw, nk, nocc, nunocc);
   if (need == 0) {
+    // the plan is invalid: run it once more to report why
+    if (pw->nfft > 0)
+      return wfprod_pw_fft_run(ctx, pw, nk, nocc, nunocc, nullptr, nullptr, nullptr, ldc, col0,
+                               nullptr, 0, nullptr, nullptr);
     PwPlan pl;
     return plan_pw(ctx, pw, &pl);
   }

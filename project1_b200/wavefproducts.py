@@ -55,7 +55,8 @@ class PwDesc:
         gs = (C.c_int32 * 3)(*[int(x) for x in pw["gshift"]])
         self.c = _lib.spx_pw_desc(self.gpt1.shape[0], self.gpt2.shape[0], self.ngptm,
                                   int(pw["step_radius"]), self.gpt1.ctypes.data,
-                                  self.gpt2.ctypes.data, self.gptm.ctypes.data, gs, 0,
+                                  self.gpt2.ctypes.data, self.gptm.ctypes.data, gs,
+                                  int(pw.get("nfft", 0)),
                                   self.cstep.ctypes.data, float(pw["vol"]))
 
 

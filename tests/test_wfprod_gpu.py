@@ -173,3 +173,81 @@ def test_chi0_from_coeffs_equals_products_then_accumulate(ctx):
                      _dev(omega), b, precision="split")
     torch.cuda.synchronize()
     assert torch.equal(a, b)
+
+
+# ---- FFT branch (src/wavefproducts.f:576-758) -------------------------------------
+
+@pytest.mark.parametrize("kw,shifted,nfft", [
+    (dict(), False, 24), (dict(), True, 24), (dict(nk=1, nocc=1, nunocc=1, ngptm=1), True, 20),
+    (dict(ngpt=150, ngptm=70, nunocc=9, step_radius=0), False, 27),
+    (dict(ngpt=120, ngptm=33, nunocc=5, step_radius=4), True, 30)])
+def test_pw_fft_branch_matches_oracle(ctx, kw, shifted, nfft):
+    w = small_workload(**kw)
+    pw = shifted_pw(w) if shifted else inputs.pw_basis(w)
+    c1, c2 = inputs.pw_coeffs(w, pw)
+    ref = oracle.wfprod_pw_fft(pw, w.nk, w.nocc, w.nunocc, c1, c2, nfft)
+    cp = _cprod_dev(w.ngptm, w.npair)
+    wavefproducts2_pw(ctx, dict(pw, nfft=nfft), _dev(c1), _dev(c2), cp, 0)
+    assert _rel(cp.cpu().numpy().T, ref) <= PROD_TOL
+
+
+def test_pw_fft_branch_equals_explicit_without_aliasing(ctx):
+    """On a grid that holds the whole product the two branches agree to rounding."""
+    w = small_workload(nk=2, nocc=3, nunocc=40)
+    pw = shifted_pw(w)
+    c1, c2 = inputs.pw_coeffs(w, pw)
+    a = _cprod_dev(w.ngptm, w.npair)
+    b = _cprod_dev(w.ngptm, w.npair)
+    wavefproducts2_pw(ctx, pw, _dev(c1), _dev(c2), a, 0)
+    wavefproducts2_pw(ctx, dict(pw, nfft=32), _dev(c1), _dev(c2), b, 0)
+    assert _rel(b.cpu().numpy(), a.cpu().numpy()) <= PROD_TOL
+
+
+def test_pw_fft_branch_aliasing_grid_follows_reference(ctx):
+    """A grid too small for the product wraps around exactly as the reference's does."""
+    w = small_workload(nk=1, nocc=2, nunocc=3, ngpt=100, ngptm=30)
+    pw = inputs.pw_basis(w)
+    c1, c2 = inputs.pw_coeffs(w, pw)
+    ref = oracle.wfprod_pw_fft(pw, w.nk, w.nocc, w.nunocc, c1, c2, 9)
+    exp = np.zeros((w.npair, w.ngptm), complex, order="F")
+    oracle.wfprod_pw(pw, w.nk, w.nocc, w.nunocc, c1, c2, exp, 0)
+    assert _rel(ref, exp) > 1e-6                                  # it does alias
+    cp = _cprod_dev(w.ngptm, w.npair)
+    wavefproducts2_pw(ctx, dict(pw, nfft=9), _dev(c1), _dev(c2), cp, 0)
+    assert _rel(cp.cpu().numpy().T, ref) <= PROD_TOL
+
+
+def test_pw_fft_branch_full_basis(ctx):
+    """The configs' interstitial basis on the 48^3 grid, a few band pairs."""
+    w = inputs.WfprodWorkload("c4sub", nk=1, nocc=2, nunocc=3)
+    pw = inputs.pw_basis(w)
+    c1, c2 = inputs.pw_coeffs(w, pw)
+    ref = oracle.wfprod_pw_fft(pw, w.nk, w.nocc, w.nunocc, c1, c2, 48)
+    cp = _cprod_dev(w.ngptm, w.npair)
+    wavefproducts2_pw(ctx, dict(pw, nfft=48), _dev(c1), _dev(c2), cp, 0)
+    assert _rel(cp.cpu().numpy().T, ref) <= 1e-11
+
+
+def test_chi0_from_coeffs_fft_branch(ctx):
+    w, mt, pw, m1, m2, p1, p2, ediff, omega = _fused_case(natom=1, lcut=2, lcutm=2, ngptm=30,
+                                                         nk=2, nocc=3, nunocc=20)
+    a = torch.zeros((len(omega), npack(w.nbas)), dtype=torch.complex128, device=DEV)
+    b = torch.zeros_like(a)
+    chi0_from_coeffs(ctx, mt, pw, _dev(m1), _dev(m2), _dev(p1), _dev(p2), _dev(ediff),
+                     _dev(omega), a, precision="fp64")
+    chi0_from_coeffs(ctx, mt, dict(pw, nfft=32), _dev(m1), _dev(m2), _dev(p1), _dev(p2),
+                     _dev(ediff), _dev(omega), b, precision="fp64")
+    emax, _ = normalized_error(b.cpu().numpy().T, a.cpu().numpy().T, w.nbas)
+    assert emax <= 1e-10
+
+
+def test_pw_fft_branch_rejects_bad_grids(ctx):
+    w = small_workload(nk=1, nocc=1, nunocc=2)
+    pw = inputs.pw_basis(w)
+    c1, c2 = inputs.pw_coeffs(w, pw)
+    cp = _cprod_dev(w.ngptm, w.npair)
+    with pytest.raises(SpexGpuError):
+        wavefproducts2_pw(ctx, dict(pw, nfft=65), _dev(c1), _dev(c2), cp, 0)
+    with pytest.raises(SpexGpuError):       # more than 16 distinct components per axis
+        big = dict(pw, gptm=inputs._sphere(3000), nfft=48)
+        wavefproducts2_pw(ctx, big, _dev(c1), _dev(c2), _cprod_dev(3000, w.npair), 0)
