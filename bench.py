@@ -434,7 +434,7 @@ def bench_products(args, dev, stream):
     convolution) and split chi0 in one call, M never leaving the device."""
     import torch
     import project1_b200 as spx
-    from project1_b200 import inputs
+    from project1_b200 import _lib, inputs
     from project1_b200.wavefproducts import (MtDesc, PwDesc, chi0_from_coeffs, wavefproducts2_mt,
                                              wavefproducts2_pw)
     w = inputs.WFPROD_CONFIGS["c4"]
@@ -472,18 +472,23 @@ def bench_products(args, dev, stream):
     cp = torch.zeros((w.nbas, w.npair), dtype=torch.complex128, device=dev)
     mt_ms = timed(lambda: wavefproducts2_mt(ctx, mt, m1, m2, cp, stream=sc), 1, 2)
     pw_ms = timed(lambda: wavefproducts2_pw(ctx, pw, p1, p2, cp, w.nbasp, stream=sc), 1, 2)
+    ctx_s = spx.Context(dev.index or 0, products=_lib.SPX_PRODUCTS_SPLIT)
+    pws_ms = timed(lambda: wavefproducts2_pw(ctx_s, pw, p1, p2, cp, w.nbasp, stream=sc), 1, 2)
+    ctx_s.close()
     pwf = PwDesc(dict(inputs.pw_basis(w), nfft=48))
     pwf_ms = timed(lambda: wavefproducts2_pw(ctx, pwf, p1, p2, cp, w.nbasp, stream=sc), 1, 2)
     fl_mt = 8.0 * w.nunocc * w.maxlm * w.nocc * w.maxllm * w.nk * w.natom
     fl_pw = 8.0 * w.nunocc * w.ngpt * w.nocc * w.ngptm * w.nk
     res = {"workload": f"c4: {w.natom} atoms lmax {w.lcut} x {w.nrad} radial (maxlm {w.maxlm}), "
                        f"{w.ngpt} PW, {w.ngptm} MPB PW, N_MB {w.nbas}, {w.nk} k, {w.nocc} x {w.nunocc} "
-                       f"bands, {w.nw} freqs; products FP64, chi0 split",
+                       f"bands, {w.nw} freqs; chi0 split, interstitial product GEMM on int8 "
+                       f"slices (MT and convolution FP64)",
            "value": w.flops / (ms * 1e-3) / 1e12, "unit": UNIT + " (chi0 flops over products + chi0 time)",
            "ms_per_step": ms, "steps": args.products_steps, "warmup": args.products_warmup,
            "chi0_kernel_ms": st["ms_gram"], "products_and_prep_ms": st["ms_prep"],
            "mt_ms": mt_ms, "mt_tflops_fp64": fl_mt / (mt_ms * 1e-3) / 1e12,
            "pw_ms": pw_ms, "pw_tflops_fp64": fl_pw / (pw_ms * 1e-3) / 1e12,
+           "pw_split_ms": pws_ms, "pw_split_tflops_equiv": fl_pw / (pws_ms * 1e-3) / 1e12,
            "pw_fft_branch_ms": pwf_ms, "pw_fft_grid": 48,
            "kernels_per_step": st["kernel_launches"], "m_bytes_on_device": 16 * w.nbas * w.npair}
     ctx.close()

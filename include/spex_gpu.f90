@@ -15,6 +15,7 @@ module spex_gpu
                                SPX_ECUDA = -3, SPX_ETIMEOUT = -4, SPX_ENOTSUP = -5, &
                                SPX_ENODEV = -6
   integer(c_int), parameter :: SPX_FP64 = 0, SPX_SPLIT = 1
+  integer(c_int), parameter :: SPX_PRODUCTS_AUTO = 0, SPX_PRODUCTS_FP64 = 1, SPX_PRODUCTS_SPLIT = 2
 
   type, bind(c) :: spx_options
     integer(c_int32_t) :: struct_size = 40
@@ -24,7 +25,7 @@ module spex_gpu
     integer(c_int32_t) :: chunk_pairs = 0
     integer(c_int32_t) :: timeout_ms = 0
     integer(c_int32_t) :: split_variant = 0
-    integer(c_int32_t) :: reserved = 0
+    integer(c_int32_t) :: products = 0           ! SPX_PRODUCTS_AUTO / _FP64 / _SPLIT
   end type
 
   type, bind(c) :: spx_chi0_stats

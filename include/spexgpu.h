@@ -48,6 +48,16 @@ extern "C" {
                              partials, FP64 reduction; weights always in FP64;
                              per element |error| <= 1e-6 sqrt|chi_ii chi_jj|     */
 
+/* spx_options.products: the interstitial (explicit-convolution) product GEMM
+ * AUTO: FP64, except inside spx_chi0_from_coeffs_dev with SPX_SPLIT, where it runs
+ *       on int8 digit slices (A 3, B 4 digits, exact int32 sums; per value the
+ *       slicing error is 2^-17/127 of the row scale, the same as the split
+ *       accumulation's own slicing of M);
+ * FP64: always FP64 (the drop-in); SPLIT: always int8 slices.                  */
+#define SPX_PRODUCTS_AUTO  0
+#define SPX_PRODUCTS_FP64  1
+#define SPX_PRODUCTS_SPLIT 2
+
 typedef struct spx_ctx spx_ctx;
 
 typedef struct spx_options {
@@ -59,7 +69,7 @@ typedef struct spx_options {
   int32_t timeout_ms;       /* bound on every device-side wait, 0 = 4000 ms      */
   int32_t split_variant;    /* split-path kernel: 0 auto, 1 one CTA per tile,
                                2 CTA pair (tcgen05 cta_group::2)                 */
-  int32_t reserved;
+  int32_t products;         /* interstitial product GEMM: SPX_PRODUCTS_*         */
 } spx_options;
 
 /* Per-call statistics filled by the accumulation entry points (may be NULL). */

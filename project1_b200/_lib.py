@@ -13,6 +13,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libspexgpu.so"
 
 SPX_OK, SPX_EINVAL, SPX_ENOMEM, SPX_ECUDA, SPX_ETIMEOUT, SPX_ENOTSUP, SPX_ENODEV = 0, -1, -2, -3, -4, -5, -6
 SPX_FP64, SPX_SPLIT = 0, 1
+SPX_PRODUCTS_AUTO, SPX_PRODUCTS_FP64, SPX_PRODUCTS_SPLIT = 0, 1, 2
 
 
 class SpexGpuError(RuntimeError):
@@ -30,7 +31,7 @@ class spx_options(C.Structure):
         ("chunk_pairs", C.c_int32),
         ("timeout_ms", C.c_int32),
         ("split_variant", C.c_int32),
-        ("reserved", C.c_int32),
+        ("products", C.c_int32),
     ]
 
 

@@ -528,9 +528,9 @@ namespace spx {
 int wfprod_mt_run(spx_ctx*, const spx_mt_desc*, int, int, int, const double2*, const double2*,
                   double2*, int64_t, void*, size_t, cudaStream_t, int*);
 int wfprod_pw_run(spx_ctx*, const spx_pw_desc*, int, int, int, const double2*, const double2*,
-                  double2*, int64_t, int, void*, size_t, cudaStream_t, int*);
+                  double2*, int64_t, int, void*, size_t, cudaStream_t, int*, bool);
 size_t wfprod_mt_workspace(const spx_mt_desc*, int, int);
-size_t wfprod_pw_workspace(const spx_pw_desc*, int, int, int);
+size_t wfprod_pw_workspace(const spx_pw_desc*, int, int, int, bool);
 }  // namespace spx
 
 extern "C" int spx_chi0_from_coeffs_dev(spx_ctx* ctx, const spx_mt_desc* mt,
@@ -566,7 +566,11 @@ extern "C" int spx_chi0_from_coeffs_dev(spx_ctx* ctx, const spx_mt_desc* mt,
   cudaStream_t s = pick_stream(ctx, stream);
   const int64_t ldc = (int64_t)align_up((size_t)npair, 16);
   const size_t m_bytes = align_up(sizeof(double2) * (size_t)ldc * nbas, 256);
-  const size_t prod_bytes = std::max(wfprod_mt_workspace(mt, nk, nocc), wfprod_pw_workspace(pw, nk, nocc, nunocc));
+  // interstitial products on int8 slices when the accumulation is split anyway
+  const bool split_products = ctx->opt.products == SPX_PRODUCTS_SPLIT ||
+                              (ctx->opt.products == SPX_PRODUCTS_AUTO && precision == SPX_SPLIT);
+  const size_t prod_bytes = std::max(wfprod_mt_workspace(mt, nk, nocc),
+                                     wfprod_pw_workspace(pw, nk, nocc, nunocc, split_products));
   const int64_t ldw = ldc;
   const size_t w_bytes = align_up(sizeof(double) * (size_t)ldw * nw, 256);
   const size_t s_bytes = precision == SPX_SPLIT ? split_workspace_bytes(npair, nbas, nw) : 0;
@@ -584,7 +588,7 @@ extern "C" int spx_chi0_from_coeffs_dev(spx_ctx* ctx, const spx_mt_desc* mt,
   if (!rc)
     rc = wfprod_pw_run(ctx, pw, nk, nocc, nunocc, reinterpret_cast<const double2*>(cpw_occ),
                        reinterpret_cast<const double2*>(cpw_unocc), M, ldc, mt->natom * maxllm,
-                       sc, scratch, s, &launches);
+                       sc, scratch, s, &launches, split_products);
   if (rc) {
     ctx->timing = false;
     return rc;

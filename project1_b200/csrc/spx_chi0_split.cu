@@ -21,9 +21,10 @@
 // the scale factors stay FP64 throughout; near-degenerate pairs therefore keep
 // their FP64 weights.
 //
-// Error (per element, relative to sqrt|chi_ii chi_jj|): slicing of A <= 2^-24/127
-// times the column crest factor, slicing of B <= 2^-32/127 times the weighted
-// crest factor, dropped orders g >= 4 bounded by the same; see the accuracy tests.
+// Error (per element, relative to sqrt|chi_ii chi_jj|): slicing of A (half a unit of
+// its third digit, 2^-17/127 of the column scale per value) <= 2^-17/127 times the
+// column crest factor max|x| sqrt(P)/||x||, slicing of B <= 2^-25/127 times the
+// weighted crest factor, dropped orders g >= 4 below that; see the accuracy tests.
 //
 // Tile layout: a 64 x 64 complex tile is a 128 x 128 real-stacked product: A rows
 // are (Re M_i | Im M_i) for 64 mixed-basis functions, B rows likewise for the
@@ -963,6 +964,379 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
         return rc;
       if ((rc = prep(s + 1))) return rc;
     }
+  }
+  return SPX_OK;
+}
+
+}  // namespace spx
+
+// ---------------------------------------------------------------------------
+// K4s: the interstitial product GEMM of the explicit convolution
+// (src/wavefproducts.f:945, cprod += conj(cpw2^H cpw3)/sqrt(vol)) on the same
+// int8 digit slices as K2. C_b(m, col) = alpha * sum_k A_b(m, k) conj(B_b(col, k)):
+// A = the unoccupied coefficients (rows n'), B = the gathered convolution
+// cpw0(G2 - G_M + g) (rows (n, ig)), one batch per k point. Each row is scaled
+// by its own largest |Re|, |Im| over k; A keeps 3 digits, B 4, and the nine
+// products with t + u <= 3 are summed exactly in int32 (k <= 32768 per launch),
+// so the only rounding is the slicing: 2^-17/127 of A's row scale per value, so
+// |error of C(m, col)| <= 2^-17/127 * crest(A_m) * ||A_m|| ||B_col||.
+// Items are rectangular (batch, column tile, row tile), row tiles fastest so that
+// concurrent CTAs share the large B tile through L2. The epilogue adds alpha
+// times the tile into cprod's columns: each double is written by one thread.
+
+namespace spx {
+
+struct SgParams {
+  int nbatch, mtiles, ntiles, nitems, nk;
+  int64_t RA, RB;          // real-stacked rows per batch of the A and B planes
+  int M, ncol, ncin;       // valid rows of A, columns (= rows of B), col = n*ncin + c
+  const double* sA;        // row scales [batch][mtiles*64]
+  const double* sB;        // [batch][ntiles*64]
+  double* out;             // cprod as doubles, at (row 0, column 0) of batch 0
+  int64_t sO2, sOn, sOc;   // complex strides: batch, n, c
+  double alpha;
+  int* status;
+  uint64_t timeout_ns;
+};
+
+__global__ void __launch_bounds__(SP_THREADS, 1)
+    split_gemm_kernel(const __grid_constant__ CUtensorMap mapA,
+                      const __grid_constant__ CUtensorMap mapB, SgParams prm) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  SplitSmem& sm = *reinterpret_cast<SplitSmem*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < SP_ST; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], 1);
+    }
+    mbar_init(&sm.tfull, 1);
+    mbar_init(&sm.tempty, 4);
+    mbar_init(&sm.xfull, 4);
+    mbar_init(&sm.xfree, 4);
+    mbar_init(&sm.mdone, 1);
+    fence_barrier_init();
+  }
+  if (warp == 1) tmem_alloc(&sm.tmem_base, SP_TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sm.tmem_base;
+  auto decode = [&](int item, int* b, int* mt, int* ct) {
+    *mt = item % prm.mtiles;
+    const int r = item / prm.mtiles;
+    *ct = r % prm.ntiles;
+    *b = r / prm.ntiles;
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int st = 0;
+      uint32_t ph = 0;
+      bool issued[SP_ST];
+      uint32_t last_ph[SP_ST];
+      for (int s = 0; s < SP_ST; ++s) issued[s] = false, last_ph[s] = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; item < prm.nitems && ok; item += gridDim.x) {
+        int b, mt, ct;
+        decode(item, &b, &mt, &ct);
+        const int ra = (int)(b * prm.RA) + mt * SP_ROWS, rb = (int)(b * prm.RB) + ct * SP_ROWS;
+        for (int ks = 0; ks < prm.nk; ++ks) {
+          if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&sm.full[st], (uint32_t)((SP_SA + SP_SB) * SP_PLANE));
+          tma_load_4d(&sm.a[st][0][0], &mapA, 0, ra, ks, 0, &sm.full[st]);
+          tma_load_4d(&sm.b[st][0][0], &mapB, 0, rb, ks, 0, &sm.full[st]);
+          issued[st] = true;
+          last_ph[st] = ph;
+          if (++st == SP_ST) st = 0, ph ^= 1u;
+        }
+      }
+      for (int s = 0; s < SP_ST; ++s)
+        if (issued[s]) mbar_drain(&sm.full[s], last_ph[s], prm.timeout_ns);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int st = 0;
+      uint32_t ph = 0;
+      int j = 0;
+      bool committed = false;
+      for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j) {
+        if (!mbar_wait(&sm.tempty, (uint32_t)(j & 1) ^ 1u, prm.timeout_ns, prm.status)) break;
+        tc_fence_after();
+        bool ok = true;
+        for (int ks = 0; ks < prm.nk; ++ks) {
+          if (!mbar_wait(&sm.full[st], ph, prm.timeout_ns, prm.status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll
+          for (int kk = 0; kk < SP_NKS; ++kk) {
+            uint64_t da[SP_SA], db[SP_SB];
+#pragma unroll
+            for (int t = 0; t < SP_SA; ++t) da[t] = desc_sw64(&sm.a[st][t][0]) + (uint64_t)(kk * 2);
+#pragma unroll
+            for (int u = 0; u < SP_SB; ++u) db[u] = desc_sw64(&sm.b[st][u][0]) + (uint64_t)(kk * 2);
+            const uint32_t k0 = (ks > 0 || kk > 0);
+            mma_i8<1>(tmem + 0 * 128, da[0], db[0], SP_IDESC, k0);
+            mma_i8<2>(tmem + 1 * 128, da[0], db[1], SP_IDESC, k0);
+            mma_i8<2>(tmem + 2 * 128, da[0], db[2], SP_IDESC, k0);
+            mma_i8<3>(tmem + 3 * 128, da[0], db[3], SP_IDESC, k0);
+            mma_i8<1>(tmem + 1 * 128, da[1], db[0], SP_IDESC, 1u);
+            mma_i8<2>(tmem + 2 * 128, da[1], db[1], SP_IDESC, 1u);
+            mma_i8<3>(tmem + 3 * 128, da[1], db[2], SP_IDESC, 1u);
+            mma_i8<1>(tmem + 2 * 128, da[2], db[0], SP_IDESC, 1u);
+            mma_i8<3>(tmem + 3 * 128, da[2], db[1], SP_IDESC, 1u);
+          }
+          tc_commit(&sm.empty[st]);
+          committed = true;
+          if (++st == SP_ST) st = 0, ph ^= 1u;
+        }
+        if (!ok) break;
+        tc_commit(&sm.tfull);
+      }
+      if (committed) {
+        tc_commit(&sm.mdone);
+        mbar_drain(&sm.mdone, 0u, prm.timeout_ns);
+      }
+    }
+  } else {
+    const int q = warp & 3;
+    const bool is_re = q < 2;
+    const int ii = (q & 1) * 32 + lane;
+    const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16);
+    int j = 0;
+    uint32_t xseq = 0;
+    for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j) {
+      if (!mbar_wait_idle(&sm.tfull, (uint32_t)(j & 1), prm.timeout_ns, prm.status)) break;
+      tc_fence_after();
+      int b, mt, ct;
+      decode(item, &b, &mt, &ct);
+      const int gm = mt * SP_TILE + ii;
+      const double sm_ = prm.sA[(int64_t)b * prm.mtiles * SP_TILE + gm];
+      const double fac = prm.alpha * sm_ * (1.0 / (127.0 * 127.0 * 16777216.0));
+      const double* sbb = prm.sB + (int64_t)b * prm.ntiles * SP_TILE;
+      double* ob = prm.out + 2 * (b * prm.sO2 + gm) + (is_re ? 0 : 1);
+      bool ok = true;
+      for (int js = 0; js < 2 && ok; ++js, ++xseq) {
+        long long tre[32], tim[32];
+        load_orders(tl + (uint32_t)(js * 32), tre);
+        load_orders(tl + (uint32_t)(64 + js * 32), tim);
+        if (!mbar_wait(&sm.xfree, (xseq & 1u) ^ 1u, prm.timeout_ns, prm.status)) {
+          ok = false;
+          break;
+        }
+#pragma unroll
+        for (int k = 0; k < 32; ++k) sm.xchg[is_re ? 0 : 1][ii][k] = tim[k];
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.xfull);
+        if (!mbar_wait(&sm.xfull, xseq & 1u, prm.timeout_ns, prm.status)) {
+          ok = false;
+          break;
+        }
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+          const int gc = ct * SP_TILE + js * 32 + k;
+          const long long partner = sm.xchg[is_re ? 1 : 0][ii][k];
+          const long long v = is_re ? tre[k] + partner : tre[k] - partner;
+          if (gm < prm.M && gc < prm.ncol) {
+            const int n = gc / prm.ncin, c = gc - n * prm.ncin;
+            double* o = ob + 2 * (n * prm.sOn + c * prm.sOc);
+            *o += fac * sbb[gc] * (double)v;
+          }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.xfree);
+      }
+      if (!ok) break;
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.tempty);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc(tmem, SP_TMEM_COLS);
+}
+
+// Row sources of the two operands: A rows are contiguous in k, B rows are gathered.
+struct SgSrcRows {
+  const double2* base;
+  int64_t ld, bstride;
+  __device__ __forceinline__ double2 get(int b, int r, int k) const {
+    return base[b * bstride + (int64_t)r * ld + k];
+  }
+};
+struct SgSrcGather {
+  const double2* grid;      // [batch][n][box]
+  int64_t bstride, nstride;
+  const int64_t* coff;      // per c
+  const int* koff;          // per k
+  int ncin;
+  __device__ __forceinline__ double2 get(int b, int r, int k) const {
+    const int n = r / ncin, c = r - n * ncin;
+    return grid[b * bstride + n * nstride + coff[c] + koff[k]];
+  }
+};
+
+// s[b*rows_pad + r] = max_k max(|Re|, |Im|) of row r of batch b (0 for padding rows).
+template <class Src>
+__global__ void sgemm_rowmax_kernel(Src src, int rows, int rows_pad, int K, double* s) {
+  const int r = blockIdx.x, b = blockIdx.y;
+  double m = 0.0;
+  if (r < rows)
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+      const double2 v = src.get(b, r, k);
+      m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+    }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) s[(int64_t)b * rows_pad + r] = m;
+  }
+}
+
+// S digits of round(x * 127/s * 2^(8(S-1))) into planes [t][k-block][row][64 B] with
+// real-stacked rows b*R + 128*(r/64) + {r%64 Re, 64 + r%64 Im}. One thread = one row
+// and 16 consecutive k; a warp = 8 consecutive rows x the 4 quarters of a k-block.
+template <int S, class Src>
+__global__ void __launch_bounds__(128)
+    sgemm_quant_kernel(Src src, int rows, int rows_pad, int K, int nkb, int nbatch, int64_t R,
+                       const double* __restrict__ s, int8_t* __restrict__ planes) {
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int ngroup = rows_pad / 8;
+  if (tid >= (int64_t)ngroup * 32 * nkb * nbatch) return;
+  const int lane8 = (int)(tid & 7), quarter = (int)((tid >> 3) & 3);
+  const int64_t rest = tid >> 5;
+  const int r = (int)(rest % ngroup) * 8 + lane8;
+  const int64_t kbb = rest / ngroup;
+  const int kb = (int)(kbb % nkb), b = (int)(kbb / nkb);
+  const int k0 = kb * SP_KB + quarter * 16;
+  const int64_t rows_total = (int64_t)nbatch * R;
+  const int64_t rr = (int64_t)b * R + (r / SP_TILE) * SP_ROWS + (r % SP_TILE);
+  const int64_t pstride = (int64_t)nkb * rows_total * SP_KB;
+  const int64_t o_re = ((int64_t)kb * rows_total + rr) * SP_KB + quarter * 16;
+  const int64_t o_im = o_re + (int64_t)SP_TILE * SP_KB;
+  const double sc = r < rows ? s[(int64_t)b * rows_pad + r] : 0.0;
+  const double inv = sc > 0.0 ? 127.0 * (S == 4 ? 16777216.0 : 65536.0) / sc : 0.0;
+  uint32_t wr[S][4], wi[S][4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint32_t yr[4], yi[4], pr[S], pi[S];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int k = k0 + 4 * q + e;
+      double2 v = make_double2(0.0, 0.0);
+      if (r < rows && k < K) v = src.get(b, r, k);
+      yr[e] = round_mul(v.x, inv);
+      yi[e] = round_mul(v.y, inv);
+    }
+    digit_planes<S>(yr, pr);
+    digit_planes<S>(yi, pi);
+#pragma unroll
+    for (int t = 0; t < S; ++t) wr[t][q] = pr[t], wi[t][q] = pi[t];
+  }
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    *reinterpret_cast<uint4*>(planes + o_re + t * pstride) = make_uint4(wr[t][0], wr[t][1], wr[t][2], wr[t][3]);
+    *reinterpret_cast<uint4*>(planes + o_im + t * pstride) = make_uint4(wi[t][0], wi[t][1], wi[t][2], wi[t][3]);
+  }
+}
+
+// Bytes of scratch for one launch group of `nbatch` batches (planes and scales).
+size_t sgemm_workspace_bytes(int nbatch, int M, int ncol, int K) {
+  const int64_t mt = (M + SP_TILE - 1) / SP_TILE, nt = (ncol + SP_TILE - 1) / SP_TILE;
+  const int64_t kp = (int64_t)align_up((size_t)std::min(std::max(K, 1), SP_SLAB), SP_KB);
+  return align_up((size_t)SP_SA * kp * nbatch * mt * SP_ROWS, 1024) +
+         align_up((size_t)SP_SB * kp * nbatch * nt * SP_ROWS, 1024) +
+         align_up(sizeof(double) * nbatch * mt * SP_TILE, 256) +
+         align_up(sizeof(double) * nbatch * nt * SP_TILE, 256) + 2048;
+}
+
+// The interstitial product GEMM on int8 slices for `nbatch` k points: A rows from
+// cpw_unocc (contiguous), B rows gathered from the convolved grids.
+int sgemm_products(spx_ctx* ctx, int nbatch, int M, int ncol, int K, const double2* A,
+                   int64_t lda, int64_t a_bstride, const double2* grid, int64_t g_bstride,
+                   int64_t g_nstride, const int64_t* coff, const int* koff, int ncin,
+                   double2* out, int64_t sO2, int64_t sOn, int64_t sOc, double alpha, void* ws,
+                   size_t ws_bytes, cudaStream_t s, int* launches) {
+  if (nbatch <= 0 || M <= 0 || ncol <= 0 || K <= 0) return SPX_OK;
+  const int mt = (M + SP_TILE - 1) / SP_TILE, nt = (ncol + SP_TILE - 1) / SP_TILE;
+  const int64_t RA = (int64_t)mt * SP_ROWS, RB = (int64_t)nt * SP_ROWS;
+  if ((int64_t)nbatch * RB > 2147483647LL || (int64_t)nbatch * mt * nt > 2147483647LL)
+    return set_error(ctx, SPX_EINVAL, "product GEMM too large for one launch group");
+  uint8_t* base = (uint8_t*)align_up((size_t)ws, 1024);
+  const size_t need = sgemm_workspace_bytes(nbatch, M, ncol, K);
+  if (!ws || ws_bytes < need + 1024) return set_error(ctx, SPX_ENOMEM, "split product scratch too small");
+  const size_t smem = sizeof(SplitSmem) + 1024;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  int rc;
+  // k is cut into exact int32 slabs of at most 32768; each slab adds into the output
+  for (int kbeg = 0; kbeg < K; kbeg += SP_SLAB) {
+    const int Ks = std::min(SP_SLAB, K - kbeg);
+    const int nkb = (int)(align_up((size_t)Ks, SP_KB) / SP_KB);
+    const int64_t kp = (int64_t)nkb * SP_KB;
+    int8_t* PA = (int8_t*)base;
+    int8_t* PB = (int8_t*)(base + align_up((size_t)SP_SA * kp * nbatch * RA, 1024));
+    double* sA = (double*)((uint8_t*)PB + align_up((size_t)SP_SB * kp * nbatch * RB, 1024));
+    double* sB = (double*)((uint8_t*)sA + align_up(sizeof(double) * nbatch * mt * SP_TILE, 256));
+    SgSrcRows sa{A + kbeg, lda, a_bstride};
+    SgSrcGather sb{grid, g_bstride, g_nstride, coff, koff + kbeg, ncin};
+    sgemm_rowmax_kernel<<<dim3(mt * SP_TILE, nbatch), 256, 0, s>>>(sa, M, mt * SP_TILE, Ks, sA);
+    sgemm_rowmax_kernel<<<dim3(nt * SP_TILE, nbatch), 256, 0, s>>>(sb, ncol, nt * SP_TILE, Ks, sB);
+    const int64_t ta = (int64_t)mt * SP_TILE / 8 * 32 * nkb * nbatch;
+    const int64_t tb = (int64_t)nt * SP_TILE / 8 * 32 * nkb * nbatch;
+    sgemm_quant_kernel<SP_SA><<<(unsigned)((ta + 127) / 128), 128, 0, s>>>(sa, M, mt * SP_TILE, Ks, nkb, nbatch, RA, sA, PA);
+    sgemm_quant_kernel<SP_SB><<<(unsigned)((tb + 127) / 128), 128, 0, s>>>(sb, ncol, nt * SP_TILE, Ks, nkb, nbatch, RB, sB, PB);
+    if ((rc = check_cuda(ctx, cudaGetLastError(), "split product operand preparation"))) return rc;
+    *launches += 4;
+    CUtensorMap mapA, mapB;
+    const uint64_t rta = (uint64_t)nbatch * RA, rtb = (uint64_t)nbatch * RB;
+    const uint64_t da[4] = {SP_KB, rta, (uint64_t)nkb, SP_SA};
+    const uint64_t sta[3] = {SP_KB, rta * SP_KB, (uint64_t)nkb * rta * SP_KB};
+    const uint32_t ba[4] = {SP_KB, SP_ROWS, 1, SP_SA};
+    if ((rc = make_tmap_u8_4d(ctx, &mapA, PA, da, sta, ba, CU_TENSOR_MAP_SWIZZLE_64B))) return rc;
+    const uint64_t db[4] = {SP_KB, rtb, (uint64_t)nkb, SP_SB};
+    const uint64_t stb[3] = {SP_KB, rtb * SP_KB, (uint64_t)nkb * rtb * SP_KB};
+    const uint32_t bb[4] = {SP_KB, SP_ROWS, 1, SP_SB};
+    if ((rc = make_tmap_u8_4d(ctx, &mapB, PB, db, stb, bb, CU_TENSOR_MAP_SWIZZLE_64B))) return rc;
+    SgParams prm;
+    prm.nbatch = nbatch;
+    prm.mtiles = mt;
+    prm.ntiles = nt;
+    prm.nitems = nbatch * mt * nt;
+    prm.nk = nkb;
+    prm.RA = RA;
+    prm.RB = RB;
+    prm.M = M;
+    prm.ncol = ncol;
+    prm.ncin = ncin;
+    prm.sA = sA;
+    prm.sB = sB;
+    prm.out = reinterpret_cast<double*>(out);
+    prm.sO2 = sO2;
+    prm.sOn = sOn;
+    prm.sOc = sOc;
+    prm.alpha = alpha;
+    prm.status = ctx->d_status;
+    prm.timeout_ns = (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
+    const int grid_n = std::min(prm.nitems, ctx->num_sms);
+    split_gemm_kernel<<<grid_n, SP_THREADS, smem, s>>>(mapA, mapB, prm);
+    if ((rc = check_cuda(ctx, cudaGetLastError(), "split_gemm_kernel launch"))) return rc;
+    *launches += 1;
   }
   return SPX_OK;
 }

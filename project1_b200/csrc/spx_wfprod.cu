@@ -549,16 +549,23 @@ static int plan_pw(spx_ctx* ctx, const spx_pw_desc* d, PwPlan* pl) {
 }
 
 size_t wfprod_pw_fft_workspace(const spx_pw_desc* d, int nk, int nocc, int nunocc);
+size_t sgemm_workspace_bytes(int nbatch, int M, int ncol, int K);
+int sgemm_products(spx_ctx* ctx, int nbatch, int M, int ncol, int K, const double2* A,
+                   int64_t lda, int64_t a_bstride, const double2* grid, int64_t g_bstride,
+                   int64_t g_nstride, const int64_t* coff, const int* koff, int ncin,
+                   double2* out, int64_t sO2, int64_t sOn, int64_t sOc, double alpha, void* ws,
+                   size_t ws_bytes, cudaStream_t s, int* launches);
 int wfprod_pw_fft_run(spx_ctx* ctx, const spx_pw_desc* d, int nk, int nocc, int nunocc,
                       const double2* c1, const double2* c2, double2* cprod, int64_t ldc, int col0,
                       void* ws, size_t ws_bytes, cudaStream_t s, int* launches);
 
-size_t wfprod_pw_workspace(const spx_pw_desc* d, int nk, int nocc, int nunocc) {
+size_t wfprod_pw_workspace(const spx_pw_desc* d, int nk, int nocc, int nunocc, bool split) {
   if (d->nfft > 0) return wfprod_pw_fft_workspace(d, nk, nocc, nunocc);
   spx_ctx dummy;
   PwPlan pl;
   if (plan_pw(&dummy, d, &pl)) return 0;
-  const size_t perk = align_up(sizeof(double2) * nocc * (size_t)(pl.b1.size() + pl.b0.size()), 256);
+  size_t perk = align_up(sizeof(double2) * nocc * (size_t)(pl.b1.size() + pl.b0.size()), 256);
+  if (split) perk += sgemm_workspace_bytes(1, nunocc, nocc * d->ngptm, d->ngpt2);
   const size_t fixed = align_up(sizeof(int) * std::max(d->ngpt1, 1), 256) +
                        align_up(sizeof(int) * std::max(d->ngpt2, 1), 256) +
                        align_up(sizeof(int64_t) * std::max(d->ngptm, 1), 256) + 4096;
@@ -568,9 +575,10 @@ size_t wfprod_pw_workspace(const spx_pw_desc* d, int nk, int nocc, int nunocc) {
 }
 
 // Runs the explicit-convolution PW products into cprod columns [col0, col0+ngptm).
+// split: the product GEMM on int8 digit slices (K4s) instead of FP64 (K4c).
 int wfprod_pw_run(spx_ctx* ctx, const spx_pw_desc* d, int nk, int nocc, int nunocc,
                   const double2* c1, const double2* c2, double2* cprod, int64_t ldc, int col0,
-                  void* ws, size_t ws_bytes, cudaStream_t s, int* launches) {
+                  void* ws, size_t ws_bytes, cudaStream_t s, int* launches, bool split) {
   if (d->nfft > 0)
     return wfprod_pw_fft_run(ctx, d, nk, nocc, nunocc, c1, c2, cprod, ldc, col0, ws, ws_bytes, s,
                              launches);
@@ -578,7 +586,9 @@ int wfprod_pw_run(spx_ctx* ctx, const spx_pw_desc* d, int nk, int nocc, int nuno
   int rc = plan_pw(ctx, d, &pl);
   if (rc) return rc;
   if (d->ngptm == 0 || nk == 0 || nocc == 0 || nunocc == 0) return SPX_OK;
-  const size_t perk = align_up(sizeof(double2) * nocc * (size_t)(pl.b1.size() + pl.b0.size()), 256) + 512;
+  const size_t sg_perk = split ? sgemm_workspace_bytes(1, nunocc, nocc * d->ngptm, d->ngpt2) : 0;
+  const size_t perk =
+      align_up(sizeof(double2) * nocc * (size_t)(pl.b1.size() + pl.b0.size()), 256) + 512 + sg_perk;
   Carve cv{(char*)ws, ws_bytes};
   int* d_gidx = cv.take<int>(d->ngpt1);
   int* d_koff = cv.take<int>(d->ngpt2);
@@ -591,6 +601,8 @@ int wfprod_pw_run(spx_ctx* ctx, const spx_pw_desc* d, int nk, int nocc, int nuno
   const int kchunk = (int)std::min<size_t>({(size_t)nk, cv.left / perk, (size_t)(65535 / nocc)});
   double2* grid1 = cv.take<double2>((size_t)kchunk * nocc * pl.b1.size());
   double2* grid0 = cv.take<double2>((size_t)kchunk * nocc * pl.b0.size());
+  const size_t sg_bytes = split ? sgemm_workspace_bytes(kchunk, nunocc, nocc * d->ngptm, d->ngpt2) + 1024 : 0;
+  void* sg_ws = split ? (void*)cv.take<uint8_t>(sg_bytes) : nullptr;
   if (!cv.ok) return set_error(ctx, SPX_ENOMEM, "plane-wave scratch too small");
   const double2 alpha = make_double2(1.0 / std::sqrt(d->vol), 0.0);
   if ((d->ngpt1 && (rc = check_cuda(ctx, cudaMemcpyAsync(d_gidx, pl.gidx1.data(), sizeof(int) * d->ngpt1, cudaMemcpyHostToDevice, s), "copy plan"))) ||
@@ -620,6 +632,17 @@ int wfprod_pw_run(spx_ctx* ctx, const spx_pw_desc* d, int nk, int nocc, int nuno
       ++*launches;
     }
     if (d->ngpt2 == 0) continue;
+    if (split) {
+      rc = sgemm_products(ctx, kn, nunocc, nocc * d->ngptm, d->ngpt2,
+                          c2 + (int64_t)k0 * nunocc * d->ngpt2, d->ngpt2,
+                          (int64_t)nunocc * d->ngpt2, grid0, (int64_t)nocc * pl.b0.size(),
+                          pl.b0.size(), d_coff, d_koff, d->ngptm,
+                          cprod + (int64_t)k0 * nocc * nunocc + ldc * col0,
+                          (int64_t)nocc * nunocc, nunocc, ldc, 1.0 / std::sqrt(d->vol), sg_ws,
+                          sg_bytes, s, launches);
+      if (rc) return rc;
+      continue;
+    }
     // batches b = k: A = cpw2(k, :, :), B(col = n*ngptm + ig, ig2) = grid0(k, n)[coff[ig] + koff[ig2]]
     ZgParams prm{};
     prm.A = c2 + (int64_t)k0 * nunocc * d->ngpt2;
@@ -692,7 +715,8 @@ extern "C" int spx_wfprod_pw_dev(spx_ctx* ctx, const spx_pw_desc* pw, int32_t nk
   if (col0 < 0) return set_error(ctx, SPX_EINVAL, "negative col0");
   if ((int64_t)nk * nocc * nunocc == 0) return SPX_OK;
   cudaSetDevice(ctx->device);
-  const size_t need = wfprod_pw_workspace(pw, nk, nocc, nunocc);
+  const bool split = ctx->opt.products == SPX_PRODUCTS_SPLIT;
+  const size_t need = wfprod_pw_workspace(pw, nk, nocc, nunocc, split);
   if (need == 0) {
     // the plan is invalid: run it once more to report why
     if (pw->nfft > 0)
@@ -706,5 +730,5 @@ extern "C" int spx_wfprod_pw_dev(spx_ctx* ctx, const spx_pw_desc* pw, int32_t nk
   cudaStream_t s = pick_stream(ctx, stream);
   return wfprod_pw_run(ctx, pw, nk, nocc, nunocc, reinterpret_cast<const double2*>(cpw_occ),
                        reinterpret_cast<const double2*>(cpw_unocc), reinterpret_cast<double2*>(cprod),
-                       ldc, col0, ctx->ws, ctx->ws_bytes, s, &launches);
+                       ldc, col0, ctx->ws, ctx->ws_bytes, s, &launches, split);
 }

@@ -61,10 +61,11 @@ class Context:
     """One libspexgpu context: a device, its streams and workspace."""
 
     def __init__(self, device: int = 0, workspace_limit: int = 0, chunk_pairs: int = 0,
-                 timeout_ms: int = 0, pinned_limit: int = 0, split_variant: int = 0):
+                 timeout_ms: int = 0, pinned_limit: int = 0, split_variant: int = 0,
+                 products: int = 0):
         self.lib = _lib.load()
         opt = _lib.spx_options(C.sizeof(_lib.spx_options), 0, workspace_limit, pinned_limit,
-                               chunk_pairs, timeout_ms, split_variant, 0)
+                               chunk_pairs, timeout_ms, split_variant, products)
         h = C.c_void_p()
         rc = self.lib.spx_ctx_create(device, C.byref(opt), C.byref(h))
         if rc != 0:

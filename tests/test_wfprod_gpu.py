@@ -7,7 +7,7 @@ torch = pytest.importorskip("torch")
 
 import oracle
 import project1_b200 as spx
-from project1_b200 import inputs
+from project1_b200 import _lib, inputs
 from project1_b200.wavefproducts import (MtDesc, PwDesc, chi0_from_coeffs, wavefproducts2_mt,
                                          wavefproducts2_pw)
 from project1_b200.susceptibility import SpexGpuError, npack
@@ -158,8 +158,11 @@ def test_chi0_from_coeffs_matches_oracle_chain(ctx, precision, tol):
     assert st["kernel_launches"] >= 5
 
 
-def test_chi0_from_coeffs_equals_products_then_accumulate(ctx):
-    """The fused call is the composition of the three public calls, bit for bit."""
+@pytest.mark.parametrize("products", [_lib.SPX_PRODUCTS_FP64, _lib.SPX_PRODUCTS_SPLIT])
+def test_chi0_from_coeffs_equals_products_then_accumulate(products):
+    """The fused call is the composition of the three public calls, bit for bit, with
+    the interstitial products in FP64 or on int8 slices alike."""
+    ctx = spx.Context(0, products=products)
     w, mt, pw, m1, m2, p1, p2, ediff, omega = _fused_case(nk=1, nocc=3, nunocc=50)
     ldc = (w.npair + 15) // 16 * 16
     cp = _cprod_dev(w.nbas, ldc)
@@ -173,6 +176,7 @@ def test_chi0_from_coeffs_equals_products_then_accumulate(ctx):
                      _dev(omega), b, precision="split")
     torch.cuda.synchronize()
     assert torch.equal(a, b)
+    ctx.close()
 
 
 # ---- FFT branch (src/wavefproducts.f:576-758) -------------------------------------
@@ -251,3 +255,47 @@ def test_pw_fft_branch_rejects_bad_grids(ctx):
     with pytest.raises(SpexGpuError):       # more than 16 distinct components per axis
         big = dict(pw, gptm=inputs._sphere(3000), nfft=48)
         wavefproducts2_pw(ctx, big, _dev(c1), _dev(c2), _cprod_dev(3000, w.npair), 0)
+
+
+# ---- interstitial products on int8 digit slices (K4s) ---------------------------
+# max |error| / max |cprod|. The slicing bound is 2^-17/127 * crest(A_m) * ||A_m|| ||B_col||
+# (6e-8 times a crest factor of about 5-10 for the damped plane-wave rows); measured ~1e-7.
+SPLIT_PROD_TOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def ctx_split():
+    c = spx.Context(0, products=_lib.SPX_PRODUCTS_SPLIT)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("kw,shifted", [
+    (dict(), False), (dict(), True), (dict(nk=1, nocc=1, nunocc=1, ngptm=1), True),
+    (dict(ngpt=150, ngptm=70, nunocc=100, step_radius=0), False),
+    (dict(ngpt=120, ngptm=33, nunocc=65, nk=3, step_radius=4), True)])
+def test_pw_split_products_match_oracle(ctx_split, kw, shifted):
+    w = small_workload(**kw)
+    pw = shifted_pw(w) if shifted else inputs.pw_basis(w)
+    c1, c2 = inputs.pw_coeffs(w, pw)
+    ref = np.zeros((w.npair, w.ngptm), complex, order="F")
+    oracle.wfprod_pw(pw, w.nk, w.nocc, w.nunocc, c1, c2, ref, 0)
+    cp = _cprod_dev(w.ngptm, w.npair)
+    wavefproducts2_pw(ctx_split, pw, _dev(c1), _dev(c2), cp, 0)
+    assert _rel(cp.cpu().numpy().T, ref) <= SPLIT_PROD_TOL
+
+
+def test_pw_split_products_full_basis(ctx, ctx_split):
+    """The configs' interstitial basis (3000 PW, 1014 MPB PW) against the FP64 GEMM,
+    with a padded leading dimension and a column offset."""
+    w = inputs.WfprodWorkload("c4sub", nk=2, nocc=3, nunocc=70)
+    pw = inputs.pw_basis(w)
+    c1, c2 = inputs.pw_coeffs(w, pw)
+    ldc, col0 = w.npair + 7, 11
+    a = _cprod_dev(col0 + w.ngptm, ldc, 0.5)
+    b = _cprod_dev(col0 + w.ngptm, ldc, 0.5)
+    wavefproducts2_pw(ctx, pw, _dev(c1), _dev(c2), a, col0)
+    wavefproducts2_pw(ctx_split, pw, _dev(c1), _dev(c2), b, col0)
+    a, b = a.cpu().numpy(), b.cpu().numpy()
+    assert np.array_equal(b[:col0], a[:col0]) and np.array_equal(b[:, w.npair:], a[:, w.npair:])
+    assert _rel(b - 0.5, a - 0.5) <= SPLIT_PROD_TOL
