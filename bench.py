@@ -438,6 +438,9 @@ def bench_products(args, dev, stream):
     from project1_b200.wavefproducts import (MtDesc, PwDesc, chi0_from_coeffs, wavefproducts2_mt,
                                              wavefproducts2_pw)
     w = inputs.WFPROD_CONFIGS["c4"]
+    if args.c4_kpts:
+        import dataclasses
+        w = dataclasses.replace(w, nk=args.c4_kpts)
     mt, pw = MtDesc(inputs.mt_basis(w)), PwDesc(inputs.pw_basis(w))
     m1, m2 = inputs.mt_coeffs(w)
     p1, p2 = inputs.pw_coeffs(w, {"gpt1": pw.gpt1, "gpt2": pw.gpt2})
@@ -563,6 +566,7 @@ def main():
     ap.add_argument("--products-warmup", type=int, default=3)
     ap.add_argument("--batched-steps", type=int, default=1, help="configs[3] timed batches (0: skip)")
     ap.add_argument("--batched-warmup", type=int, default=1)
+    ap.add_argument("--c4-kpts", type=int, default=0, help="override configs[4]'s k-point count (profiling)")
     ap.add_argument("--precision", choices=["split", "fp64"], default=None,
                     help="force the measured path (profiling captures)")
     ap.add_argument("--kpts", type=int, default=0, help="override the k-point count (profiling)")
