@@ -14,7 +14,8 @@
 //   * warp 0 streams 16-pair slabs of the two 64-column panels of M
 //     (p-contiguous columns, exactly the Fortran cprod layout) into shared
 //     memory with 1-D bulk TMA copies, one per column, plus the 16 weights,
-//     one stage ahead of the math; a CTA barrier releases each stage;
+//     one stage ahead of the math; each warp releases a stage on an mbarrier
+//     when it is done with it, and only warp 0 waits for that before refilling;
 //   * four warps each own a 32x32 complex sub-tile and run
 //     mma.sync m16n8kKI f64 on re/im planes: re += ar*(w br) + ai*(w bi),
 //     im += ai*(w br) - ar*(w bi);
@@ -56,6 +57,7 @@ struct __align__(16) F64Smem {
   double2 b[F64_ST][F64_B][F64_ROW];
   double w[F64_ST][F64_KC];
   uint64_t full[F64_ST];
+  uint64_t empty[F64_ST];  // every warp has finished with the stage
 };
 
 // Upper-triangle tile t -> (bi, bj), bi <= bj, column-major over the triangle.
@@ -129,7 +131,10 @@ __global__ void __launch_bounds__(F64_THREADS, 2) chi0_fp64_kernel(F64Params prm
   for (int t = threadIdx.x; t < 2 * F64_ST * F64_B * F64_ROW; t += blockDim.x)
     reinterpret_cast<double2*>(smem_raw)[t] = make_double2(0.0, 0.0);
   if (threadIdx.x == 0) {
-    for (int s = 0; s < F64_ST; ++s) mbar_init(&sm.full[s], 1);
+    for (int s = 0; s < F64_ST; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], F64_WARPS);
+    }
     fence_barrier_init();
   }
   __syncthreads();
@@ -143,8 +148,10 @@ __global__ void __launch_bounds__(F64_THREADS, 2) chi0_fp64_kernel(F64Params prm
   const int64_t total = my_items * nchunk;
   auto chunk_item = [&](int64_t c) { return blockIdx.x + (c / nchunk) * (int64_t)gridDim.x; };
   auto chunk_p0 = [&](int64_t c) { return (c % nchunk) * (int64_t)F64_KC; };
+  // chunks [0, issued) have their copies issued (tracked by warp 0)
+  int64_t issued = total < F64_ST - 1 ? total : (int64_t)(F64_ST - 1);
   if (warp == 0)
-    for (int64_t c = 0; c < F64_ST - 1 && c < total; ++c)
+    for (int64_t c = 0; c < issued; ++c)
       f64_issue(sm, prm, (int)(c % F64_ST), chunk_item(c), chunk_p0(c), lane);
 
   const int wi = warp & 1, wj = warp >> 1;
@@ -165,10 +172,22 @@ __global__ void __launch_bounds__(F64_THREADS, 2) chi0_fp64_kernel(F64Params prm
 #pragma unroll
           for (int r = 0; r < 4; ++r) accR[mt][nt][r] = accI[mt][nt][r] = 0.0;
     }
-    // stage (c-1) % F64_ST was released by the barrier at the end of chunk c-1
-    if (warp == 0 && c + F64_ST - 1 < total)
+    // chunk c + F64_ST - 1 goes into the stage of chunk c - 1, once all four warps
+    // have released that one (its release completes phase (c-1)/F64_ST of empty)
+    if (warp == 0 && c + F64_ST - 1 < total) {
+      const int64_t prev = c - 1;
+      int ok = 1;
+      if (prev >= 0 && lane == 0)
+        ok = mbar_wait(&sm.empty[(int)(prev % F64_ST)], (uint32_t)((prev / F64_ST) & 1),
+                       prm.timeout_ns, prm.status);
+      if (!__shfl_sync(0xffffffffu, ok, 0)) {
+        failed = true;
+        break;
+      }
       f64_issue(sm, prm, (int)((c + F64_ST - 1) % F64_ST), chunk_item(c + F64_ST - 1),
                 chunk_p0(c + F64_ST - 1), lane);
+      issued = c + F64_ST;
+    }
     if (!mbar_wait(&sm.full[st], ph, prm.timeout_ns, prm.status)) {
       failed = true;
       break;
@@ -222,7 +241,9 @@ __global__ void __launch_bounds__(F64_THREADS, 2) chi0_fp64_kernel(F64Params prm
         }
       }
     }
-    __syncthreads();  // every warp is done with stage st
+    // this warp is done with stage st; only the issuing warp waits for all four
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sm.empty[st]);
 
     if (p0 + F64_KC >= prm.P) {
       // last slab of this item: add the tile into the packed upper triangle
@@ -251,7 +272,7 @@ __global__ void __launch_bounds__(F64_THREADS, 2) chi0_fp64_kernel(F64Params prm
   }
   if (failed && warp == 0) {
     // never leave with bulk copies still landing in this CTA's shared memory
-    for (int64_t k = c; k < c + F64_ST && k < total; ++k)
+    for (int64_t k = c; k < issued; ++k)
       mbar_drain(&sm.full[(int)(k % F64_ST)], (uint32_t)((k / F64_ST) & 1), prm.timeout_ns);
   }
 }
