@@ -141,6 +141,15 @@ module spex_gpu
       type(spx_chi0_stats), intent(out) :: stats
     end function
 
+    ! transform to the Coulomb eigenbasis, src/susceptibility.f:806-832 (device arrays)
+    integer(c_int) function spx_trafo_dev(ctx, cprod, ldc, npair, nbas, ctrafo, ldt, dim, out, &
+                                          ldo, stream) bind(c, name='spx_trafo_dev')
+      import :: c_int, c_int32_t, c_int64_t, c_ptr
+      type(c_ptr), value :: ctx, cprod, ctrafo, out, stream
+      integer(c_int64_t), value :: ldc, npair, ldt, ldo
+      integer(c_int32_t), value :: nbas, dim
+    end function
+
     ! the q loop around susceptibility, src/correlation.f:293-339
     integer(c_int) function spx_chi0_batched(ctx, nq, q, nw, omega, precision, flags, stream, &
                                              stats) bind(c, name='spx_chi0_batched')

@@ -214,6 +214,17 @@ int spx_chi0_from_coeffs_dev(spx_ctx* ctx, const spx_mt_desc* mt, const spx_pw_d
                              int32_t nw, const double* omega, int32_t precision,
                              double* susceph, void* stream, spx_chi0_stats* stats);
 
+/* ---- transform to the Coulomb eigenbasis ------------------------------------
+ * Replaces src/susceptibility.f:806-832 (the FULLPW branch of the complex build):
+ * cprod(:, :dim) = conj(conj(cprod) * ctrafo), i.e.
+ *   out(p, j) = sum_{i < nbas} cprod(p, i) * conj(ctrafo(i, j)),  p < npair, j < dim.
+ * Column-major device arrays: cprod (ldc, nbas), ctrafo (ldt, dim), out (ldo, dim).
+ * out may be cprod itself (in place, as in the reference; then ldo == ldc); a
+ * partial overlap is rejected. FP64 on the DMMA path. Ordered on `stream`. */
+int spx_trafo_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
+                  int32_t nbas, const double* ctrafo, int64_t ldt, int32_t dim,
+                  double* out, int64_t ldo, void* stream);
+
 /* ---- many q points in one launch (K7) ---------------------------------------
  * The q loop of the reference driver (src/correlation.f:293-339 calls
  * `susceptibility` once per q point) as one call: every q has its own N_MB,

@@ -170,3 +170,12 @@ def wfprod_pw_fft(pw, nk, nocc, nunocc, cpw_occ, cpw_unocc, nfft):
                 res[k, n, npr] = prod[out_idx]
     # layout p = n' + nu*(n + no*k)
     return res.reshape(nk * nocc * nunocc, -1)
+
+
+def trafo(cprod, ctrafo, dim=None):
+    """Transform to the Coulomb eigenbasis as src/susceptibility.f:806-832 writes it for
+    the complex build with FULLPW: cprod(:, :dim) = conj(matmul(conj(cprod), ctrafo))."""
+    c = np.asarray(cprod)
+    t = np.asarray(ctrafo)
+    dim = t.shape[1] if dim is None else dim
+    return np.conj(np.conj(c) @ t[:, :dim])

@@ -43,9 +43,11 @@ constexpr int ZG_ROW = ZG_KC + 4;    // padded shared row, double2 units
 constexpr int ZG_THREADS = 128;
 
 struct ZgParams {
-  // A_b(m, k) = A[b1*sA1 + b2*sA2 + m*lda + k]
+  // A_b(m, k) = A[b1*sA1 + b2*sA2 + m*lda + k], or with a_mcontig
+  // A[b1*sA1 + b2*sA2 + m + k*lda] (a Fortran column-major panel)
   const double2* A;
   int64_t lda, sA1, sA2;
+  int a_mcontig;
   // B_b(col, k) = B[b1*sB1 + b2*sB2 + colOff(col) + kOff(k)], col = n*ncin + c,
   // colOff = n*sBn + (cOff ? cOff[c] : c*sBc), kOff = kOff ? kOff[k] : k
   const double2* B;
@@ -55,7 +57,8 @@ struct ZgParams {
   // O_b(m, col) = O[b1*sO1 + b2*sO2 + m + n*sOn + c*sOc]
   double2* O;
   int64_t sO1, sO2, sOn, sOc;
-  const double2* alpha;  // per b1
+  const double2* alpha;  // per b1, or null: alpha_v
+  double2 alpha_v;
   int M, ncol, ncin, K, nb1;
   int mtiles, ntiles;
 };
@@ -99,7 +102,8 @@ __global__ void __launch_bounds__(ZG_THREADS, 2) zgemm_gather_kernel(ZgParams pr
   // loader role: thread -> (row r, 8 consecutive k); rows of A are m, rows of B col
   const int lr = threadIdx.x >> 1, lk = (threadIdx.x & 1) * 8;
   const bool a_ok = m0 + lr < prm.M;
-  const double2* a_row = prm.A + b1 * prm.sA1 + b2 * prm.sA2 + (int64_t)(a_ok ? m0 + lr : 0) * prm.lda;
+  const int64_t a_mstride = prm.a_mcontig ? 1 : prm.lda, a_kstride = prm.a_mcontig ? prm.lda : 1;
+  const double2* a_row = prm.A + b1 * prm.sA1 + b2 * prm.sA2 + (int64_t)(a_ok ? m0 + lr : 0) * a_mstride;
   const int col = c0 + lr;
   const bool b_ok = col < prm.ncol;
   const double2* b_row;
@@ -115,7 +119,7 @@ __global__ void __launch_bounds__(ZG_THREADS, 2) zgemm_gather_kernel(ZgParams pr
       const int k = k0 + lk + j;
       const bool kin = k < prm.K;
       const int kk = kin ? k : 0;
-      cp_async16(&sm.a[st][lr][lk + j], a_row + kk, a_ok && kin);
+      cp_async16(&sm.a[st][lr][lk + j], a_row + kk * a_kstride, a_ok && kin);
       const int64_t ko = prm.kOff ? (int64_t)__ldg(prm.kOff + kk) : (int64_t)kk;
       cp_async16(&sm.b[st][lr][lk + j], b_ok && kin ? b_row + ko : prm.B, b_ok && kin);
     }
@@ -184,7 +188,7 @@ __global__ void __launch_bounds__(ZG_THREADS, 2) zgemm_gather_kernel(ZgParams pr
     __syncthreads();  // stage st is refilled by the next iteration's issue
   }
 
-  const double2 al = prm.alpha[b1];
+  const double2 al = prm.alpha ? prm.alpha[b1] : prm.alpha_v;
   double2* ob = prm.O + b1 * prm.sO1 + b2 * prm.sO2;
 #pragma unroll
   for (int nt = 0; nt < 4; ++nt)
@@ -731,4 +735,75 @@ extern "C" int spx_wfprod_pw_dev(spx_ctx* ctx, const spx_pw_desc* pw, int32_t nk
   return wfprod_pw_run(ctx, pw, nk, nocc, nunocc, reinterpret_cast<const double2*>(cpw_occ),
                        reinterpret_cast<const double2*>(cpw_unocc), reinterpret_cast<double2*>(cprod),
                        ldc, col0, ctx->ws, ctx->ws_bytes, s, &launches, split);
+}
+
+// ---------------------------------------------------------------------------
+// Transform to the Coulomb eigenbasis (src/susceptibility.f:806-832, FULLPW branch of
+// the complex build): cprod(:, :dim) = conj(conj(cprod) ctrafo), i.e.
+//   out(p, j) = sum_i cprod(p, i) conj(ctrafo(i, j)),
+// which is K4c with the p-contiguous cprod panel as A and the columns of ctrafo as
+// the rows of B. In place (out == cprod), rows go through a scratch panel in chunks,
+// as the reference's row blocks do, so that no output overwrites an input still read.
+
+extern "C" int spx_trafo_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
+                             int32_t nbas, const double* ctrafo, int64_t ldt, int32_t dim,
+                             double* out, int64_t ldo, void* stream) {
+  if (!ctx) return SPX_EINVAL;
+  if (npair < 0 || nbas < 0 || dim < 0) return set_error(ctx, SPX_EINVAL, "negative size");
+  if (npair == 0 || dim == 0) return SPX_OK;
+  if (!cprod || !out || (nbas > 0 && !ctrafo)) return set_error(ctx, SPX_EINVAL, "null array argument");
+  if (ldc < npair || ldo < npair || ldt < nbas) return set_error(ctx, SPX_EINVAL, "leading dimension too small");
+  if (out == cprod && ldo != ldc) return set_error(ctx, SPX_EINVAL, "in place needs ldo == ldc");
+  if (out != cprod) {
+    // a partial overlap of the two panels would let outputs overwrite inputs
+    const char* a0 = (const char*)cprod;
+    const char* a1 = a0 + 16 * (size_t)(ldc * (nbas - 1) + npair);
+    const char* b0 = (const char*)out;
+    const char* b1 = b0 + 16 * (size_t)(ldo * (dim - 1) + npair);
+    if (nbas > 0 && a0 < b1 && b0 < a1) return set_error(ctx, SPX_EINVAL, "cprod and out overlap");
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = pick_stream(ctx, stream);
+  int rc;
+  ZgParams prm{};
+  prm.a_mcontig = 1;
+  prm.lda = ldc;
+  prm.B = reinterpret_cast<const double2*>(ctrafo);
+  prm.sBc = ldt;
+  prm.ncin = dim;
+  prm.alpha_v = make_double2(1.0, 0.0);
+  prm.ncol = dim;
+  prm.K = nbas;
+  prm.nb1 = 1;
+  if (out != cprod) {
+    if ((rc = check_cuda(ctx, cudaMemset2DAsync(out, 16 * ldo, 0, 16 * npair, dim, s), "zero out")))
+      return rc;
+    if (nbas == 0) return SPX_OK;
+    prm.A = reinterpret_cast<const double2*>(cprod);
+    prm.O = reinterpret_cast<double2*>(out);
+    prm.sOc = ldo;
+    prm.M = (int)std::min<int64_t>(npair, 2147483647);
+    if (npair > 2147483647) return set_error(ctx, SPX_EINVAL, "npair too large");
+    return launch_zgemm(ctx, prm, 1, s);
+  }
+  // in place: row chunks through the workspace
+  const int64_t chunk = std::min<int64_t>(npair, 65536);
+  if ((rc = ensure_workspace(ctx, 16 * (size_t)chunk * std::max(dim, 1) + 256))) return rc;
+  double2* tmp = reinterpret_cast<double2*>(ctx->ws);
+  for (int64_t r0 = 0; r0 < npair; r0 += chunk) {
+    const int64_t len = std::min<int64_t>(chunk, npair - r0);
+    if ((rc = check_cuda(ctx, cudaMemsetAsync(tmp, 0, 16 * (size_t)len * dim, s), "zero chunk")))
+      return rc;
+    if (nbas > 0) {
+      prm.A = reinterpret_cast<const double2*>(cprod) + r0;
+      prm.O = tmp;
+      prm.sOc = len;
+      prm.M = (int)len;
+      if ((rc = launch_zgemm(ctx, prm, 1, s))) return rc;
+    }
+    if ((rc = check_cuda(ctx, cudaMemcpy2DAsync(out + 2 * r0, 16 * ldo, tmp, 16 * len, 16 * len, dim,
+                                                cudaMemcpyDeviceToDevice, s), "copy chunk")))
+      return rc;
+  }
+  return SPX_OK;
 }

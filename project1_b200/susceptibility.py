@@ -165,6 +165,22 @@ class Context:
         rc = self.lib.spx_scale_dev(self.handle, _ptr(z), z.numel(), factor, torch_stream(stream, z))
         self._check(rc, "spx_scale_dev")
 
+    # ---- transform to the Coulomb eigenbasis -----------------------------------------
+
+    def trafo_dev(self, cprod, ctrafo, out=None, npair: Optional[int] = None, stream=None):
+        """out(p, j) = sum_i cprod(p, i) conj(ctrafo(i, j)) (src/susceptibility.f:806-832).
+
+        cprod: complex128 (nbas, ldc) == Fortran (ldc, nbas); ctrafo: (dim, ldt) ==
+        Fortran (ldt, dim); out: (dim, ldo) or None for in place (then dim <= nbas)."""
+        nbas, ldc = cprod.shape
+        dim, ldt = ctrafo.shape
+        npair = ldc if npair is None else npair
+        o = cprod if out is None else out
+        rc = self.lib.spx_trafo_dev(self.handle, _ptr(cprod), ldc, npair, nbas, _ptr(ctrafo), ldt,
+                                    dim, _ptr(o), o.shape[1], torch_stream(stream, cprod))
+        self._check(rc, "spx_trafo_dev")
+        return o
+
     # ---- many q points in one launch ---------------------------------------------
 
     def chi0_batched(self, qs, omega, precision: str = "split", flags: int = 0, stream=None,

@@ -65,3 +65,12 @@ def test_linearity_in_weights():
     m, d, om, ws, w, ref = case("tiny")
     a = oracle.chi0(m, 2.5 * w)
     np.testing.assert_allclose(a, 2.5 * ref, rtol=1e-13, atol=1e-17)
+
+
+def test_trafo_oracle_is_the_reference_formula():
+    """conj(conj(M) T) equals M conj(T): the two forms of src/susceptibility.f:806-832."""
+    rng = np.random.default_rng(1)
+    m = rng.standard_normal((30, 8)) + 1j * rng.standard_normal((30, 8))
+    t = rng.standard_normal((8, 5)) + 1j * rng.standard_normal((8, 5))
+    assert np.allclose(oracle.trafo(m, t), m @ np.conj(t), rtol=0, atol=1e-14)
+    assert np.allclose(oracle.trafo(m, t, dim=3), (m @ np.conj(t))[:, :3], rtol=0, atol=1e-14)

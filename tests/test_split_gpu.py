@@ -108,3 +108,19 @@ def test_split_cta_pair_equals_single_cta(nbas, npair, nw):
     ref = oracle.chi0(m, oracle.weights(d, om, None, 0.5), accurate=True)
     emax, fro = normalized_error(outs[1], ref, nbas)
     assert emax <= SPLIT_TOL and fro <= SPLIT_FRO, (emax, fro)
+
+
+def test_split_host_ramp_equals_device_path(ctx):
+    """With default chunking, the host-pointer call streams chunks of 32768, 65536,
+    98304, ... pairs. They fall on the 32768-pair exact slabs of the split path, so
+    its result equals the device call's bit for bit (pinned source)."""
+    nbas, npair = 72, 150000
+    m, d, om = random_case(nbas, npair, 2, seed=21, degfrac=0.01)
+    dev = run_dev(ctx, m, d, om, None, 0.5, precision="split")
+    t = torch.from_numpy(np.ascontiguousarray(m.T)).pin_memory()
+    out = np.zeros((nbas * (nbas + 1) // 2, 2), complex, order="F")
+    with spx.Context(0) as c:
+        st = c.chi0_accumulate_host_ptr(t.data_ptr(), npair, npair, nbas, d, om, out,
+                                        scale_all=0.5, precision="split")
+    assert st["h2d_bytes"] >= m.nbytes
+    assert np.array_equal(out, dev)
