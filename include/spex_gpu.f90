@@ -141,6 +141,25 @@ module spex_gpu
       type(spx_chi0_stats), intent(out) :: stats
     end function
 
+    ! Hilbert-mesh weights, src/susceptibility.f:996-1078 + src/hilbert.f:193-300
+    integer(c_int) function spx_weights_hilbert_dev(ctx, npair, nfrqs, wtetra, ldt, thr, nw, wghtSr, &
+                                                    scale_all, w, ldw, stream) bind(c, name='spx_weights_hilbert_dev')
+      import :: c_int, c_int32_t, c_int64_t, c_ptr, c_double
+      type(c_ptr), value :: ctx, wtetra, wghtSr, w, stream
+      integer(c_int64_t), value :: npair, ldt, ldw
+      integer(c_int32_t), value :: nfrqs, nw
+      real(c_double), value :: thr, scale_all
+    end function
+
+    integer(c_int) function spx_chi0_accumulate_w_dev(ctx, cprod, ldc, npair, nbas, w, ldw, nw, &
+        precision, susceph, stream, stats) bind(c, name='spx_chi0_accumulate_w_dev')
+      import :: c_int, c_int32_t, c_int64_t, c_ptr, spx_chi0_stats
+      type(c_ptr), value :: ctx, cprod, w, susceph, stream
+      integer(c_int64_t), value :: ldc, npair, ldw
+      integer(c_int32_t), value :: nbas, nw, precision
+      type(spx_chi0_stats), intent(out) :: stats
+    end function
+
     ! transform to the Coulomb eigenbasis, src/susceptibility.f:806-832 (device arrays)
     integer(c_int) function spx_trafo_dev(ctx, cprod, ldc, npair, nbas, ctrafo, ldt, dim, out, &
                                           ldo, stream) bind(c, name='spx_trafo_dev')

@@ -214,6 +214,23 @@ int spx_chi0_from_coeffs_dev(spx_ctx* ctx, const spx_mt_desc* mt, const spx_pw_d
                              int32_t nw, const double* omega, int32_t precision,
                              double* susceph, void* stream, spx_chi0_stats* stats);
 
+/* ---- Hilbert-mesh path, imaginary axis -------------------------------------
+ * The default HILBERT path accumulates the spectral function on a frequency mesh
+ * (tetrahedron weights wtetra(p, s), src/susceptibility.f:996-1078) and
+ * Hilbert-transforms it with the getwghtS weights (src/hilbert.f:193-300). For
+ * imaginary frequencies the two collapse into effective pair weights
+ *   w(p, f) = scale_all * sum_s [wtetra(p, s) > thr] wtetra(p, s) * wghtSr(s, f),
+ * which spx_chi0_accumulate_w_dev then accumulates (weights of any sign).
+ * Device arrays: wtetra (ldt, nfrqs), wghtSr (nfrqs, nw), w (ldw, nw);
+ * nfrqs * nw <= 25600. */
+int spx_weights_hilbert_dev(spx_ctx* ctx, int64_t npair, int32_t nfrqs, const double* wtetra,
+                            int64_t ldt, double thr, int32_t nw, const double* wghtSr,
+                            double scale_all, double* w, int64_t ldw, void* stream);
+int spx_chi0_accumulate_w_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
+                              int32_t nbas, const double* w, int64_t ldw, int32_t nw,
+                              int32_t precision, double* susceph, void* stream,
+                              spx_chi0_stats* stats);
+
 /* ---- transform to the Coulomb eigenbasis ------------------------------------
  * Replaces src/susceptibility.f:806-832 (the FULLPW branch of the complex build):
  * cprod(:, :dim) = conj(conj(cprod) * ctrafo), i.e.

@@ -179,3 +179,98 @@ def trafo(cprod, ctrafo, dim=None):
     t = np.asarray(ctrafo)
     dim = t.shape[1] if dim is None else dim
     return np.conj(np.conj(c) @ t[:, :dim])
+
+
+def _ln(z: complex) -> complex:
+    """Principal logarithm as src/hilbert.f:283-296 defines it: a real negative argument
+    gives +i pi whatever the sign of its zero imaginary part."""
+    import cmath
+    if z.real < 0 and z.imag == 0:
+        return complex(np.log(-z.real), np.pi)
+    return cmath.log(z)
+
+
+def getwghtS(frq, frqs, disorder=0.0, md=0, iterm=0):
+    """Hilbert-transform weights of a spectral function given on the mesh frqs, for the
+    frequencies frq: chi(w) = sum_s S(frqs_s) wghtS(s, w). Restates getwghtS,
+    src/hilbert.f:193-281, step by step (1-based mesh indices kept as in the source;
+    i = 0 is the interval before the first mesh point). Returns (wghtSr, wghtSi),
+    each (nfrqs, nfrq)."""
+    frq = np.asarray(frq, dtype=complex)
+    frqs = np.asarray(frqs, dtype=float)
+    nfrq, nfrqs = frq.size, frqs.size
+    wr = np.zeros((nfrqs, nfrq))
+    wi = np.zeros((nfrqs, nfrq))
+    if nfrq == 0:
+        return wr, wi
+    F = lambda i: frqs[i - 1]                      # 1-based access
+    winc = F(2) - F(1)
+    a = 0.5
+    if nfrqs >= 3:
+        a = winc / (F(3) - F(1))
+    img = 1j
+    isign = -1 if iterm == 2 else 1
+    while True:
+        for j in range(nfrq):
+            w = frq[j] * isign
+            i2 = 1 if F(1) == 0 else 0
+            while i2 < nfrqs:
+                i1 = i2
+                rdum = abs(w - F(i1 + 1))
+                if rdum > min(winc / 3, 1e-6):
+                    i2 = i1 + 1
+                else:
+                    i2 = i1 + 2
+                    if i2 > nfrqs:
+                        break
+                w1 = max(0.0, F(i1 + 1) - a * winc) if i1 == 0 else F(i1)
+                w2 = F(i2)
+                int1 = int2 = 0j
+                cdum = 0j
+                rdum = rdum1 = rdum2 = 0.0
+                if w + w1 - img * disorder != 0:
+                    cdum = _ln(w - w1 + img * disorder) - _ln(w - w2 + img * disorder)
+                if w1 != 0 and md > 0:
+                    rdum = np.log(w2) - np.log(w1)
+                    rdum1 = w2 ** -1 - w1 ** -1
+                    rdum2 = (w2 ** -2 - w1 ** -2) / 2
+                if md == 0:
+                    int1 = cdum
+                    int2 = cdum * (w + img * disorder) - (w2 - w1)
+                elif md == 1:
+                    int2 = cdum
+                    int1 = (cdum + rdum) / (w + img * disorder) if w - img * disorder != 0 else rdum1
+                elif md == 2:
+                    if w - img * disorder != 0:
+                        int2 = (cdum + rdum) / (w + img * disorder)
+                        int1 = (int2 + rdum1) / (w + img * disorder)
+                    else:
+                        int2 = rdum1
+                        int1 = rdum2
+                if i2 - i1 == 1:
+                    c = (w2 * int1 - int2) / (w2 - w1)
+                    if i1 > 0:
+                        wr[i1 - 1, j] += c.real
+                        wi[i1 - 1, j] += c.imag
+                    c = (int2 - w1 * int1) / (w2 - w1)
+                    wr[i2 - 1, j] += c.real
+                    wi[i2 - 1, j] += c.imag
+                else:
+                    if i1 > 0:
+                        wr[i1 - 1, j] += isign
+                    i1 += 1
+                    wr[i1 - 1, j] += np.real(int1)
+                    wi[i1 - 1, j] += np.imag(int1)
+                    wr[i2 - 1, j] = wr[i1 - 1, j] - isign
+        if iterm == 0 and isign == 1:
+            isign = -1
+            continue
+        return wr, wi
+
+
+def hilbert_weights(wtetra, wghtSr, thr=0.0, scale_all=1.0):
+    """Effective imaginary-axis weights of the Hilbert-mesh path:
+    w_eff(p, f) = scale_all * sum_s wtetra(p, s) wghtSr(s, f), weights <= thr dropped as
+    the index lists of src/susceptibility.f:1066-1075 drop them."""
+    wt = np.where(np.asarray(wtetra) > thr, wtetra, 0.0)
+    return scale_all * (wt @ np.asarray(wghtSr))

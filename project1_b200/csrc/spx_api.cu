@@ -26,6 +26,8 @@ namespace spx {
 int launch_weights(spx_ctx*, int64_t, int64_t, const double*, const double*, double, int,
                    const double*, double*, cudaStream_t);
 int launch_scale(spx_ctx*, double*, int64_t, double, cudaStream_t);
+int launch_hilbert_weights(spx_ctx*, int64_t, int, int, const double*, int64_t, const double*,
+                           double, double, double*, int64_t, cudaStream_t);
 int launch_gen_normal(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, double, double*,
                       cudaStream_t);
 int launch_gen_cmatrix(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, int64_t, int64_t,
@@ -617,6 +619,78 @@ extern "C" int spx_chi0_from_coeffs_dev(spx_ctx* ctx, const spx_mt_desc* mt,
     rc = collect_status(ctx, s, "chi0_from_coeffs_dev");
     if (rc) return rc;
     // the products count as preparation: everything before the first accumulation mark
+    timing_collect(ctx, &stats->ms_prep, &stats->ms_gram);
+    stats->kernel_launches = launches;
+    stats->ms_total =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return SPX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Hilbert-mesh weights and the accumulation with caller-given weights
+
+extern "C" int spx_weights_hilbert_dev(spx_ctx* ctx, int64_t npair, int32_t nfrqs,
+                                       const double* wtetra, int64_t ldt, double thr, int32_t nw,
+                                       const double* wghtSr, double scale_all, double* w,
+                                       int64_t ldw, void* stream) {
+  if (!ctx) return SPX_EINVAL;
+  if (npair < 0 || nfrqs < 0 || nw < 0) return set_error(ctx, SPX_EINVAL, "negative size");
+  if (npair == 0 || nw == 0) return SPX_OK;
+  if (!w || (nfrqs > 0 && (!wtetra || !wghtSr))) return set_error(ctx, SPX_EINVAL, "null array argument");
+  if (ldw < npair || (nfrqs > 0 && ldt < npair)) return set_error(ctx, SPX_EINVAL, "leading dimension too small");
+  cudaSetDevice(ctx->device);
+  return launch_hilbert_weights(ctx, npair, nfrqs, nw, wtetra, ldt, wghtSr, thr, scale_all, w, ldw,
+                                pick_stream(ctx, stream));
+}
+
+extern "C" int spx_chi0_accumulate_w_dev(spx_ctx* ctx, const double* cprod, int64_t ldc,
+                                         int64_t npair, int32_t nbas, const double* w, int64_t ldw,
+                                         int32_t nw, int32_t precision, double* susceph,
+                                         void* stream, spx_chi0_stats* stats) {
+  // the shared argument check, with w standing in for ediff and omega
+  int rc = check_chi0_args(ctx, cprod, ldc, npair, nbas, w, nw, w, precision, susceph);
+  if (rc) return rc;
+  if (npair > 0 && nw > 0 && ldw < npair) return set_error(ctx, SPX_EINVAL, "ldw < npair");
+  cudaSetDevice(ctx->device);
+  auto t0 = std::chrono::steady_clock::now();
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->precision = precision;
+    stats->flops = 8.0 * (double)nbas * nbas * (double)npair * nw;
+  }
+  if (npair == 0 || nbas == 0 || nw == 0) return SPX_OK;
+  cudaStream_t s = pick_stream(ctx, stream);
+  // the kernels read the weights with 16-pair bulk copies: an aligned, padded copy
+  const int64_t ldi = (int64_t)align_up((size_t)npair, 16);
+  const size_t wbytes = align_up(sizeof(double) * (size_t)ldi * nw, 256);
+  const size_t sbytes = precision == SPX_SPLIT ? split_workspace_bytes(npair, nbas, nw) : 0;
+  if ((rc = ensure_workspace(ctx, wbytes + sbytes))) return rc;
+  double* W = (double*)ctx->ws;
+  void* sws = (char*)ctx->ws + wbytes;
+  if ((rc = check_cuda(ctx, cudaMemsetAsync(W, 0, wbytes, s), "zero weights")) ||
+      (rc = check_cuda(ctx, cudaMemcpy2DAsync(W, sizeof(double) * ldi, w, sizeof(double) * ldw,
+                                              sizeof(double) * npair, nw, cudaMemcpyDeviceToDevice, s),
+                       "copy weights")))
+    return rc;
+  int launches = 0;
+  ctx->timing = stats != nullptr;
+  ctx->nmarks = 0;
+  if (precision == SPX_FP64) {
+    timing_mark(ctx, s, 1);
+    rc = launch_chi0_fp64(ctx, reinterpret_cast<const double2*>(cprod), ldc, npair, nbas, W, ldi, nw,
+                          reinterpret_cast<double2*>(susceph), s, 8);
+    ++launches;
+  } else {
+    rc = split_chi0_slab(ctx, reinterpret_cast<const double2*>(cprod), ldc, npair, nbas, W, ldi, nw,
+                         reinterpret_cast<double2*>(susceph), sws, sbytes, s, &launches, 0, 0);
+  }
+  timing_mark(ctx, s, 2);
+  ctx->timing = false;
+  if (rc) return rc;
+  if (stats) {
+    rc = collect_status(ctx, s, "chi0_accumulate_w_dev");
+    if (rc) return rc;
     timing_collect(ctx, &stats->ms_prep, &stats->ms_gram);
     stats->kernel_launches = launches;
     stats->ms_total =

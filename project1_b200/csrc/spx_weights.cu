@@ -143,4 +143,49 @@ int launch_weights_noctx(int num_sms, int64_t P, int64_t ldw, const double* edif
   return cudaGetLastError() == cudaSuccess ? SPX_OK : SPX_ECUDA;
 }
 
+
+// Effective imaginary-axis weights of the Hilbert-mesh path:
+//   w(p, f) = scale * sum_s [wtetra(p, s) > thr] wtetra(p, s) * wghtSr(s, f)
+// (the spectral function on the mesh, src/susceptibility.f:996-1078, followed by the
+// Hilbert weights of src/hilbert.f:193-300). One thread per pair, the weight table
+// in shared memory, frequencies in groups of 8 accumulators.
+__global__ void hilbert_weights_kernel(int64_t P, int S, int nw, const double* __restrict__ wt,
+                                       int64_t ldt, const double* __restrict__ ws, double thr,
+                                       double scale, double* __restrict__ W, int64_t ldw) {
+  extern __shared__ double sws[];
+  for (int i = threadIdx.x; i < S * nw; i += blockDim.x) sws[i] = ws[i];
+  __syncthreads();
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    for (int f0 = 0; f0 < nw; f0 += 8) {
+      double acc[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc[k] = 0.0;
+      for (int s = 0; s < S; ++s) {
+        const double v = wt[p + ldt * s];
+        if (!(v > thr)) continue;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (f0 + k < nw) acc[k] = fma(v, sws[s + S * (f0 + k)], acc[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (f0 + k < nw) W[p + ldw * (f0 + k)] = scale * acc[k];
+    }
+  }
+}
+
+int launch_hilbert_weights(spx_ctx* ctx, int64_t P, int S, int nw, const double* wt, int64_t ldt,
+                           const double* ws, double thr, double scale, double* W, int64_t ldw,
+                           cudaStream_t stream) {
+  if (P <= 0 || nw <= 0) return SPX_OK;
+  const size_t smem = sizeof(double) * (size_t)S * nw;
+  if (smem > 200 * 1024)
+    return set_error(ctx, SPX_EINVAL, "nfrqs * nw too large (at most 25600 weights)");
+  cudaFuncSetAttribute(hilbert_weights_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int grid = (int)std::min<int64_t>((P + 255) / 256, (int64_t)ctx->num_sms * 8);
+  hilbert_weights_kernel<<<grid, 256, smem, stream>>>(P, S, nw, wt, ldt, ws, thr, scale, W, ldw);
+  return check_cuda(ctx, cudaGetLastError(), "hilbert_weights_kernel launch");
+}
+
 }  // namespace spx

@@ -165,6 +165,35 @@ class Context:
         rc = self.lib.spx_scale_dev(self.handle, _ptr(z), z.numel(), factor, torch_stream(stream, z))
         self._check(rc, "spx_scale_dev")
 
+    # ---- Hilbert-mesh weights and caller-given weights ----------------------------
+
+    def weights_hilbert_dev(self, wtetra, wghtSr, w, thr: float = 0.0, scale_all: float = 1.0,
+                            npair: Optional[int] = None, stream=None) -> None:
+        """w(p, f) = scale_all sum_s [wtetra > thr] wtetra(p, s) wghtSr(s, f).
+
+        wtetra: float64 (nfrqs, ldt) == Fortran (ldt, nfrqs); wghtSr: (nw, nfrqs) ==
+        Fortran (nfrqs, nw); w: (nw, ldw) == Fortran (ldw, nw)."""
+        nfrqs, ldt = wtetra.shape
+        nw, ldw = w.shape
+        npair = ldt if npair is None else npair
+        rc = self.lib.spx_weights_hilbert_dev(self.handle, npair, nfrqs, _ptr(wtetra), ldt, thr, nw,
+                                              _ptr(wghtSr), scale_all, _ptr(w), ldw, torch_stream(stream, w))
+        self._check(rc, "spx_weights_hilbert_dev")
+
+    def chi0_accumulate_w_dev(self, cprod, w, susceph, precision: str = "fp64",
+                              npair: Optional[int] = None, stream=None, stats: bool = False):
+        """susceph += sum_p cprod(p,i) conj(cprod(p,j)) w(p,f) with given weights w (nw, ldw)."""
+        nbas, ldc = cprod.shape
+        nw, ldw = w.shape
+        npair = ldc if npair is None else npair
+        st = _lib.spx_chi0_stats() if stats else None
+        rc = self.lib.spx_chi0_accumulate_w_dev(self.handle, _ptr(cprod), ldc, npair, nbas, _ptr(w), ldw,
+                                                nw, PRECISIONS[precision], _ptr(susceph),
+                                                torch_stream(stream, susceph),
+                                                C.byref(st) if st is not None else None)
+        self._check(rc, "spx_chi0_accumulate_w_dev")
+        return _stats(st) if st is not None else None
+
     # ---- transform to the Coulomb eigenbasis -----------------------------------------
 
     def trafo_dev(self, cprod, ctrafo, out=None, npair: Optional[int] = None, stream=None):

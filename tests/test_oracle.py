@@ -74,3 +74,28 @@ def test_trafo_oracle_is_the_reference_formula():
     t = rng.standard_normal((8, 5)) + 1j * rng.standard_normal((8, 5))
     assert np.allclose(oracle.trafo(m, t), m @ np.conj(t), rtol=0, atol=1e-14)
     assert np.allclose(oracle.trafo(m, t, dim=3), (m @ np.conj(t))[:, :3], rtol=0, atol=1e-14)
+
+
+def test_getwghtS_hat_reproduces_the_pole_weight():
+    """A unit-area hat at a mesh point, transformed with the Hilbert weights of the
+    imaginary axis (both branches), gives the HILBERT NONE weight -2D/(w^2+D^2)."""
+    frqs = np.concatenate([[0.0], np.geomspace(1e-3, 60.0, 400)])
+    omega = np.array([0.3, 2.0, 15.0])
+    wr, wi = oracle.getwghtS(1j * omega, frqs, 0.0, 0, 0)
+    for s0 in (120, 250, 330):
+        D = frqs[s0]
+        hat = 2.0 / (frqs[s0 + 1] - frqs[s0 - 1])
+        w_eff = hat * wr[s0]
+        exact = -2 * D / (omega ** 2 + D ** 2)
+        assert np.allclose(w_eff, exact, rtol=2e-3, atol=0), (D, w_eff, exact)
+        # the Hermitian part carries no imaginary weight on the imaginary axis
+        assert np.abs(hat * wi[s0]).max() <= 1e-12 * np.abs(exact).max()
+
+
+def test_hilbert_weights_threshold():
+    rng = np.random.default_rng(0)
+    wt = rng.uniform(0, 1, (50, 7)) * (rng.uniform(0, 1, (50, 7)) > 0.5)
+    ws = rng.standard_normal((7, 3))
+    a = oracle.hilbert_weights(wt, ws, thr=0.3, scale_all=0.5)
+    b = 0.5 * np.where(wt > 0.3, wt, 0) @ ws
+    assert np.allclose(a, b)
