@@ -160,6 +160,15 @@ module spex_gpu
       type(spx_chi0_stats), intent(out) :: stats
     end function
 
+    ! q -> 0 head and wings, src/susceptibility.f:1092-1157 (device arrays)
+    integer(c_int) function spx_headwings_dev(ctx, cprod, ldc, npair, dim, dcprod, ldd, w, ldw, nw, &
+                                              head, wing, stream) bind(c, name='spx_headwings_dev')
+      import :: c_int, c_int32_t, c_int64_t, c_ptr
+      type(c_ptr), value :: ctx, cprod, dcprod, w, head, wing, stream
+      integer(c_int64_t), value :: ldc, npair, ldd, ldw
+      integer(c_int32_t), value :: dim, nw
+    end function
+
     ! transform to the Coulomb eigenbasis, src/susceptibility.f:806-832 (device arrays)
     integer(c_int) function spx_trafo_dev(ctx, cprod, ldc, npair, nbas, ctrafo, ldt, dim, out, &
                                           ldo, stream) bind(c, name='spx_trafo_dev')

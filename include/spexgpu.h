@@ -231,6 +231,18 @@ int spx_chi0_accumulate_w_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, in
                               int32_t precision, double* susceph, void* stream,
                               spx_chi0_stats* stats);
 
+/* ---- q -> 0 head and wings (FP64) --------------------------------------------
+ * Replaces src/susceptibility.f:1092-1157 for HILBERT NONE-style weights: with the
+ * momentum-matrix products dcprod(p, 1:3) (src/dwavefproducts.f),
+ *   head(ij(k1,k2), f) += sum_p dcprod(p,k1) conj(dcprod(p,k2)) w(p,f),  k1 <= k2,
+ *                         ij = k2(k2+1)/2 + k1 (0-based), head is (6, nw),
+ *   wing(k2, i, f)     += sum_p cprod(p,i) conj(dcprod(p,k2)) w(p,f), wing (3, dim, nw).
+ * Column-major complex device arrays: cprod (ldc, dim), dcprod (ldd, 3); w (ldw, nw)
+ * real. Always FP64 (complex DMMA, split over the pairs, summed in a fixed order). */
+int spx_headwings_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
+                      int32_t dim, const double* dcprod, int64_t ldd, const double* w,
+                      int64_t ldw, int32_t nw, double* head, double* wing, void* stream);
+
 /* ---- transform to the Coulomb eigenbasis ------------------------------------
  * Replaces src/susceptibility.f:806-832 (the FULLPW branch of the complex build):
  * cprod(:, :dim) = conj(conj(cprod) * ctrafo), i.e.

@@ -274,3 +274,22 @@ def hilbert_weights(wtetra, wghtSr, thr=0.0, scale_all=1.0):
     the index lists of src/susceptibility.f:1066-1075 drop them."""
     wt = np.where(np.asarray(wtetra) > thr, wtetra, 0.0)
     return scale_all * (wt @ np.asarray(wghtSr))
+
+
+def headwings(cprod, dcprod, w):
+    """Head (6, nw) and wings (3, dim, nw) as the loops of src/susceptibility.f:1092-1157
+    accumulate them with HILBERT NONE weights (the spectral_function sums of :1779-1782):
+    head(ij, f) = sum_p dcprod(p,k1) conj(dcprod(p,k2)) w(p,f), ij = k2(k2+1)/2 + k1, k1 <= k2;
+    wing(k2, i, f) = sum_p cprod(p,i) conj(dcprod(p,k2)) w(p,f)."""
+    c = np.asarray(cprod)
+    d = np.asarray(dcprod)
+    w = np.asarray(w)
+    nw = w.shape[1]
+    head = np.zeros((6, nw), complex)
+    for k2 in range(3):
+        for k1 in range(k2 + 1):
+            head[k2 * (k2 + 1) // 2 + k1] = (d[:, k1] * np.conj(d[:, k2])) @ w
+    wing = np.zeros((3, c.shape[1], nw), complex)
+    for k2 in range(3):
+        wing[k2] = (c * np.conj(d[:, k2])[:, None]).T @ w
+    return head, wing

@@ -60,6 +60,7 @@ struct ZgParams {
   const double2* alpha;  // per b1, or null: alpha_v
   double2 alpha_v;
   int M, ncol, ncin, K, nb1;
+  int K_last;  // K of the last batch when > 0 (split-K over batches)
   int mtiles, ntiles;
 };
 
@@ -98,6 +99,7 @@ __global__ void __launch_bounds__(ZG_THREADS, 2) zgemm_gather_kernel(ZgParams pr
   const int b = blockIdx.y;
   const int b1 = b % prm.nb1, b2 = b / prm.nb1;
   const int m0 = tm * ZG_B, c0 = tn * ZG_B;
+  const int Kb = (prm.K_last > 0 && b == (int)gridDim.y - 1) ? prm.K_last : prm.K;
 
   // loader role: thread -> (row r, 8 consecutive k); rows of A are m, rows of B col
   const int lr = threadIdx.x >> 1, lk = (threadIdx.x & 1) * 8;
@@ -117,7 +119,7 @@ __global__ void __launch_bounds__(ZG_THREADS, 2) zgemm_gather_kernel(ZgParams pr
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const int k = k0 + lk + j;
-      const bool kin = k < prm.K;
+      const bool kin = k < Kb;
       const int kk = kin ? k : 0;
       cp_async16(&sm.a[st][lr][lk + j], a_row + kk * a_kstride, a_ok && kin);
       const int64_t ko = prm.kOff ? (int64_t)__ldg(prm.kOff + kk) : (int64_t)kk;
@@ -126,7 +128,7 @@ __global__ void __launch_bounds__(ZG_THREADS, 2) zgemm_gather_kernel(ZgParams pr
     cp_async_commit();
   };
 
-  const int nst = (prm.K + ZG_KC - 1) / ZG_KC;
+  const int nst = (Kb + ZG_KC - 1) / ZG_KC;
   issue(0, 0);
 
   const int wi = warp & 1, wj = warp >> 1;
@@ -804,6 +806,129 @@ extern "C" int spx_trafo_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int
     if ((rc = check_cuda(ctx, cudaMemcpy2DAsync(out + 2 * r0, 16 * ldo, tmp, 16 * len, 16 * len, dim,
                                                 cudaMemcpyDeviceToDevice, s), "copy chunk")))
       return rc;
+  }
+  return SPX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// q -> 0 head and wings (src/susceptibility.f:1092-1157, HILBERT NONE), FP64:
+//   head(ij(k1,k2), f) += sum_p dcprod(p,k1) conj(dcprod(p,k2)) w(p,f),  k1 <= k2,
+//   wing(k2, i, f)     += sum_p cprod(p,i)  conj(dcprod(p,k2)) w(p,f).
+// Both are the rows k < 3 of the weighted Gram of X = [dcprod | cprod]: with the
+// 3 nw rows D(a,f; p) = dcprod(p,a) w(p,f) it is one complex GEMM D conj(X)^T with a
+// long K = P, run as K4c over K chunks into per-chunk partials that a second kernel
+// sums in a fixed order and scatters into head and wing.
+
+constexpr int HW_KC = 16384;   // pairs per K chunk
+
+__global__ void hw_rows_kernel(const double2* __restrict__ dc, int64_t ldd, const double* __restrict__ w,
+                               int64_t ldw, int64_t p0, int64_t len, int nw, double2* __restrict__ D,
+                               int64_t ldD) {
+  const int64_t total = (int64_t)3 * nw * len;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = t % len;
+    const int m = (int)(t / len), a = m / nw, f = m - a * nw;
+    const double2 v = dc[a * ldd + p0 + p];
+    const double ww = w[f * ldw + p0 + p];
+    D[m * ldD + p] = make_double2(v.x * ww, v.y * ww);
+  }
+}
+
+// out(m, col) = sum over chunks of part[c][m + M*col]; then scatter
+__global__ void hw_reduce_kernel(const double2* __restrict__ part, int nchunk, int nw, int ncol,
+                                 int dim, double2* __restrict__ head, double2* __restrict__ wing) {
+  const int M = 3 * nw;
+  const int64_t total = (int64_t)M * ncol;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    double sx = 0.0, sy = 0.0;
+    for (int c = 0; c < nchunk; ++c) {
+      const double2 v = part[(int64_t)c * total + t];
+      sx += v.x;
+      sy += v.y;
+    }
+    const int m = (int)(t % M), col = (int)(t / M);
+    const int a = m / nw, f = m - a * nw;
+    if (col < 3) {
+      if (a <= col) {
+        double2* o = head + (col * (col + 1) / 2 + a) + 6 * (int64_t)f;
+        o->x += sx;
+        o->y += sy;
+      }
+    } else {
+      const int i = col - 3;
+      double2* o = wing + a + 3 * ((int64_t)i + (int64_t)dim * f);
+      o->x += sx;
+      o->y -= sy;   // wing = conj of the Gram's (k2, 3 + i) element
+    }
+  }
+}
+
+extern "C" int spx_headwings_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
+                                 int32_t dim, const double* dcprod, int64_t ldd, const double* w,
+                                 int64_t ldw, int32_t nw, double* head, double* wing, void* stream) {
+  if (!ctx) return SPX_EINVAL;
+  if (npair < 0 || dim < 0 || nw < 0) return set_error(ctx, SPX_EINVAL, "negative size");
+  if (npair == 0 || nw == 0) return SPX_OK;
+  if (!dcprod || !w || !head || (dim > 0 && (!cprod || !wing)))
+    return set_error(ctx, SPX_EINVAL, "null array argument");
+  if (ldd < npair || ldw < npair || (dim > 0 && ldc < npair))
+    return set_error(ctx, SPX_EINVAL, "leading dimension too small");
+  if (nw > 1024) return set_error(ctx, SPX_EINVAL, "nw > 1024");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = pick_stream(ctx, stream);
+  const int M = 3 * nw, ncol = 3 + dim;
+  // pair ranges of at most 64 chunks per pass: D (M x range) and the chunk partials
+  const int64_t range = std::min<int64_t>(npair, (int64_t)64 * HW_KC);
+  const int64_t ldD = (int64_t)align_up((size_t)range, 2);
+  const int maxchunk = (int)((range + HW_KC - 1) / HW_KC);
+  const size_t d_bytes = align_up(sizeof(double2) * (size_t)M * ldD, 256);
+  const size_t p_bytes = align_up(sizeof(double2) * (size_t)maxchunk * M * ncol, 256);
+  int rc;
+  if ((rc = ensure_workspace(ctx, d_bytes + p_bytes + 256))) return rc;
+  double2* D = reinterpret_cast<double2*>(ctx->ws);
+  double2* part = reinterpret_cast<double2*>((char*)ctx->ws + d_bytes);
+  const double2* dc = reinterpret_cast<const double2*>(dcprod);
+  const double2* cp = reinterpret_cast<const double2*>(cprod);
+  for (int64_t p0 = 0; p0 < npair; p0 += range) {
+    const int64_t len = std::min<int64_t>(range, npair - p0);
+    const int nchunk = (int)((len + HW_KC - 1) / HW_KC);
+    const int64_t tot = (int64_t)M * len;
+    hw_rows_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, (int64_t)ctx->num_sms * 16), 256, 0, s>>>(
+        dc, ldd, w, ldw, p0, len, nw, D, ldD);
+    if ((rc = check_cuda(ctx, cudaGetLastError(), "hw_rows_kernel launch"))) return rc;
+    if ((rc = check_cuda(ctx, cudaMemsetAsync(part, 0, sizeof(double2) * (size_t)nchunk * M * ncol, s),
+                         "zero partials")))
+      return rc;
+    // chunk b2 of the K4c launch: A = D[:, b2 KC ...], B rows = columns of [dcprod | cprod]
+    // (the two panels differ in leading dimension: one launch each)
+    for (int panel = 0; panel < 2; ++panel) {
+      const int pcols = panel == 0 ? 3 : dim;
+      if (pcols == 0) continue;
+      ZgParams prm{};
+      prm.A = D;
+      prm.lda = ldD;
+      prm.sA2 = HW_KC;
+      prm.B = panel == 0 ? dc + p0 : cp + p0;
+      prm.sBc = panel == 0 ? ldd : ldc;
+      prm.sB2 = HW_KC;
+      prm.ncin = pcols;
+      prm.O = part + (panel == 0 ? 0 : (int64_t)M * 3);
+      prm.sOc = M;
+      prm.sO2 = (int64_t)M * ncol;
+      prm.alpha_v = make_double2(1.0, 0.0);
+      prm.M = M;
+      prm.ncol = pcols;
+      prm.K = (int)std::min<int64_t>(HW_KC, len);
+      prm.K_last = (int)(len - (int64_t)(nchunk - 1) * HW_KC);
+      prm.nb1 = 1;
+      if ((rc = launch_zgemm(ctx, prm, nchunk, s))) return rc;
+    }
+    const int64_t tot2 = (int64_t)M * ncol;
+    hw_reduce_kernel<<<(unsigned)std::min<int64_t>((tot2 + 255) / 256, (int64_t)ctx->num_sms * 8), 256, 0, s>>>(
+        part, nchunk, nw, ncol, dim, reinterpret_cast<double2*>(head), reinterpret_cast<double2*>(wing));
+    if ((rc = check_cuda(ctx, cudaGetLastError(), "hw_reduce_kernel launch"))) return rc;
   }
   return SPX_OK;
 }

@@ -194,6 +194,20 @@ class Context:
         self._check(rc, "spx_chi0_accumulate_w_dev")
         return _stats(st) if st is not None else None
 
+    # ---- q -> 0 head and wings -------------------------------------------------------
+
+    def headwings_dev(self, cprod, dcprod, w, head, wing, npair: Optional[int] = None,
+                      stream=None) -> None:
+        """head (nw, 6) and wing (nw, dim, 3) complex, row-major == Fortran (6, nw) and
+        (3, dim, nw); cprod (dim, ldc), dcprod (3, ldd), w (nw, ldw)."""
+        dim, ldc = cprod.shape
+        ldd = dcprod.shape[1]
+        nw, ldw = w.shape
+        npair = ldd if npair is None else npair
+        rc = self.lib.spx_headwings_dev(self.handle, _ptr(cprod), ldc, npair, dim, _ptr(dcprod), ldd,
+                                        _ptr(w), ldw, nw, _ptr(head), _ptr(wing), torch_stream(stream, head))
+        self._check(rc, "spx_headwings_dev")
+
     # ---- transform to the Coulomb eigenbasis -----------------------------------------
 
     def trafo_dev(self, cprod, ctrafo, out=None, npair: Optional[int] = None, stream=None):
