@@ -169,6 +169,14 @@ module spex_gpu
       integer(c_int32_t), value :: dim, nw
     end function
 
+    ! dielectric matrix and inverse, src/correlation.f:614-636, 703-745 (device arrays)
+    integer(c_int) function spx_dielec_dev(ctx, nbas, nw, susceph, coul, invert, head, wing, stream) &
+                                           bind(c, name='spx_dielec_dev')
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: ctx, susceph, coul, head, wing, stream
+      integer(c_int32_t), value :: nbas, nw, invert
+    end function
+
     ! transform to the Coulomb eigenbasis, src/susceptibility.f:806-832 (device arrays)
     integer(c_int) function spx_trafo_dev(ctx, cprod, ldc, npair, nbas, ctrafo, ldt, dim, out, &
                                           ldo, stream) bind(c, name='spx_trafo_dev')

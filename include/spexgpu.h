@@ -254,6 +254,19 @@ int spx_trafo_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
                   int32_t nbas, const double* ctrafo, int64_t ldt, int32_t dim,
                   double* out, int64_t ldo, void* stream);
 
+/* ---- dielectric matrix and its inverse (FP64) ------------------------------
+ * Replaces src/correlation.f:614-636 and :703-745 for the imaginary frequencies: in
+ * place on the packed susceph (npack, nw),
+ *   eps_ij = delta_ij - sqrt(coul_i) chi_ij sqrt(coul_j),
+ * and with invert != 0 its inverse (Cholesky; eps must be positive definite, as it
+ * is for a negative semi-definite chi, otherwise SPX_EINVAL names the frequency).
+ * coul: Coulomb eigenvalues (nbas), device. head (6, nw) and wing (3, nbas, nw) may
+ * be NULL; if given they become 1 - 4 pi head and -sqrt(4 pi) sqrt(coul_i) wing.
+ * The factorisation uses cuSOLVER, loaded at the first inverting call. */
+int spx_dielec_dev(spx_ctx* ctx, int32_t nbas, int32_t nw, double* susceph,
+                   const double* coul, int32_t invert, double* head, double* wing,
+                   void* stream);
+
 /* ---- many q points in one launch (K7) ---------------------------------------
  * The q loop of the reference driver (src/correlation.f:293-339 calls
  * `susceptibility` once per q point) as one call: every q has its own N_MB,

@@ -293,3 +293,33 @@ def headwings(cprod, dcprod, w):
     for k2 in range(3):
         wing[k2] = (c * np.conj(d[:, k2])[:, None]).T @ w
     return head, wing
+
+
+def dielec(susceph, coul, invert=True, head=None, wing=None):
+    """The dielectric matrices of src/correlation.f:614-636 from packed chi (npack, nw):
+    suscep = -suscep; times sqrt(coul_i) sqrt(coul_j); plus 1 on the diagonal; then the
+    inverse of each (src/correlation.f:703-745, zpptrf/zpptri). Returns the packed
+    result and the transformed head (6, nw) and wing (3, nbas, nw) if given."""
+    sp = np.asarray(susceph)
+    npk, nw = sp.shape
+    n = int(round((np.sqrt(8 * npk + 1) - 1) / 2))
+    sq = np.sqrt(np.asarray(coul))
+    iu, ju = np.triu_indices(n)
+    idx = ju * (ju + 1) // 2 + iu
+    out = np.zeros_like(sp)
+    for f in range(nw):
+        full = np.zeros((n, n), complex)
+        full[iu, ju] = sp[idx, f]
+        full[ju, iu] = np.conj(sp[idx, f])
+        eps = np.eye(n) - sq[:, None] * full * sq[None, :]
+        if invert:
+            eps = np.linalg.inv(eps)
+        out[idx, f] = eps[iu, ju]
+    res = [out]
+    if head is not None:
+        h = -4 * np.pi * np.asarray(head)
+        h[[0, 2, 5]] += 1.0
+        res.append(h)
+    if wing is not None:
+        res.append(-np.sqrt(4 * np.pi) * sq[None, :, None] * np.asarray(wing))
+    return res if len(res) > 1 else out

@@ -66,7 +66,7 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
         subprocess.run(cmd, check=True)
         objs.append(str(obj))
     cmd = [nvcc, "-shared", "-cudart", "static", "-gencode", "arch=compute_100a,code=sm_100a",
-           *objs, "-o", str(LIB) + ".tmp"]
+           *objs, "-ldl", "-o", str(LIB) + ".tmp"]
     if host_cc:
         cmd[1:1] = ["-ccbin", host_cc]
     subprocess.run(cmd, check=True)

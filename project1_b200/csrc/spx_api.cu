@@ -259,9 +259,14 @@ extern "C" int spx_ctx_create(int device, const spx_options* opt, spx_ctx** out)
   return SPX_OK;
 }
 
+namespace spx {
+void dielec_release(spx_ctx* ctx);
+}
+
 extern "C" int spx_ctx_destroy(spx_ctx* ctx) {
   if (!ctx) return SPX_EINVAL;
   cudaSetDevice(ctx->device);
+  spx::dielec_release(ctx);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   if (ctx->prep_stream) cudaStreamSynchronize(ctx->prep_stream);

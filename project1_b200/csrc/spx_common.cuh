@@ -45,6 +45,7 @@ struct spx_ctx {
   };
   std::vector<BatchGraph> graphs;
   uint64_t graph_clock = 0;
+  void* dn = nullptr;  // dense-solver handle of the dielectric inversion, made on first use
 };
 
 namespace spx {

@@ -208,6 +208,18 @@ class Context:
                                         _ptr(w), ldw, nw, _ptr(head), _ptr(wing), torch_stream(stream, head))
         self._check(rc, "spx_headwings_dev")
 
+    # ---- dielectric matrix ----------------------------------------------------------
+
+    def dielec_dev(self, susceph, coul, invert: bool = True, head=None, wing=None,
+                   stream=None) -> None:
+        """In place: susceph (nw, npack) -> eps = 1 - v^1/2 chi v^1/2, inverted if asked
+        (src/correlation.f:614-636, :703-745); head (nw, 6), wing (nw, nbas, 3) optional."""
+        nw, npk = susceph.shape
+        nbas = int(round((np.sqrt(8 * npk + 1) - 1) / 2))
+        rc = self.lib.spx_dielec_dev(self.handle, nbas, nw, _ptr(susceph), _ptr(coul), int(invert),
+                                     _ptr(head), _ptr(wing), torch_stream(stream, susceph))
+        self._check(rc, "spx_dielec_dev")
+
     # ---- transform to the Coulomb eigenbasis -----------------------------------------
 
     def trafo_dev(self, cprod, ctrafo, out=None, npair: Optional[int] = None, stream=None):
