@@ -1164,6 +1164,198 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
   if (warp == 1) tmem_dealloc(tmem, SP_TMEM_COLS);
 }
 
+// The same GEMM with 32-column tiles (N = 64 real rows of B, stacked in 32-blocks)
+// and two TMEM buffers of 4 orders x 64 columns: the MMAs of item j+1 run while the
+// epilogue drains item j, which the short K of the product GEMM needs (47 stages at
+// configs[4], against 512 for K2).
+constexpr int SG_TB = 32;                        // complex B rows per tile
+constexpr int SG_ST = 4;
+constexpr int SG_BPLANE = 2 * SG_TB * SP_KB;     // 4096 bytes
+constexpr uint32_t SG_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(2 * SG_TB / 8) << 17) |
+                              ((uint32_t)(SP_ROWS / 16) << 24);
+
+struct __align__(1024) SgSmem {
+  uint8_t a[SG_ST][SP_SA][SP_PLANE];
+  uint8_t b[SG_ST][SP_SB][SG_BPLANE];
+  long long xchg[2][SP_TILE][33];
+  uint64_t full[SG_ST];
+  uint64_t empty[SG_ST];
+  uint64_t tfull[2], tempty[2];
+  uint64_t xfull, xfree, mdone;
+  uint32_t tmem_base;
+};
+
+// T = ((D0*256 + D1)*256 + D2)*256 + D3 for 32 columns, orders 64 columns apart.
+__device__ __forceinline__ void load_orders64(uint32_t taddr, long long (&T)[32]) {
+  int32_t r[32];
+  tmem_ld32(taddr, r);
+  tmem_wait_ld();
+#pragma unroll
+  for (int k = 0; k < 32; ++k) T[k] = r[k];
+#pragma unroll
+  for (int g = 1; g < 4; ++g) {
+    tmem_ld32(taddr + (uint32_t)(g * 64), r);
+    tmem_wait_ld();
+#pragma unroll
+    for (int k = 0; k < 32; ++k) T[k] = T[k] * 256 + r[k];
+  }
+}
+
+__global__ void __launch_bounds__(SP_THREADS, 1)
+    split_gemm2_kernel(const __grid_constant__ CUtensorMap mapA,
+                       const __grid_constant__ CUtensorMap mapB, SgParams prm) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  SgSmem& sm = *reinterpret_cast<SgSmem*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < SG_ST; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&sm.tfull[b], 1);
+      mbar_init(&sm.tempty[b], 4);
+    }
+    mbar_init(&sm.xfull, 4);
+    mbar_init(&sm.xfree, 4);
+    mbar_init(&sm.mdone, 1);
+    fence_barrier_init();
+  }
+  if (warp == 1) tmem_alloc(&sm.tmem_base, SP_TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sm.tmem_base;
+  const int mtiles = prm.mtiles, ntiles = prm.ntiles;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int st = 0;
+      uint32_t ph = 0;
+      bool issued[SG_ST];
+      uint32_t last_ph[SG_ST];
+      for (int s = 0; s < SG_ST; ++s) issued[s] = false, last_ph[s] = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; item < prm.nitems && ok; item += gridDim.x) {
+        const int mt = item % mtiles, r = item / mtiles, ct = r % ntiles, b = r / ntiles;
+        const int ra = (int)(b * prm.RA) + mt * SP_ROWS, rb = (int)(b * prm.RB) + ct * (2 * SG_TB);
+        for (int ks = 0; ks < prm.nk; ++ks) {
+          if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&sm.full[st], (uint32_t)(SP_SA * SP_PLANE + SP_SB * SG_BPLANE));
+          tma_load_4d(&sm.a[st][0][0], &mapA, 0, ra, ks, 0, &sm.full[st]);
+          tma_load_4d(&sm.b[st][0][0], &mapB, 0, rb, ks, 0, &sm.full[st]);
+          issued[st] = true;
+          last_ph[st] = ph;
+          if (++st == SG_ST) st = 0, ph ^= 1u;
+        }
+      }
+      for (int s = 0; s < SG_ST; ++s)
+        if (issued[s]) mbar_drain(&sm.full[s], last_ph[s], prm.timeout_ns);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int st = 0;
+      uint32_t ph = 0;
+      int j = 0;
+      bool committed = false;
+      for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j) {
+        const int buf = j & 1;
+        // this buffer's previous item (j - 2) has been drained (first use: immediately)
+        if (!mbar_wait(&sm.tempty[buf], (uint32_t)((j >> 1) & 1) ^ 1u, prm.timeout_ns, prm.status)) break;
+        tc_fence_after();
+        const uint32_t tb = tmem + (uint32_t)(buf * 256);
+        bool ok = true;
+        for (int ks = 0; ks < prm.nk; ++ks) {
+          if (!mbar_wait(&sm.full[st], ph, prm.timeout_ns, prm.status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll
+          for (int kk = 0; kk < SP_NKS; ++kk) {
+            uint64_t da[SP_SA], db[SP_SB];
+#pragma unroll
+            for (int t = 0; t < SP_SA; ++t) da[t] = desc_sw64(&sm.a[st][t][0]) + (uint64_t)(kk * 2);
+#pragma unroll
+            for (int u = 0; u < SP_SB; ++u) db[u] = desc_sw64(&sm.b[st][u][0]) + (uint64_t)(kk * 2);
+            const uint32_t k0 = (ks > 0 || kk > 0);
+            mma_i8<1>(tb + 0 * 64, da[0], db[0], SG_IDESC, k0);
+            mma_i8<2>(tb + 1 * 64, da[0], db[1], SG_IDESC, k0);
+            mma_i8<2>(tb + 2 * 64, da[0], db[2], SG_IDESC, k0);
+            mma_i8<3>(tb + 3 * 64, da[0], db[3], SG_IDESC, k0);
+            mma_i8<1>(tb + 1 * 64, da[1], db[0], SG_IDESC, 1u);
+            mma_i8<2>(tb + 2 * 64, da[1], db[1], SG_IDESC, 1u);
+            mma_i8<3>(tb + 3 * 64, da[1], db[2], SG_IDESC, 1u);
+            mma_i8<1>(tb + 2 * 64, da[2], db[0], SG_IDESC, 1u);
+            mma_i8<3>(tb + 3 * 64, da[2], db[1], SG_IDESC, 1u);
+          }
+          tc_commit(&sm.empty[st]);
+          committed = true;
+          if (++st == SG_ST) st = 0, ph ^= 1u;
+        }
+        if (!ok) break;
+        tc_commit(&sm.tfull[buf]);
+      }
+      if (committed) {
+        tc_commit(&sm.mdone);
+        mbar_drain(&sm.mdone, 0u, prm.timeout_ns);
+      }
+    }
+  } else {
+    const int q = warp & 3;
+    const bool is_re = q < 2;
+    const int ii = (q & 1) * 32 + lane;
+    const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16);
+    int j = 0;
+    uint32_t xseq = 0;
+    for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j, ++xseq) {
+      const int buf = j & 1;
+      if (!mbar_wait_idle(&sm.tfull[buf], (uint32_t)((j >> 1) & 1), prm.timeout_ns, prm.status)) break;
+      tc_fence_after();
+      const int mt = item % mtiles, r = item / mtiles, ct = r % ntiles, b = r / ntiles;
+      long long tre[32], tim[32];
+      load_orders64(tl + (uint32_t)(buf * 256), tre);
+      load_orders64(tl + (uint32_t)(buf * 256 + SG_TB), tim);
+      // the buffer is read: the MMAs of item j + 2 may overwrite it
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.tempty[buf]);
+      const int gm = mt * SP_TILE + ii;
+      const double fac = prm.alpha * prm.sA[(int64_t)b * mtiles * SP_TILE + gm] *
+                         (1.0 / (127.0 * 127.0 * 16777216.0));
+      const double* sbb = prm.sB + (int64_t)b * ntiles * SG_TB;
+      double* ob = prm.out + 2 * (b * prm.sO2 + gm) + (is_re ? 0 : 1);
+      if (!mbar_wait(&sm.xfree, (xseq & 1u) ^ 1u, prm.timeout_ns, prm.status)) break;
+#pragma unroll
+      for (int k = 0; k < 32; ++k) sm.xchg[is_re ? 0 : 1][ii][k] = tim[k];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.xfull);
+      if (!mbar_wait(&sm.xfull, xseq & 1u, prm.timeout_ns, prm.status)) break;
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        const int gc = ct * SG_TB + k;
+        const long long partner = sm.xchg[is_re ? 1 : 0][ii][k];
+        const long long v = is_re ? tre[k] + partner : tre[k] - partner;
+        if (gm < prm.M && gc < prm.ncol) {
+          const int n = gc / prm.ncin, c = gc - n * prm.ncin;
+          double* o = ob + 2 * (n * prm.sOn + c * prm.sOc);
+          *o += fac * sbb[gc] * (double)v;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.xfree);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc(tmem, SP_TMEM_COLS);
+}
+
 // Row sources of the two operands: A rows are contiguous in k, B rows are gathered.
 struct SgSrcRows {
   const double2* base;
@@ -1206,9 +1398,9 @@ __global__ void sgemm_rowmax_kernel(Src src, int rows, int rows_pad, int K, doub
 }
 
 // S digits of round(x * 127/s * 2^(8(S-1))) into planes [t][k-block][row][64 B] with
-// real-stacked rows b*R + 128*(r/64) + {r%64 Re, 64 + r%64 Im}. One thread = one row
+// real-stacked rows b*R + 2 TB (r/TB) + {r%TB Re, TB + r%TB Im}. One thread = one row
 // and 16 consecutive k; a warp = 8 consecutive rows x the 4 quarters of a k-block.
-template <int S, class Src>
+template <int S, int TB, class Src>
 __global__ void __launch_bounds__(128)
     sgemm_quant_kernel(Src src, int rows, int rows_pad, int K, int nkb, int nbatch, int64_t R,
                        const double* __restrict__ s, int8_t* __restrict__ planes) {
@@ -1222,10 +1414,10 @@ __global__ void __launch_bounds__(128)
   const int kb = (int)(kbb % nkb), b = (int)(kbb / nkb);
   const int k0 = kb * SP_KB + quarter * 16;
   const int64_t rows_total = (int64_t)nbatch * R;
-  const int64_t rr = (int64_t)b * R + (r / SP_TILE) * SP_ROWS + (r % SP_TILE);
+  const int64_t rr = (int64_t)b * R + (r / TB) * (2 * TB) + (r % TB);
   const int64_t pstride = (int64_t)nkb * rows_total * SP_KB;
   const int64_t o_re = ((int64_t)kb * rows_total + rr) * SP_KB + quarter * 16;
-  const int64_t o_im = o_re + (int64_t)SP_TILE * SP_KB;
+  const int64_t o_im = o_re + (int64_t)TB * SP_KB;
   const double sc = r < rows ? s[(int64_t)b * rows_pad + r] : 0.0;
   const double inv = sc > 0.0 ? 127.0 * (S == 4 ? 16777216.0 : 65536.0) / sc : 0.0;
   uint32_t wr[S][4], wi[S][4];
@@ -1254,7 +1446,8 @@ __global__ void __launch_bounds__(128)
 
 // Bytes of scratch for one launch group of `nbatch` batches (planes and scales).
 size_t sgemm_workspace_bytes(int nbatch, int M, int ncol, int K) {
-  const int64_t mt = (M + SP_TILE - 1) / SP_TILE, nt = (ncol + SP_TILE - 1) / SP_TILE;
+  const int64_t mt = (M + SP_TILE - 1) / SP_TILE, nt2 = (ncol + SG_TB - 1) / SG_TB;
+  const int64_t nt = (nt2 + 1) / 2;  // in 64-row units: B has 2 SG_TB rows per tile
   const int64_t kp = (int64_t)align_up((size_t)std::min(std::max(K, 1), SP_SLAB), SP_KB);
   return align_up((size_t)SP_SA * kp * nbatch * mt * SP_ROWS, 1024) +
          align_up((size_t)SP_SB * kp * nbatch * nt * SP_ROWS, 1024) +
@@ -1270,17 +1463,17 @@ int sgemm_products(spx_ctx* ctx, int nbatch, int M, int ncol, int K, const doubl
                    double2* out, int64_t sO2, int64_t sOn, int64_t sOc, double alpha, void* ws,
                    size_t ws_bytes, cudaStream_t s, int* launches) {
   if (nbatch <= 0 || M <= 0 || ncol <= 0 || K <= 0) return SPX_OK;
-  const int mt = (M + SP_TILE - 1) / SP_TILE, nt = (ncol + SP_TILE - 1) / SP_TILE;
-  const int64_t RA = (int64_t)mt * SP_ROWS, RB = (int64_t)nt * SP_ROWS;
+  const int mt = (M + SP_TILE - 1) / SP_TILE, nt = (ncol + SG_TB - 1) / SG_TB;
+  const int64_t RA = (int64_t)mt * SP_ROWS, RB = (int64_t)nt * 2 * SG_TB;
   if ((int64_t)nbatch * RB > 2147483647LL || (int64_t)nbatch * mt * nt > 2147483647LL)
     return set_error(ctx, SPX_EINVAL, "product GEMM too large for one launch group");
   uint8_t* base = (uint8_t*)align_up((size_t)ws, 1024);
   const size_t need = sgemm_workspace_bytes(nbatch, M, ncol, K);
   if (!ws || ws_bytes < need + 1024) return set_error(ctx, SPX_ENOMEM, "split product scratch too small");
-  const size_t smem = sizeof(SplitSmem) + 1024;
+  const size_t smem = sizeof(SgSmem) + 1024;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(split_gemm2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = true;
   }
   int rc;
@@ -1293,14 +1486,15 @@ int sgemm_products(spx_ctx* ctx, int nbatch, int M, int ncol, int K, const doubl
     int8_t* PB = (int8_t*)(base + align_up((size_t)SP_SA * kp * nbatch * RA, 1024));
     double* sA = (double*)((uint8_t*)PB + align_up((size_t)SP_SB * kp * nbatch * RB, 1024));
     double* sB = (double*)((uint8_t*)sA + align_up(sizeof(double) * nbatch * mt * SP_TILE, 256));
+    const int rows_b = nt * SG_TB;  // padded B rows (complex) per batch
     SgSrcRows sa{A + kbeg, lda, a_bstride};
     SgSrcGather sb{grid, g_bstride, g_nstride, coff, koff + kbeg, ncin};
     sgemm_rowmax_kernel<<<dim3(mt * SP_TILE, nbatch), 256, 0, s>>>(sa, M, mt * SP_TILE, Ks, sA);
-    sgemm_rowmax_kernel<<<dim3(nt * SP_TILE, nbatch), 256, 0, s>>>(sb, ncol, nt * SP_TILE, Ks, sB);
+    sgemm_rowmax_kernel<<<dim3(rows_b, nbatch), 256, 0, s>>>(sb, ncol, rows_b, Ks, sB);
     const int64_t ta = (int64_t)mt * SP_TILE / 8 * 32 * nkb * nbatch;
-    const int64_t tb = (int64_t)nt * SP_TILE / 8 * 32 * nkb * nbatch;
-    sgemm_quant_kernel<SP_SA><<<(unsigned)((ta + 127) / 128), 128, 0, s>>>(sa, M, mt * SP_TILE, Ks, nkb, nbatch, RA, sA, PA);
-    sgemm_quant_kernel<SP_SB><<<(unsigned)((tb + 127) / 128), 128, 0, s>>>(sb, ncol, nt * SP_TILE, Ks, nkb, nbatch, RB, sB, PB);
+    const int64_t tb = (int64_t)rows_b / 8 * 32 * nkb * nbatch;
+    sgemm_quant_kernel<SP_SA, SP_TILE><<<(unsigned)((ta + 127) / 128), 128, 0, s>>>(sa, M, mt * SP_TILE, Ks, nkb, nbatch, RA, sA, PA);
+    sgemm_quant_kernel<SP_SB, SG_TB><<<(unsigned)((tb + 127) / 128), 128, 0, s>>>(sb, ncol, rows_b, Ks, nkb, nbatch, RB, sB, PB);
     if ((rc = check_cuda(ctx, cudaGetLastError(), "split product operand preparation"))) return rc;
     *launches += 4;
     CUtensorMap mapA, mapB;
@@ -1311,7 +1505,7 @@ int sgemm_products(spx_ctx* ctx, int nbatch, int M, int ncol, int K, const doubl
     if ((rc = make_tmap_u8_4d(ctx, &mapA, PA, da, sta, ba, CU_TENSOR_MAP_SWIZZLE_64B))) return rc;
     const uint64_t db[4] = {SP_KB, rtb, (uint64_t)nkb, SP_SB};
     const uint64_t stb[3] = {SP_KB, rtb * SP_KB, (uint64_t)nkb * rtb * SP_KB};
-    const uint32_t bb[4] = {SP_KB, SP_ROWS, 1, SP_SB};
+    const uint32_t bb[4] = {SP_KB, 2 * SG_TB, 1, SP_SB};
     if ((rc = make_tmap_u8_4d(ctx, &mapB, PB, db, stb, bb, CU_TENSOR_MAP_SWIZZLE_64B))) return rc;
     SgParams prm;
     prm.nbatch = nbatch;
@@ -1334,8 +1528,8 @@ int sgemm_products(spx_ctx* ctx, int nbatch, int M, int ncol, int K, const doubl
     prm.status = ctx->d_status;
     prm.timeout_ns = (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
     const int grid_n = std::min(prm.nitems, ctx->num_sms);
-    split_gemm_kernel<<<grid_n, SP_THREADS, smem, s>>>(mapA, mapB, prm);
-    if ((rc = check_cuda(ctx, cudaGetLastError(), "split_gemm_kernel launch"))) return rc;
+    split_gemm2_kernel<<<grid_n, SP_THREADS, smem, s>>>(mapA, mapB, prm);
+    if ((rc = check_cuda(ctx, cudaGetLastError(), "split_gemm2_kernel launch"))) return rc;
     *launches += 1;
   }
   return SPX_OK;
