@@ -999,171 +999,6 @@ struct SgParams {
   uint64_t timeout_ns;
 };
 
-__global__ void __launch_bounds__(SP_THREADS, 1)
-    split_gemm_kernel(const __grid_constant__ CUtensorMap mapA,
-                      const __grid_constant__ CUtensorMap mapB, SgParams prm) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  SplitSmem& sm = *reinterpret_cast<SplitSmem*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < SP_ST; ++s) {
-      mbar_init(&sm.full[s], 1);
-      mbar_init(&sm.empty[s], 1);
-    }
-    mbar_init(&sm.tfull, 1);
-    mbar_init(&sm.tempty, 4);
-    mbar_init(&sm.xfull, 4);
-    mbar_init(&sm.xfree, 4);
-    mbar_init(&sm.mdone, 1);
-    fence_barrier_init();
-  }
-  if (warp == 1) tmem_alloc(&sm.tmem_base, SP_TMEM_COLS);
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = sm.tmem_base;
-  auto decode = [&](int item, int* b, int* mt, int* ct) {
-    *mt = item % prm.mtiles;
-    const int r = item / prm.mtiles;
-    *ct = r % prm.ntiles;
-    *b = r / prm.ntiles;
-  };
-
-  if (warp == 0) {
-    if (lane == 0) {
-      int st = 0;
-      uint32_t ph = 0;
-      bool issued[SP_ST];
-      uint32_t last_ph[SP_ST];
-      for (int s = 0; s < SP_ST; ++s) issued[s] = false, last_ph[s] = 0;
-      bool ok = true;
-      for (int item = blockIdx.x; item < prm.nitems && ok; item += gridDim.x) {
-        int b, mt, ct;
-        decode(item, &b, &mt, &ct);
-        const int ra = (int)(b * prm.RA) + mt * SP_ROWS, rb = (int)(b * prm.RB) + ct * SP_ROWS;
-        for (int ks = 0; ks < prm.nk; ++ks) {
-          if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) {
-            ok = false;
-            break;
-          }
-          mbar_arrive_expect_tx(&sm.full[st], (uint32_t)((SP_SA + SP_SB) * SP_PLANE));
-          tma_load_4d(&sm.a[st][0][0], &mapA, 0, ra, ks, 0, &sm.full[st]);
-          tma_load_4d(&sm.b[st][0][0], &mapB, 0, rb, ks, 0, &sm.full[st]);
-          issued[st] = true;
-          last_ph[st] = ph;
-          if (++st == SP_ST) st = 0, ph ^= 1u;
-        }
-      }
-      for (int s = 0; s < SP_ST; ++s)
-        if (issued[s]) mbar_drain(&sm.full[s], last_ph[s], prm.timeout_ns);
-    }
-  } else if (warp == 1) {
-    if (lane == 0) {
-      int st = 0;
-      uint32_t ph = 0;
-      int j = 0;
-      bool committed = false;
-      for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j) {
-        if (!mbar_wait(&sm.tempty, (uint32_t)(j & 1) ^ 1u, prm.timeout_ns, prm.status)) break;
-        tc_fence_after();
-        bool ok = true;
-        for (int ks = 0; ks < prm.nk; ++ks) {
-          if (!mbar_wait(&sm.full[st], ph, prm.timeout_ns, prm.status)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-#pragma unroll
-          for (int kk = 0; kk < SP_NKS; ++kk) {
-            uint64_t da[SP_SA], db[SP_SB];
-#pragma unroll
-            for (int t = 0; t < SP_SA; ++t) da[t] = desc_sw64(&sm.a[st][t][0]) + (uint64_t)(kk * 2);
-#pragma unroll
-            for (int u = 0; u < SP_SB; ++u) db[u] = desc_sw64(&sm.b[st][u][0]) + (uint64_t)(kk * 2);
-            const uint32_t k0 = (ks > 0 || kk > 0);
-            mma_i8<1>(tmem + 0 * 128, da[0], db[0], SP_IDESC, k0);
-            mma_i8<2>(tmem + 1 * 128, da[0], db[1], SP_IDESC, k0);
-            mma_i8<2>(tmem + 2 * 128, da[0], db[2], SP_IDESC, k0);
-            mma_i8<3>(tmem + 3 * 128, da[0], db[3], SP_IDESC, k0);
-            mma_i8<1>(tmem + 1 * 128, da[1], db[0], SP_IDESC, 1u);
-            mma_i8<2>(tmem + 2 * 128, da[1], db[1], SP_IDESC, 1u);
-            mma_i8<3>(tmem + 3 * 128, da[1], db[2], SP_IDESC, 1u);
-            mma_i8<1>(tmem + 2 * 128, da[2], db[0], SP_IDESC, 1u);
-            mma_i8<3>(tmem + 3 * 128, da[2], db[1], SP_IDESC, 1u);
-          }
-          tc_commit(&sm.empty[st]);
-          committed = true;
-          if (++st == SP_ST) st = 0, ph ^= 1u;
-        }
-        if (!ok) break;
-        tc_commit(&sm.tfull);
-      }
-      if (committed) {
-        tc_commit(&sm.mdone);
-        mbar_drain(&sm.mdone, 0u, prm.timeout_ns);
-      }
-    }
-  } else {
-    const int q = warp & 3;
-    const bool is_re = q < 2;
-    const int ii = (q & 1) * 32 + lane;
-    const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16);
-    int j = 0;
-    uint32_t xseq = 0;
-    for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j) {
-      if (!mbar_wait_idle(&sm.tfull, (uint32_t)(j & 1), prm.timeout_ns, prm.status)) break;
-      tc_fence_after();
-      int b, mt, ct;
-      decode(item, &b, &mt, &ct);
-      const int gm = mt * SP_TILE + ii;
-      const double sm_ = prm.sA[(int64_t)b * prm.mtiles * SP_TILE + gm];
-      const double fac = prm.alpha * sm_ * (1.0 / (127.0 * 127.0 * 16777216.0));
-      const double* sbb = prm.sB + (int64_t)b * prm.ntiles * SP_TILE;
-      double* ob = prm.out + 2 * (b * prm.sO2 + gm) + (is_re ? 0 : 1);
-      bool ok = true;
-      for (int js = 0; js < 2 && ok; ++js, ++xseq) {
-        long long tre[32], tim[32];
-        load_orders(tl + (uint32_t)(js * 32), tre);
-        load_orders(tl + (uint32_t)(64 + js * 32), tim);
-        if (!mbar_wait(&sm.xfree, (xseq & 1u) ^ 1u, prm.timeout_ns, prm.status)) {
-          ok = false;
-          break;
-        }
-#pragma unroll
-        for (int k = 0; k < 32; ++k) sm.xchg[is_re ? 0 : 1][ii][k] = tim[k];
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.xfull);
-        if (!mbar_wait(&sm.xfull, xseq & 1u, prm.timeout_ns, prm.status)) {
-          ok = false;
-          break;
-        }
-#pragma unroll
-        for (int k = 0; k < 32; ++k) {
-          const int gc = ct * SP_TILE + js * 32 + k;
-          const long long partner = sm.xchg[is_re ? 1 : 0][ii][k];
-          const long long v = is_re ? tre[k] + partner : tre[k] - partner;
-          if (gm < prm.M && gc < prm.ncol) {
-            const int n = gc / prm.ncin, c = gc - n * prm.ncin;
-            double* o = ob + 2 * (n * prm.sOn + c * prm.sOc);
-            *o += fac * sbb[gc] * (double)v;
-          }
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.xfree);
-      }
-      if (!ok) break;
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&sm.tempty);
-    }
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  if (warp == 1) tmem_dealloc(tmem, SP_TMEM_COLS);
-}
-
 // The same GEMM with 32-column tiles (N = 64 real rows of B, stacked in 32-blocks)
 // and two TMEM buffers of 4 orders x 64 columns: the MMAs of item j+1 run while the
 // epilogue drains item j, which the short K of the product GEMM needs (47 stages at
@@ -1342,8 +1177,8 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
         const long long v = is_re ? tre[k] + partner : tre[k] - partner;
         if (gm < prm.M && gc < prm.ncol) {
           const int n = gc / prm.ncin, c = gc - n * prm.ncin;
-          double* o = ob + 2 * (n * prm.sOn + c * prm.sOc);
-          *o += fac * sbb[gc] * (double)v;
+          // one add per element per launch: a reduction that nothing waits on
+          atomicAdd(ob + 2 * (n * prm.sOn + c * prm.sOc), fac * sbb[gc] * (double)v);
         }
       }
       __syncwarp();
