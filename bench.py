@@ -377,7 +377,7 @@ def run_ours(args):
 
 
 def bench_batched(args, dev, stream):
-    """32 uneven q points, M generated on the device slab by slab, all q in
+    """Batched workload: 32 uneven q points, M generated on the device slab by slab, all q in
     one replayed CUDA graph per step (autotuned per (N, P) bucket in the warm-up)."""
     import torch
     import project1_b200 as spx
@@ -430,7 +430,7 @@ def bench_batched(args, dev, stream):
 
 
 def bench_products(args, dev, stream):
-    """wave-function products (MT Gaunt contraction + interstitial
+    """Products workload: wave-function products (MT Gaunt contraction + interstitial
     convolution) and split chi0 in one call, M never leaving the device."""
     import torch
     import project1_b200 as spx
@@ -562,11 +562,11 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=10.0)
     ap.add_argument("--no-check", dest="check", action="store_false")
-    ap.add_argument("--products-steps", type=int, default=3, help="configs[4] timed steps (0: skip)")
+    ap.add_argument("--products-steps", type=int, default=3, help="timed steps of the fused products workload (0: skip)")
     ap.add_argument("--products-warmup", type=int, default=3)
-    ap.add_argument("--batched-steps", type=int, default=1, help="configs[3] timed batches (0: skip)")
+    ap.add_argument("--batched-steps", type=int, default=1, help="timed batches of the batched q-point workload (0: skip)")
     ap.add_argument("--batched-warmup", type=int, default=1)
-    ap.add_argument("--c4-kpts", type=int, default=0, help="override configs[4]'s k-point count (profiling)")
+    ap.add_argument("--c4-kpts", type=int, default=0, help="override the products workload's k-point count (profiling)")
     ap.add_argument("--precision", choices=["split", "fp64"], default=None,
                     help="force the measured path (profiling captures)")
     ap.add_argument("--kpts", type=int, default=0, help="override the k-point count (profiling)")

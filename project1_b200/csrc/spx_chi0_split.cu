@@ -1002,7 +1002,7 @@ struct SgParams {
 // The same GEMM with 32-column tiles (N = 64 real rows of B, stacked in 32-blocks)
 // and two TMEM buffers of 4 orders x 64 columns: the MMAs of item j+1 run while the
 // epilogue drains item j, which the short K of the product GEMM needs (47 stages at
-// configs[4], against 512 for K2).
+// 3000 plane waves, against 512 for K2).
 constexpr int SG_TB = 32;                        // complex B rows per tile
 constexpr int SG_ST = 4;
 constexpr int SG_BPLANE = 2 * SG_TB * SP_KB;     // 4096 bytes

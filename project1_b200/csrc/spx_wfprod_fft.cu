@@ -9,7 +9,7 @@
 // Here only what the gather needs is computed:
 //   * band grids (K5a, `dft_pass_kernel` x3): the coefficients live in a small
 //     G box, so each of the three separable passes sums only over the box
-//     extent of its axis (19 of 48 for configs[4]); the last pass applies
+//     extent of its axis (19 of 48 for a 3000-wave sphere on a 48^3 grid); the last pass applies
 //     conj, 1/sqrt(vol), theta or 1/nnfft;
 //   * pair z and y passes (K5b, `fft_pair_zy_kernel`): one CTA per (occupied
 //     band, x plane, group of unoccupied bands) forms the product line by line

@@ -100,7 +100,7 @@ def small(name: str, nbas: int, nk: int, nocc: int, nunocc: int, nw: int,
 
 
 # ---------------------------------------------------------------------------
-# wave-function products: 2 atoms, lmax 8, 3 radial functions per l,
+# wave-function products workload: 2 atoms, lmax 8, 3 radial functions per l,
 # seeded sparse Gaunt table (5 % of the valid entries), seeded radial integrals;
 # 3000 plane waves per k damped by exp(-|G|^2/50); 1014 mixed-basis plane waves.
 
@@ -219,7 +219,7 @@ def pw_coeffs(w: WfprodWorkload, pw: dict):
 
 
 # ---------------------------------------------------------------------------
-# batched uneven q points: 32 q with N_MB ~ U{600..1800}, band windows
+# batched uneven q-point workload: 32 q with N_MB ~ U{600..1800}, band windows
 # occ ~ U{20..60} x unocc ~ U{150..500}, 64 k points, 24 frequencies, M generated
 # per q from its own Philox stream.
 

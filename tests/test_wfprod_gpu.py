@@ -54,7 +54,7 @@ def test_mt_matches_oracle(ctx, kw):
 
 
 def test_mt_full_product_basis_few_bands(ctx):
-    """The configs' MT basis (lmax 8, 3 radial functions, 243 x 243 per atom, 5 % Gaunt)."""
+    """The products workload's MT basis (lmax 8, 3 radial functions, 243 x 243 per atom, 5 % Gaunt)."""
     w = inputs.WfprodWorkload("c4sub", nk=1, nocc=3, nunocc=20)
     mt = inputs.mt_basis(w)
     c1, c2 = inputs.mt_coeffs(w)
@@ -81,7 +81,7 @@ def test_pw_matches_oracle(ctx, kw, shifted):
 
 
 def test_pw_full_basis_against_fft_branch(ctx):
-    """The configs' interstitial basis (3000 PW, 1014 MPB PW, 48^3 grid): checked against
+    """The products workload's interstitial basis (3000 PW, 1014 MPB PW, 48^3 grid): checked against
     the numpy restatement of the reference's FFT branch on a few band pairs."""
     w = inputs.WfprodWorkload("c4sub", nk=1, nocc=2, nunocc=3)
     pw = inputs.pw_basis(w)
@@ -222,7 +222,7 @@ def test_pw_fft_branch_aliasing_grid_follows_reference(ctx):
 
 
 def test_pw_fft_branch_full_basis(ctx):
-    """The configs' interstitial basis on the 48^3 grid, a few band pairs."""
+    """The products workload's interstitial basis on the 48^3 grid, a few band pairs."""
     w = inputs.WfprodWorkload("c4sub", nk=1, nocc=2, nunocc=3)
     pw = inputs.pw_basis(w)
     c1, c2 = inputs.pw_coeffs(w, pw)
@@ -286,7 +286,7 @@ def test_pw_split_products_match_oracle(ctx_split, kw, shifted):
 
 
 def test_pw_split_products_full_basis(ctx, ctx_split):
-    """The configs' interstitial basis (3000 PW, 1014 MPB PW) against the FP64 GEMM,
+    """The products workload's interstitial basis (3000 PW, 1014 MPB PW) against the FP64 GEMM,
     with a padded leading dimension and a column offset."""
     w = inputs.WfprodWorkload("c4sub", nk=2, nocc=3, nunocc=70)
     pw = inputs.pw_basis(w)
