@@ -329,6 +329,13 @@ int spx_tune_lookup(const spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
 int spx_tune_save(const spx_ctx* ctx, const char* path);
 int spx_tune_load(spx_ctx* ctx, const char* path);
 
+/* ---- diagnostics ------------------------------------------------------------
+ * Runs one kernel that waits, with the library's bounded device wait, on a barrier
+ * phase that nothing completes. It returns SPX_ETIMEOUT after about timeout_ms
+ * (1..10000) and leaves the context usable: the failure path every kernel of the
+ * library takes when a wait runs out. No counterpart in the reference. */
+int spx_selftest_wait_dev(spx_ctx* ctx, int32_t timeout_ms);
+
 /* ---- seeded synthetic inputs (K8) -------------------------------------------
  * Philox4x32-10 (Salmon et al., SC'11) with a Box-Muller transform written from
  * basic IEEE operations only, so host and device produce identical bits.

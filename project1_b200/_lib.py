@@ -128,6 +128,7 @@ SIGNATURES = {
     "spx_headwings_dev": (
         C.c_int, [_P, _P, _I64, _I64, _I32, _P, _I64, _P, _I64, _I32, _P, _P, _P]),
     "spx_dielec_dev": (C.c_int, [_P, _I32, _I32, _P, _P, _I32, _P, _P, _P]),
+    "spx_selftest_wait_dev": (C.c_int, [_P, _I32]),
     "spx_trafo_dev": (C.c_int, [_P, _P, _I64, _I64, _I32, _P, _I64, _I32, _P, _I64, _P]),
     "spx_chi0_batched": (
         C.c_int, [_P, _I32, C.POINTER(spx_q_desc), _I32, _P, _I32, _I32, _P, C.POINTER(spx_chi0_stats)]),

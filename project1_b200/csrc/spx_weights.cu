@@ -188,4 +188,28 @@ int launch_hilbert_weights(spx_ctx* ctx, int64_t P, int S, int nw, const double*
   return check_cuda(ctx, cudaGetLastError(), "hilbert_weights_kernel launch");
 }
 
+
+// One bounded wait on an mbarrier phase that nothing completes: the failure path of
+// every device-side wait in this library (status word set, kernel returns).
+__global__ void wait_selftest_kernel(int* status, uint64_t timeout_ns) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  mbar_wait(&bar, 0u, timeout_ns, status);  // no thread ever arrives
+  __syncthreads();
+}
+
 }  // namespace spx
+
+extern "C" int spx_selftest_wait_dev(spx_ctx* ctx, int32_t timeout_ms) {
+  if (!ctx) return SPX_EINVAL;
+  if (timeout_ms <= 0 || timeout_ms > 10000) return spx::set_error(ctx, SPX_EINVAL, "timeout_ms must be 1..10000");
+  cudaSetDevice(ctx->device);
+  spx::wait_selftest_kernel<<<1, 32, 0, ctx->stream>>>(ctx->d_status, (uint64_t)timeout_ms * 1000000ull);
+  int rc = spx::check_cuda(ctx, cudaGetLastError(), "wait_selftest_kernel launch");
+  if (rc) return rc;
+  return spx::collect_status(ctx, ctx->stream, "selftest_wait");
+}

@@ -156,3 +156,24 @@ def test_bad_arguments_raise(ctx):
         ctx.chi0_accumulate_dev(to_dev_cprod(m), torch.from_numpy(d).to(DEV), torch.from_numpy(om).to(DEV),
                                 out, npair=11)
     assert e.value.status == SPX_EINVAL
+
+
+def test_bounded_wait_reports_timeout_and_context_survives():
+    """A device wait on a barrier phase that nothing completes runs out after its limit,
+    is reported as SPX_ETIMEOUT with a message, and the context keeps working."""
+    import time
+    from project1_b200 import _lib
+    with spx.Context(0) as c:
+        t0 = time.perf_counter()
+        rc = c.lib.spx_selftest_wait_dev(c.handle, 200)
+        dt = time.perf_counter() - t0
+        assert rc == _lib.SPX_ETIMEOUT
+        assert "time limit" in c.lib.spx_last_error(c.handle).decode()
+        assert 0.15 < dt < 5.0
+        # the status word was cleared: ordinary work runs and is correct
+        m, d, om = random_case(40, 200, 2, seed=1)
+        ref = oracle.chi0(m, oracle.weights(d, om))
+        out = np.zeros((40 * 41 // 2, 2), complex, order="F")
+        c.chi0_accumulate(m, d, om, out)
+        emax, _ = normalized_error(out, ref, 40)
+        assert emax <= FP64_TOL
