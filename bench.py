@@ -274,6 +274,8 @@ def run_ours(args):
     if args.precision:
         head = args.precision
 
+    # the autotuner picks the accumulation kernel and slab for this shape (untimed)
+    tuned = ctx.autotune_split(N, Pr, nw) if head == "split" and args.autotune else None
     sampler = ClockSampler(local) if rank == 0 else None
     ms, gram_ms, launches, clocks = timed(head, args.warmup, args.steps, sampler)
     value = w.flops / (ms * 1e-3) / 1e12   # whole job: all ranks' pairs / max-over-ranks time
@@ -292,6 +294,12 @@ def run_ours(args):
         out_h = np.zeros((npk, nw), dtype=np.complex128, order="F")
         eh = ediff_h[p_lo:p_hi].copy()
         ctx2 = spx.Context(local)
+        if tuned is not None:
+            # the tuning table travels as its JSON file
+            import tempfile
+            with tempfile.TemporaryDirectory() as td:
+                ctx.tune_save(os.path.join(td, "tune.json"))
+                ctx2.tune_load(os.path.join(td, "tune.json"))
         h2d = d2h = 0
         for it in range(1 + args.e2e_steps):
             if it == 1:
@@ -351,6 +359,7 @@ def run_ours(args):
             "data": "synthetic (seeded Philox4x32-10 normals, uniform energies, Gauss-Legendre frequencies)",
             "config": {"workload": workload_name(w), "nbas": N, "npair": P, "nw": nw,
                        "headline_precision": head, "parallelism": f"pairs sharded over {world} GPU(s)",
+                       "autotuned": None if tuned is None else {k: tuned[k] for k in ("variant", "slab_pairs", "tflops")},
                        "l2": "inputs larger than L2 (M = %.1f GB)" % (16 * N * P / 1e9)},
             "fp64": fp64, "e2e": e2e, "roofline": roof, "clocks": clocks,
             "gpu_launches": launches, "kernel_ms_per_step": kernel_ms,
@@ -562,6 +571,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=10.0)
     ap.add_argument("--no-check", dest="check", action="store_false")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default accumulation kernel instead of the tuned one")
     ap.add_argument("--products-steps", type=int, default=3, help="timed steps of the fused products workload (0: skip)")
     ap.add_argument("--products-warmup", type=int, default=3)
     ap.add_argument("--batched-steps", type=int, default=1, help="timed batches of the batched q-point workload (0: skip)")

@@ -182,9 +182,17 @@ static int chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int
     rc = launch_chi0_fp64(ctx, M, ldc, P, N, W, ldw, nw, out, s, 8);
     ++*launches;
   } else {
+    // kernel variant and slab from the context's tuning table when the caller left
+    // the variant open and the table has this shape (smaller slabs need less scratch)
+    int variant = 0, slab = 0;
+    spx_tune_entry te;
+    if (ctx->opt.split_variant == 0 && spx_tune_lookup(ctx, N, P, nw, &te) == SPX_OK) {
+      variant = te.variant;
+      slab = te.slab_pairs;
+    }
     // the split path marks its own preparation / accumulation phases
     rc = split_chi0_slab(ctx, M, ldc, P, N, W, ldw, nw, out, split_ws, split_ws_bytes, s,
-                         launches, 0, 0);
+                         launches, variant, slab);
   }
   timing_mark(ctx, s, 2);
   return rc;
