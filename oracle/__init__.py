@@ -42,8 +42,12 @@ def load() -> C.CDLL:
         lib.oracle_chi0_element.argtypes = [I64, P, P, P, I32, P]
         lib.oracle_scale.argtypes = [P, I64, D]
         lib.oracle_max_threads.restype = C.c_int
+        lib.oracle_gen_cmatrix.argtypes = [C.c_uint64, C.c_uint32, I64, I64, I64, I64, D, P, C.c_int]
+        lib.oracle_series_log.argtypes = [I64, P, P]
+        lib.oracle_series_sincos_turns.argtypes = [I64, P, P, P]
         for name in ("oracle_weights", "oracle_chi0_faithful", "oracle_chi0_accurate",
-                     "oracle_chi0_element", "oracle_scale"):
+                     "oracle_chi0_element", "oracle_scale", "oracle_gen_cmatrix",
+                     "oracle_series_log", "oracle_series_sincos_turns"):
             getattr(lib, name).restype = None
         _lib = lib
     return _lib
@@ -51,6 +55,30 @@ def load() -> C.CDLL:
 
 def _p(a: np.ndarray):
     return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def gen_cmatrix(seed: int, stream_id: int, rows: int, cols: int, col0: int = 0,
+                scale: float = 1.0, threads: int = 0) -> np.ndarray:
+    """Columns [col0, col0+cols) of the seeded (rows x ...) complex stream matrix, as a
+    Fortran (rows, cols) complex128 array: the projections the GPU library generates,
+    bit for bit, without loading the library (inputs_oracle.c)."""
+    out = np.empty((rows, cols), dtype=np.complex128, order="F")
+    load().oracle_gen_cmatrix(seed, stream_id, rows, cols, rows, col0, scale, _p(out), threads)
+    return out
+
+
+def series_log(x) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    load().oracle_series_log(x.size, _p(x), _p(y))
+    return y
+
+
+def series_sincos_turns(u):
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    s, c = np.empty_like(u), np.empty_like(u)
+    load().oracle_series_sincos_turns(u.size, _p(u), _p(s), _p(c))
+    return s, c
 
 
 def weights(ediff, omega, wscale=None, scale_all: float = 1.0) -> np.ndarray:
