@@ -186,6 +186,31 @@ module spex_gpu
       integer(c_int32_t), value :: nbas, dim
     end function
 
+    ! device-pointer form of spx_chi0_accumulate (device arrays, caller stream)
+    integer(c_int) function spx_chi0_accumulate_dev(ctx, cprod, ldc, npair, nbas, ediff, wscale, &
+        scale_all, nw, omega, precision, susceph, stream, stats) &
+        bind(c, name='spx_chi0_accumulate_dev')
+      import :: c_int, c_int32_t, c_int64_t, c_ptr, c_double, spx_chi0_stats
+      type(c_ptr), value :: ctx, cprod, ediff, wscale, omega, susceph, stream
+      integer(c_int64_t), value :: ldc, npair
+      integer(c_int32_t), value :: nbas, nw, precision
+      real(c_double), value :: scale_all
+      type(spx_chi0_stats), intent(out) :: stats
+    end function
+
+    ! allocation-free FP64 accumulation (no counterpart in the reference): for hosts
+    ! whose device heap belongs to their offload runtime; no context, static scratch,
+    ! nw <= 262144, nbas <= 46340, never inside a stream capture
+    integer(c_int) function spx_chi0_accumulate_dev_noalloc(cprod, ldc, npair, nbas, ediff, &
+        wscale, scale_all, nw, omega, susceph, stream) &
+        bind(c, name='spx_chi0_accumulate_dev_noalloc')
+      import :: c_int, c_int32_t, c_int64_t, c_ptr, c_double
+      type(c_ptr), value :: cprod, ediff, wscale, omega, susceph, stream
+      integer(c_int64_t), value :: ldc, npair
+      integer(c_int32_t), value :: nbas, nw
+      real(c_double), value :: scale_all
+    end function
+
     ! the q loop around susceptibility, src/correlation.f:293-339
     integer(c_int) function spx_chi0_batched(ctx, nq, q, nw, omega, precision, flags, stream, &
                                              stats) bind(c, name='spx_chi0_batched')

@@ -135,10 +135,13 @@ int spx_chi0_accumulate_dev(spx_ctx* ctx, const double* cprod, int64_t ldc,
  * memory belongs to its OpenMP/OpenACC offload runtime or to a pool allocator.
  * It takes no context and allocates nothing. Its scratch (the FP64 weights of
  * one slab of pairs) is a static 32 MiB device array that every GPU loading
- * the library keeps until exit. The first call on a device must come before any
- * stream capture. Calls that overlap on the GPU race on the shared scratch.
- * nw > 262144 is rejected with SPX_EINVAL. Device pointers, on the current
- * device; returns after `stream` has finished the work. */
+ * the library keeps until exit. Each call reads a status word back and
+ * synchronizes `stream`, so it must not be called while that stream is being
+ * captured into a graph. The scratch addresses are looked up on the first call on
+ * a device and again after the device's context has been replaced (e.g. by
+ * cudaDeviceReset). Calls that overlap on the GPU race on the shared scratch.
+ * nw > 262144 and nbas > 46340 are rejected with SPX_EINVAL. Device pointers, on
+ * the current device; returns after `stream` has finished the work. */
 int spx_chi0_accumulate_dev_noalloc(const double* cprod, int64_t ldc, int64_t npair,
                                     int32_t nbas, const double* ediff, const double* wscale,
                                     double scale_all, int32_t nw, const double* omega,
@@ -335,6 +338,11 @@ int spx_tune_load(spx_ctx* ctx, const char* path);
  * (1..10000) and leaves the context usable: the failure path every kernel of the
  * library takes when a wait runs out. No counterpart in the reference. */
 int spx_selftest_wait_dev(spx_ctx* ctx, int32_t timeout_ms);
+
+/* Measures the device's FP64 tensor (DMMA) peak in TFLOP/s: back-to-back
+ * m16n8k8 DMMAs on register operands, timed with CUDA events (the roofline
+ * denominator of the FP64 accumulation). No counterpart in the reference. */
+int spx_measure_dmma_peak(spx_ctx* ctx, double* tflops);
 
 /* ---- seeded synthetic inputs (K8) -------------------------------------------
  * Philox4x32-10 (Salmon et al., SC'11) with a Box-Muller transform written from

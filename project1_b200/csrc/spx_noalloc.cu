@@ -10,10 +10,15 @@
 // part of the library, and they stay there until the process exits.
 //
 // The first call on a device looks up the arrays' device addresses with
-// cudaGetSymbolAddress while that device is current. Make this first call
-// before any stream capture begins. Every call shares the same arrays, so calls
-// that overlap on the GPU (two streams, two host threads) race on them: a
+// cudaGetSymbolAddress while that device is current, and looks them up again
+// whenever the device's current context has changed since (after a
+// cudaDeviceReset or a runtime that destroys and recreates the primary context,
+// the module and its arrays are loaded anew). Every call ends by reading a status
+// word back and synchronizing its stream, so no call may be made while that
+// stream is being captured into a graph. Every call shares the same arrays, so
+// calls that overlap on the GPU (two streams, two host threads) race on them: a
 // caller must order such calls itself.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,6 +42,7 @@ namespace {
 
 struct NoallocDevice {
   bool ready = false;
+  unsigned long long ctx_id = 0;  // context the addresses below belong to
   double* weights = nullptr;  // device address of g_noalloc_weights on this device
   int* status = nullptr;      // device address of g_noalloc_status on this device
   int num_sms = 0;
@@ -46,10 +52,42 @@ constexpr int kMaxDevices = 64;
 NoallocDevice g_dev[kMaxDevices];
 std::mutex g_mu;
 
-// Once per device, with that device current: resolve the static arrays.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+// Unique id of the calling thread's current context (0 if it cannot be read).
+unsigned long long current_ctx_id() {
+  static CtxGetCurrentFn get_cur = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_cur = (CtxGetCurrentFn)p;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (CtxGetIdFn)p;
+    looked = true;
+  }
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_cur && get_id && get_cur(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS)
+    return id;
+  return 0;
+}
+
+// With the device current: resolve the static arrays for its current context
+// (once, and again after that context has been replaced).
 int noalloc_setup(int dev, NoallocDevice** out) {
   std::lock_guard<std::mutex> lock(g_mu);
   NoallocDevice& d = g_dev[dev];
+  // No current context yet (first use, or just after a device reset) reads as 0:
+  // the symbol lookup below makes the runtime bind the device's primary context,
+  // and the id is read again after it.
+  const unsigned long long before = current_ctx_id();
+  if (d.ready && (before == 0 || before != d.ctx_id)) d.ready = false;
   if (!d.ready) {
     if (cudaGetSymbolAddress((void**)&d.weights, g_noalloc_weights) != cudaSuccess ||
         cudaGetSymbolAddress((void**)&d.status, g_noalloc_status) != cudaSuccess) {
@@ -60,7 +98,8 @@ int noalloc_setup(int dev, NoallocDevice** out) {
       cudaGetLastError();
       return SPX_ECUDA;
     }
-    d.ready = true;
+    d.ctx_id = current_ctx_id();
+    d.ready = d.ctx_id != 0;
   }
   *out = &d;
   return SPX_OK;
@@ -72,7 +111,8 @@ int noalloc_setup(int dev, NoallocDevice** out) {
 // to the calling thread, with every array a device pointer and no allocation.
 // The weights of one slab of band pairs must fit the static scratch:
 // 16 * nw * 8 bytes <= SPX_NOALLOC_SCRATCH_BYTES, i.e. nw <= 262144; larger nw is
-// rejected with SPX_EINVAL. Returns after the work on `stream` has completed.
+// rejected with SPX_EINVAL, and so is nbas > 46340 (the packed index of the last
+// element must fit 31 bits). Returns after the work on `stream` has completed.
 extern "C" int spx_chi0_accumulate_dev_noalloc(const double* cprod, int64_t ldc, int64_t npair,
                                                int32_t nbas, const double* ediff,
                                                const double* wscale, double scale_all,

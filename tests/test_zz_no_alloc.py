@@ -55,6 +55,29 @@ def test_noalloc_matches_fp64_entry_point_twice(nbas, npair, nw):
         assert emax <= FP64_TOL and fro <= 1e-12, (call, emax, fro)
 
 
+def test_noalloc_several_slabs_with_pair_scales():
+    """nw = 512 leaves room for 8192 pairs of weights in the scratch, so 9001 pairs
+    run as two slabs (8192 + 809): each slab reuses the scratch, offsets cprod, ediff
+    and wscale, and adds into the output."""
+    lib = _lib.load()
+    nbas, npair, nw = 40, 9001, 512
+    m, d, om = _case(nbas, npair, nw, seed=17)
+    ws = torch.from_numpy(np.random.default_rng(2).uniform(0.5, 1.5, npair)).to(DEV)
+    npk = spx.npack(nbas)
+    ref = torch.zeros((nw, npk), dtype=torch.complex128, device=DEV)
+    with spx.Context(0) as ctx:
+        ctx.chi0_accumulate_dev(m, d, om, ref, wscale=ws, scale_all=0.25, precision="fp64")
+        torch.cuda.synchronize()
+    stream = torch.cuda.current_stream().cuda_stream
+    for call in range(2):
+        out = torch.zeros((nw, npk), dtype=torch.complex128, device=DEV)
+        rc = lib.spx_chi0_accumulate_dev_noalloc(_p(m), npair, npair, nbas, _p(d), _p(ws), 0.25, nw,
+                                                 _p(om), _p(out), C.c_void_p(stream))
+        assert rc == 0, (call, _lib.strerror(rc))
+        emax, fro = normalized_error(out.cpu().numpy().T, ref.cpu().numpy().T, nbas)
+        assert emax <= FP64_TOL and fro <= 1e-12, (call, emax, fro)
+
+
 def test_noalloc_rejects_frequency_count_beyond_scratch():
     lib = _lib.load()
     m, d, om = _case(4, 16, 1, seed=1)
