@@ -15,7 +15,9 @@ packed Hermitian output, output zeroed first (as `susceptibility` does).
                susceph copied back every step
   roofline     dominant kernel (the band-pair accumulation): achieved vs measured peak
   cpu_baseline the oracle port of the reference loop on the host cores, bounded sample
-  --impl reference  times the reference CPU loop (oracle port) alone.
+  --impl reference  times the reference CPU loop (oracle port) alone, on a fixed sample
+               of the same workload per step; it imports neither the product package
+               nor its library (inputs from oracle/ and numpy).
 
 Multi-GPU: the pair axis is sharded (the reference's Mblocks split over
 (k, occ, unocc)); each rank accumulates its share and the packed output is
@@ -109,67 +111,113 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def inputs_module():
+    """project1_b200/inputs.py loaded on its own (numpy only): the CPU arms take the
+    workload shapes and energies from it without importing the product package."""
+    import importlib.util
+    name = "spx_workload_inputs"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, ROOT / "project1_b200" / "inputs.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+class CpuSample:
+    """The oracle's faithful reference loop (src/susceptibility.f:1182-1240, per-(i,j)
+    ddot per frequency) over a fixed sample of the workload: every element i <= j < J
+    of the first J columns, all frequencies, all pairs. J is sized so that one run
+    takes about `budget_s` on `threads` host threads. M comes from the oracle's own
+    generator (the same bits as the GPU library's), energies from numpy."""
+
+    def __init__(self, w, budget_s: float, threads: int = 0):
+        import oracle
+        inp = inputs_module()
+        self.w = w
+        self.threads = threads or os.cpu_count() or 1
+        d = inp.pair_ediff(w)
+        om = inp.frequencies(w.nw)
+        self.wt = oracle.weights(d, om, None, 1.0 / w.nk)
+        probe = oracle.gen_cmatrix(w.seed, w.stream_id, w.npair, 2, 0, w.m_scale, self.threads)
+        t0 = time.perf_counter()
+        oracle.chi0(probe, self.wt, threads=min(self.threads, 3))
+        per_elem = (time.perf_counter() - t0) / 3 * min(self.threads, 3)   # thread-seconds
+        target = budget_s * self.threads / per_elem
+        self.ncol = int(max(2, min(w.nbas, (np.sqrt(8 * target + 1) - 1) / 2)))
+        self.m = oracle.gen_cmatrix(w.seed, w.stream_id, w.npair, self.ncol, 0, w.m_scale,
+                                    self.threads)
+        self.nel = self.ncol * (self.ncol + 1) // 2
+        self.full = w.nbas * (w.nbas + 1) / 2
+
+    def run(self) -> float:
+        import oracle
+        t0 = time.perf_counter()
+        oracle.chi0(self.m, self.wt, threads=self.threads)
+        return time.perf_counter() - t0
+
+    def tflops(self, dt: float) -> float:
+        """The headline metric on the sample: the workload's algorithmic flops per
+        element (8 N^2 P Nw over the N(N+1)/2 computed elements) times the sample's
+        elements, per second."""
+        return self.w.flops * (self.nel / self.full) / dt / 1e12
+
+    def describe(self, dt: float) -> str:
+        return (f"faithful per-(i,j) ddot loop (src/susceptibility.f:1182-1240) over the {self.nel} "
+                f"elements i<=j<{self.ncol} of all {self.w.nw} frequencies and all {self.w.npair} "
+                f"pairs ({self.nel / self.full:.2%} of the {self.full:.0f} elements), {dt:.1f} s per run "
+                f"on {self.threads} threads; inputs from the oracle's generator")
+
+
 def cpu_baseline(w, budget_s: float = 15.0, threads: int = 0):
-    """Faithful reference loop (oracle port) on a bounded sample: all (i<=j) elements of
-    the first J columns, timed, then scaled to the full element count."""
-    import oracle
-    from project1_b200 import inputs
-    threads = threads or os.cpu_count() or 1
-    d = inputs.pair_ediff(w)
-    om = inputs.frequencies(w.nw)
-    wt = oracle.weights(d, om, None, 1.0 / w.nk)
-    # probe with 2 columns (3 elements), then size the sample to the budget
-    ncol = 2
-    m = inputs.cprod_host(w, 0, ncol)
-    t0 = time.perf_counter()
-    oracle.chi0(m, wt, threads=min(threads, 3))
-    per_elem = (time.perf_counter() - t0) / 3 * min(threads, 3)   # thread-seconds per element
-    target = budget_s * threads / per_elem
-    ncol = int(max(2, min(w.nbas, (np.sqrt(8 * target + 1) - 1) / 2)))
-    m = inputs.cprod_host(w, 0, ncol)
-    nel = ncol * (ncol + 1) // 2
-    t0 = time.perf_counter()
-    oracle.chi0(m, wt, threads=threads)
-    dt = time.perf_counter() - t0
-    full_elems = w.nbas * (w.nbas + 1) / 2
-    t_full = dt * full_elems / nel
-    return {"value": w.flops / t_full / 1e12, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"faithful per-(i,j) ddot loop (src/susceptibility.f:1182-1240) over the "
-                      f"{nel} elements i<=j<{ncol} of all {w.nw} frequencies and all {w.npair} pairs, "
-                      f"{dt:.1f} s, scaled by the element count to {full_elems:.0f} elements",
-            "seconds_sample": dt, "seconds_full_estimate": t_full}
+    """One timed run of the faithful loop on a sample sized to `budget_s`."""
+    smp = CpuSample(w, budget_s, threads)
+    dt = smp.run()
+    return {"value": smp.tflops(dt), "unit": UNIT, "cores": smp.threads, "kind": "port",
+            "sample": smp.describe(dt), "seconds_sample": dt,
+            "seconds_full_estimate": dt * smp.full / smp.nel}
 
 
 def run_reference(args):
-    from project1_b200 import inputs
+    """--impl reference: the oracle port of the reference's CPU loop on all host threads,
+    each step one run over the same fixed sample of the workload. Rank 0 alone runs."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    w = workload_from_args(args)
-    vals = []
+    inp = inputs_module()
+    w = workload_from_args(args, inp)
+    smp = CpuSample(w, args.ref_budget)
     for _ in range(args.warmup):
-        cpu_baseline(w, budget_s=args.ref_budget)
-    for _ in range(args.steps):
-        vals.append(cpu_baseline(w, budget_s=args.ref_budget))
-    v = statistics.median([x["value"] for x in vals])
-    cb = dict(vals[-1])
-    cb["value"] = v
+        smp.run()
+    times = [smp.run() for _ in range(args.steps)]
+    rates = [smp.tflops(t) for t in times]
+    v = statistics.median(rates)
+    ms = 1e3 * statistics.mean(times)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * w.flops / (v * 1e12), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(w), "nbas": w.nbas, "npair": w.npair, "nw": w.nw},
-        "cpu_baseline": cb,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Philox4x32-10 normals from the oracle's generator, uniform energies, "
+                "Gauss-Legendre frequencies)",
+        "config": bench_config(w, args.gpus),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": smp.threads, "kind": "port",
+                         "sample": smp.describe(statistics.median(times))},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "step_definition": "one run of the reference loop over the fixed element sample; value is "
+                           "its rate in the workload's algorithmic flops",
+        "sample_fraction": smp.nel / smp.full,
+        "full_workload_s_estimate": statistics.median(times) * smp.full / smp.nel,
+        "rates_min_max": [min(rates), max(rates)],
     }))
 
 
-def workload_from_args(args):
+def workload_from_args(args, inp=None):
     """The named workload, optionally shrunk (--kpts / --freqs) for profiling captures."""
     import dataclasses
-    from project1_b200 import inputs
-    w = inputs.CONFIGS[args.workload]
+    if inp is None:
+        from project1_b200 import inputs as inp
+    w = inp.CONFIGS[args.workload]
     if args.kpts or args.freqs:
         w = dataclasses.replace(w, name=w.name + "-small", nk=args.kpts or w.nk, nw=args.freqs or w.nw)
     return w
@@ -179,6 +227,42 @@ def workload_name(w):
     return (f"{w.name}: chi0 N_MB={w.nbas}, {w.nk} k x {w.nocc} occ x {w.nunocc} unocc "
             f"(P={w.npair}), {w.nw} imaginary frequencies"
             + (f", {w.degenerate_frac:.0%} degenerate pairs" if w.degenerate_frac else ""))
+
+
+def bench_config(w, world: int) -> dict:
+    """The `config` of both arms' lines (identical for the same workload and N)."""
+    return {"workload": workload_name(w), "nbas": w.nbas, "npair": w.npair, "nw": w.nw,
+            "parallelism": f"pairs sharded over {world} GPU(s)",
+            "l2": "inputs larger than L2 (M = %.1f GB)" % (16 * w.nbas * w.npair / 1e9)}
+
+
+def int8_ops(N: int, P: int, nw: int, variant: int, slab: int) -> float:
+    """int8 ops the accumulation kernel issues for P pairs: 6 digit products per real MAC
+    of each 128 x 128 real-stacked MMA tile (one CTA: the upper 64-blocks; CTA pair: two
+    tiles per pair item), over the slabs padded to 64 pairs, 2 ops per MAC."""
+    nblk = (N + 63) // 64
+    tiles = nblk * (nblk + 1) // 2 if variant == 1 else 2 * sum(bj // 2 + 1 for bj in range(nblk))
+    pad = sum(((min(slab, P - s0) + 63) // 64) * 64 for s0 in range(0, P, slab))
+    return 2.0 * 6 * 128 * 128 * tiles * pad * nw
+
+
+def measured_traffic(kernel: str, nbas: int, nw: int, slab: int, npair_step: int):
+    """DRAM bytes of the dominant kernel from the committed ncu capture, scaled to one
+    launch (one slab of all frequencies) of this shape: the capture's bytes per pair,
+    frequency and 64-block tile. None when no capture of `kernel` is recorded."""
+    f = ROOT / "profiles" / "roofline_traffic.json"
+    if not f.exists():
+        return None
+    try:
+        rec = json.loads(f.read_text()).get(kernel)
+    except Exception:
+        return None
+    if not rec:
+        return None
+    nblk = (nbas + 63) // 64
+    per_launch = rec["bytes_per_pair_freq_tile"] * min(slab, npair_step) * nw * nblk * (nblk + 1) / 2
+    return {"bytes_per_launch": per_launch, "launches_per_step": -(-npair_step // slab),
+            "source": rec["source"]}
 
 
 def run_ours(args):
@@ -205,7 +289,7 @@ def run_ours(args):
     Pr = p_hi - p_lo
     N, nw = w.nbas, w.nw
     npk = spx.npack(N)
-    ctx = spx.Context(local)
+    ctx = spx.Context(local, split_variant=args.variant)
     stream = torch.cuda.current_stream(dev)
 
     # inputs resident in HBM: M (N, P) column blocks generated on device, bit-identical
@@ -336,17 +420,23 @@ def run_ours(args):
     if head == "split":
         roof = {"bound": "tensor", "achieved": ach, "peak": bf16s, "unit": UNIT, "frac": ach / bf16s,
                 "traffic": None, "peak_source": f"{src} bf16_tflops_sustained (kernel timed inside a long step)"}
-        # the same kernel seen from the int8 pipe it runs on: 9 digit products per real MAC of the
-        # real-stacked 128x128 tiles (CTA pairs cover row blocks in twos), 2 ops per MAC
-        nblk = (N + 63) // 64
-        blocks = sum(2 * (bj // 2 + 1) for bj in range(nblk))
-        pad = sum(((min(32768, P - s0) + 63) // 64) * 64 for s0 in range(0, P, 32768))
-        int8_ops = 2.0 * 9 * 128 * 128 * blocks * pad * nw * (Pr / P)
-        i8 = int8_ops / (kernel_ms * 1e-3) / 1e12
-        roof["int8_pipe"] = {"int8_ops_per_step": int8_ops, "achieved_tops": i8, "peak_tops": 2 * bf16s,
-                             "frac": i8 / (2 * bf16s),
+        # the same kernel seen from the int8 pipe it runs on, for the variant and slab that ran
+        variant = tuned["variant"] if tuned else (1 if ctx.split_variant == 1 else 2)
+        slab = tuned["slab_pairs"] if tuned else 32768
+        ops = int8_ops(N, Pr, nw, variant, slab)
+        i8 = ops / (kernel_ms * 1e-3) / 1e12
+        roof["int8_pipe"] = {"int8_ops_per_step": ops, "variant": variant, "slab_pairs": slab,
+                             "achieved_tops": i8, "peak_tops": 2 * bf16s, "frac": i8 / (2 * bf16s),
                              "peak_source": "2 x measured bf16 sustained (int8 peak is 16384 ops/cycle/SM "
                                             "in ncu, twice the bf16 pipe)"}
+        kname = "split_gram_kernel" if variant == 1 else "split_gram2_kernel"
+        tr = measured_traffic(kname, N, nw, slab, Pr)
+        if tr:
+            nblk = (N + 63) // 64
+            R = (nblk + 1) // 2 * 2 * 128
+            roof["traffic"] = tr["bytes_per_launch"]
+            roof["traffic_detail"] = dict(tr, kernel=kname, unit="bytes per launch (one slab, all frequencies)",
+                                          operand_plane_bytes_per_launch=3.0 * nw * R * min(slab, Pr))
     else:
         roof = {"bound": "tensor", "achieved": ach, "peak": None, "unit": UNIT, "frac": None, "traffic": None,
                 "peak_source": "FP64 DMMA has no measured peak on this pool"}
@@ -355,12 +445,12 @@ def run_ours(args):
         res = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int8x(3x4 digits)->int32->f64" if head == "split" else "f64",
+            "vs_baseline": None,
+            "dtype": "int8 (3-digit slices of sqrt|w| M, 6 products)->int32->f64" if head == "split" else "f64",
             "data": "synthetic (seeded Philox4x32-10 normals, uniform energies, Gauss-Legendre frequencies)",
-            "config": {"workload": workload_name(w), "nbas": N, "npair": P, "nw": nw,
-                       "headline_precision": head, "parallelism": f"pairs sharded over {world} GPU(s)",
-                       "autotuned": None if tuned is None else {k: tuned[k] for k in ("variant", "slab_pairs", "tflops")},
-                       "l2": "inputs larger than L2 (M = %.1f GB)" % (16 * N * P / 1e9)},
+            "config": bench_config(w, world),
+            "headline_precision": head,
+            "autotuned": None if tuned is None else {k: tuned[k] for k in ("variant", "slab_pairs", "tflops")},
             "fp64": fp64, "e2e": e2e, "roofline": roof, "clocks": clocks,
             "gpu_launches": launches, "kernel_ms_per_step": kernel_ms,
             "flops_per_step": w.flops, "flops_hermitian_per_step": w.flops_hermitian,
@@ -387,7 +477,8 @@ def run_ours(args):
 
 def bench_batched(args, dev, stream):
     """Batched workload: 32 uneven q points, M generated on the device slab by slab, all q in
-    one replayed CUDA graph per step (autotuned per (N, P) bucket in the warm-up)."""
+    one persistent kernel per step (tile shape and slab autotuned per (N, P) bucket in the
+    warm-up)."""
     import torch
     import project1_b200 as spx
     from project1_b200 import _lib, inputs
@@ -422,7 +513,22 @@ def bench_batched(args, dev, stream):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.batched_steps
-    tune = [ctx.tune_lookup(q["nbas"], q["npair"], bw.nw) for q in qs]
+    tune = [ctx.tune_lookup_batched(q["nbas"], q["npair"], bw.nw) for q in qs]
+    # accuracy at full size on three q (the two cheapest and the median by flops):
+    # the same batched call in FP64 against the split result of the timed batch
+    acc = None
+    if args.check:
+        order = sorted(range(len(qws)), key=lambda k: qws[k].flops)
+        pick = sorted({order[0], order[1], order[len(order) // 2]})
+        sub = [dict(qs[k], susceph=torch.zeros_like(qs[k]["susceph"])) for k in pick]
+        ctx.chi0_batched(sub, omega, precision="fp64", stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        per_q = [dict(compare_packed(qs[k]["susceph"], sq["susceph"], qws[k].nbas), q=k,
+                      nbas=qws[k].nbas, npair=qws[k].npair) for k, sq in zip(pick, sub)]
+        acc = {"split_vs_fp64_per_q": per_q,
+               "max_normalized": max(x["max_normalized"] for x in per_q),
+               "raw_rel_max": max(x["raw_rel_max"] for x in per_q)}
+        del sub
     res = {"workload": f"c3: {bw.nq} q, N_MB U{{{bw.nbas_range[0]}..{bw.nbas_range[1]}}}, "
                        f"occ U{{{bw.occ_range[0]}..{bw.occ_range[1]}}} x unocc "
                        f"U{{{bw.unocc_range[0]}..{bw.unocc_range[1]}}}, {bw.nk} k, {bw.nw} freqs, split",
@@ -431,9 +537,12 @@ def bench_batched(args, dev, stream):
            "warmup_s_incl_autotune_and_capture": warm_s, "flops_per_step": flops,
            "npair_total": sum(q.npair for q in qws), "graph_launches_per_step": 1,
            "kernels_per_step": kernels,
-           "tuned_choices": sorted({(t["nbas_bucket"], t["npair_bucket"], t["variant"], t["slab_pairs"])
+           "tuned_choices": sorted({(t["nbas_bucket"], t["npair_bucket"], "tile %dx%d, %d stages" % (
+                                        64, t["tile"] & 255, t["tile"] >> 8), t["slab_pairs"])
                                     for t in tune if t}),
-           "m_generated_on_device": True}
+           "schedule": "one persistent kernel per batch (accumulation and operand-preparation "
+                       "queues on every SM), captured in a CUDA graph",
+           "m_generated_on_device": True, "accuracy": acc}
     ctx.close()
     return res
 
@@ -479,9 +588,34 @@ def bench_products(args, dev, stream):
         chi0_from_coeffs(ctx, mt, pw, m1, m2, p1, p2, ediff, omega, out, scale_all=1.0 / w.nk,
                          precision="split", stream=sc)
     ms = timed(fused, args.products_warmup, args.products_steps)
+    out.zero_()
     st = chi0_from_coeffs(ctx, mt, pw, m1, m2, p1, p2, ediff, omega, out, scale_all=1.0 / w.nk,
                           precision="split", stream=sc, stats=True)
+    # accuracy at full size: the same call in FP64 (products and chi0) on every element,
+    # and sampled elements against the oracle from the FP64 products' columns
+    acc = None
+    if args.check:
+        out64 = torch.zeros_like(out)
+        chi0_from_coeffs(ctx, mt, pw, m1, m2, p1, p2, ediff, omega, out64, scale_all=1.0 / w.nk,
+                         precision="fp64", stream=sc)
+        torch.cuda.synchronize()
+        acc = {"split_vs_fp64": compare_packed(out, out64, w.nbas)}
     cp = torch.zeros((w.nbas, w.npair), dtype=torch.complex128, device=dev)
+    if args.check:
+        import oracle
+        ctx64 = spx.Context(dev.index or 0, products=_lib.SPX_PRODUCTS_FP64)
+        wavefproducts2_mt(ctx64, mt, m1, m2, cp, stream=sc)
+        wavefproducts2_pw(ctx64, pw, p1, p2, cp, w.nbasp, stream=sc)
+        torch.cuda.synchronize()
+        ctx64.close()
+        rng = np.random.default_rng(6)
+        cols = sorted(set(rng.integers(0, w.nbas, 16).tolist()) | {0, w.nbasp - 1, w.nbasp, w.nbas - 1})
+        colv = {c: cp[c].cpu().numpy() for c in cols}
+        wt = oracle.weights(inputs.pair_ediff(ew), inputs.frequencies(w.nw), None, 1.0 / w.nk)
+        acc.update(oracle_samples(out, out64, cols, colv, wt))
+        acc["oracle_columns_from"] = "FP64 device products (the split call's products are int8 slices)"
+        del out64
+        cp.zero_()
     mt_ms = timed(lambda: wavefproducts2_mt(ctx, mt, m1, m2, cp, stream=sc), 1, 2)
     pw_ms = timed(lambda: wavefproducts2_pw(ctx, pw, p1, p2, cp, w.nbasp, stream=sc), 1, 2)
     ctx_s = spx.Context(dev.index or 0, products=_lib.SPX_PRODUCTS_SPLIT)
@@ -502,48 +636,45 @@ def bench_products(args, dev, stream):
            "pw_ms": pw_ms, "pw_tflops_fp64": fl_pw / (pw_ms * 1e-3) / 1e12,
            "pw_split_ms": pws_ms, "pw_split_tflops_equiv": fl_pw / (pws_ms * 1e-3) / 1e12,
            "pw_fft_branch_ms": pwf_ms, "pw_fft_grid": 48,
-           "kernels_per_step": st["kernel_launches"], "m_bytes_on_device": 16 * w.nbas * w.npair}
+           "kernels_per_step": st["kernel_launches"], "m_bytes_on_device": 16 * w.nbas * w.npair,
+           "accuracy": acc}
     ctx.close()
     return res
 
 
-def accuracy_check(ctx, w, M, ediff, omega, stream, ediff_h, omega_h, nsample=24):
-    """Split vs FP64 on every element; FP64 vs the extended-precision oracle on sampled elements."""
+def compare_packed(a, b, N: int) -> dict:
+    """Errors of the packed output `a` (split) against `b` (FP64) on every element:
+    normalised |d chi_ij| / sqrt(|chi_ii chi_jj|) (the metric the <= 1e-6 claim uses:
+    every imaginary-axis weight has one sign, so |chi_ij| <= sqrt(chi_ii chi_jj)),
+    raw |d chi_ij| / |chi_ij|, and Frobenius."""
     import torch
-
-    import oracle
-    import project1_b200 as spx
-    from project1_b200 import inputs
-    N, nw = w.nbas, w.nw
-    outs = {}
-    for prec in ("split", "fp64"):
-        o = torch.zeros((nw, spx.npack(N)), dtype=torch.complex128, device=M.device)
-        ctx.chi0_accumulate_dev(M, ediff, omega, o, scale_all=1.0 / w.nk, precision=prec,
-                                stream=stream.cuda_stream)
-        outs[prec] = o
-    torch.cuda.synchronize()
-    a, b = outs["split"], outs["fp64"]
-    j = torch.arange(N, device=M.device)
-    dg = (j * (j + 1) // 2 + j)
-    d = b[:, dg].real.abs()                              # (nw, N)
-    iu = torch.triu_indices(N, N, device=M.device)
+    j = torch.arange(N, device=a.device)
+    d = b[:, j * (j + 1) // 2 + j].real.abs()                  # (nw, N)
+    iu = torch.triu_indices(N, N, device=a.device)
     idx = iu[1] * (iu[1] + 1) // 2 + iu[0]
-    err = (a[:, idx] - b[:, idx]).abs() / torch.sqrt(d[:, iu[0]] * d[:, iu[1]])
-    fro = float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
-    raw = (a[:, idx] - b[:, idx]).abs() / b[:, idx].abs().clamp_min(1e-300)
-    res = {"split_vs_fp64_max_normalized": float(err.max()), "split_vs_fp64_frobenius": fro,
-           "split_vs_fp64_raw_rel_median": float(raw.median()),
-           "split_vs_fp64_raw_rel_p99": float(torch.quantile(raw.flatten()[:: max(1, raw.numel() // 1000000)].float(), 0.99)),
-           "normalization": "|d chi_ij| / sqrt(|chi_ii chi_jj|) per frequency"}
-    # FP64 path vs oracle on sampled elements (columns regenerated on the host, same bits)
-    rng = np.random.default_rng(5)
-    wt = oracle.weights(ediff_h, omega_h, None, 1.0 / w.nk)
-    cols = sorted(set(rng.integers(0, N, nsample).tolist()) | {0, N - 1})
-    colv = {c: inputs.cprod_host(w, c, 1)[:, 0] for c in cols}
-    bh = b.cpu().numpy()
-    e64 = 0.0
-    es = 0.0
-    ah = a.cpu().numpy()
+    diff = (a[:, idx] - b[:, idx]).abs()
+    err = diff / torch.sqrt(d[:, iu[0]] * d[:, iu[1]])
+    raw = diff / b[:, idx].abs().clamp_min(1e-300)
+    sub = raw.flatten()[:: max(1, raw.numel() // 4000000)]
+    return {"max_normalized": float(err.max()),
+            "frac_normalized_above_1e-6": float((err > 1e-6).double().mean()),
+            "frobenius": float(torch.linalg.norm(a - b) / torch.linalg.norm(b)),
+            "raw_rel_max": float(raw.max()),
+            "raw_rel_median": float(raw.median()),
+            "raw_rel_p99": float(torch.quantile(sub, 0.99)),
+            "frac_raw_above_1e-6": float((raw > 1e-6).double().mean()),
+            "elements": int(err.numel()),
+            "claim_metric": "max_normalized (|d chi_ij| / sqrt(|chi_ii chi_jj|), every element and "
+                            "frequency); raw per-element relative error is unbounded where an "
+                            "off-diagonal chi_ij nearly cancels"}
+
+
+def oracle_samples(a, b, cols, colv, wt) -> dict:
+    """Sampled elements (i, j) of consecutive sampled columns against the oracle's
+    extended-precision element, normalised by its own diagonal."""
+    ah, bh = a.cpu().numpy(), b.cpu().numpy()
+    import oracle
+    e64 = es = 0.0
     for k in range(len(cols) - 1):
         i, jj = cols[k], cols[k + 1]
         ref = oracle.chi0_element(colv[i], colv[jj], wt)
@@ -553,9 +684,32 @@ def accuracy_check(ctx, w, M, ediff, omega, stream, ediff_h, omega_h, nsample=24
         p = jj * (jj + 1) // 2 + i
         e64 = max(e64, float(np.max(np.abs(bh[:, p] - ref) / sc)))
         es = max(es, float(np.max(np.abs(ah[:, p] - ref) / sc)))
-    res["fp64_vs_oracle_sampled_max_normalized"] = e64
-    res["split_vs_oracle_sampled_max_normalized"] = es
-    res["oracle_samples"] = len(cols) - 1
+    return {"fp64_vs_oracle_sampled_max_normalized": e64,
+            "split_vs_oracle_sampled_max_normalized": es, "oracle_samples": len(cols) - 1}
+
+
+def accuracy_check(ctx, w, M, ediff, omega, stream, ediff_h, omega_h, nsample=24):
+    """Split vs FP64 on every element; both vs the extended-precision oracle on sampled
+    elements (columns regenerated by the oracle's own generator, the same bits)."""
+    import torch
+
+    import oracle
+    import project1_b200 as spx
+    N, nw = w.nbas, w.nw
+    outs = {}
+    for prec in ("split", "fp64"):
+        o = torch.zeros((nw, spx.npack(N)), dtype=torch.complex128, device=M.device)
+        ctx.chi0_accumulate_dev(M, ediff, omega, o, scale_all=1.0 / w.nk, precision=prec,
+                                stream=stream.cuda_stream)
+        outs[prec] = o
+    torch.cuda.synchronize()
+    a, b = outs["split"], outs["fp64"]
+    res = {"split_vs_fp64": compare_packed(a, b, N)}
+    rng = np.random.default_rng(5)
+    wt = oracle.weights(ediff_h, omega_h, None, 1.0 / w.nk)
+    cols = sorted(set(rng.integers(0, N, nsample).tolist()) | {0, N - 1})
+    colv = {c: oracle.gen_cmatrix(w.seed, w.stream_id, w.npair, 1, c, w.m_scale)[:, 0] for c in cols}
+    res.update(oracle_samples(a, b, cols, colv, wt))
     return res
 
 
@@ -580,6 +734,8 @@ def main():
     ap.add_argument("--c4-kpts", type=int, default=0, help="override the products workload's k-point count (profiling)")
     ap.add_argument("--precision", choices=["split", "fp64"], default=None,
                     help="force the measured path (profiling captures)")
+    ap.add_argument("--variant", type=int, default=0, choices=[0, 1, 2],
+                    help="accumulation kernel: 1 one CTA per tile, 2 CTA pair, 0 the library's choice")
     ap.add_argument("--kpts", type=int, default=0, help="override the k-point count (profiling)")
     ap.add_argument("--freqs", type=int, default=0, help="override the frequency count (profiling)")
     args = ap.parse_args()

@@ -234,6 +234,22 @@ int spx_chi0_accumulate_w_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, in
                               int32_t precision, double* susceph, void* stream,
                               spx_chi0_stats* stats);
 
+/* ---- real-frequency polarisation (Hilbert path, suscepc) ----------------------
+ * Replaces the suscepc accumulation of src/susceptibility.f:1229-1235 (the
+ * full-matrix layout, ACCESS_CONTIG unset) with spectral_function's wghtSr and
+ * wghtSi terms (:1829-1838): with complex pair weights wr + i wi (the tetrahedron
+ * weights contracted with getwghtS's wghtSr / wghtSi of the real frequencies,
+ * spx_weights_hilbert_dev applied to each),
+ *   suscepc(i, j, f) += sum_p M(p, i) conj(M(p, j)) (wr(p, f) + i wi(p, f)),
+ * for all i, j: non-Hermitian. Evaluated as the two Hermitian sums S1 (weights
+ * wr) and S2 (weights wi) of spx_chi0_accumulate_w_dev (FP64 or split, weights of
+ * any sign) and suscepc(i,j) = S1 + i S2, suscepc(j,i) = conj(S1) + i conj(S2).
+ * Device arrays: wr, wi (ldw, nw); suscepc complex (ldo, nbas, nw), accumulated. */
+int spx_chi0_accumulate_c_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
+                              int32_t nbas, const double* wr, const double* wi, int64_t ldw,
+                              int32_t nw, int32_t precision, double* suscepc, int64_t ldo,
+                              void* stream, spx_chi0_stats* stats);
+
 /* ---- q -> 0 head and wings (FP64) --------------------------------------------
  * Replaces src/susceptibility.f:1092-1157 for HILBERT NONE-style weights: with the
  * momentum-matrix products dcprod(p, 1:3) (src/dwavefproducts.f),
@@ -261,11 +277,11 @@ int spx_trafo_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
  * Replaces src/correlation.f:614-636 and :703-745 for the imaginary frequencies: in
  * place on the packed susceph (npack, nw),
  *   eps_ij = delta_ij - sqrt(coul_i) chi_ij sqrt(coul_j),
- * and with invert != 0 its inverse (Cholesky; eps must be positive definite, as it
- * is for a negative semi-definite chi, otherwise SPX_EINVAL names the frequency).
+ * and with invert != 0 its inverse (the library's block Gauss-Jordan sweep on the
+ * DMMA path, all frequencies at once; eps must be positive definite, as it is for a
+ * negative semi-definite chi, otherwise SPX_EINVAL names the frequency).
  * coul: Coulomb eigenvalues (nbas), device. head (6, nw) and wing (3, nbas, nw) may
- * be NULL; if given they become 1 - 4 pi head and -sqrt(4 pi) sqrt(coul_i) wing.
- * The factorisation uses cuSOLVER, loaded at the first inverting call. */
+ * be NULL; if given they become 1 - 4 pi head and -sqrt(4 pi) sqrt(coul_i) wing. */
 int spx_dielec_dev(spx_ctx* ctx, int32_t nbas, int32_t nw, double* susceph,
                    const double* coul, int32_t invert, double* head, double* wing,
                    void* stream);
@@ -277,10 +293,15 @@ int spx_dielec_dev(spx_ctx* ctx, int32_t nbas, int32_t nw, double* susceph,
  * spx_chi0_accumulate_dev (same slabs and kernels, so the same bits). Its M is
  * a device array, or is generated on the device slab by slab from the seeded
  * Philox stream (cprod = NULL), so that no q's M is ever held whole.
- * Unless SPX_BATCH_NOGRAPH is given, the whole schedule (generation, weights,
- * operand preparation, accumulation of every slab of every q) is captured once
- * into a CUDA graph, cached in the context under the batch's signature, and
- * replayed with a single launch. */
+ * With SPX_SPLIT the whole batch runs as ONE persistent kernel: every SM takes
+ * accumulation items (slab, tile, frequency) and operand-preparation items
+ * (generation of M, weights, digit planes) from two device work queues, the q
+ * with most work first, with bounded waits on the slabs' readiness; the tile
+ * shape and slab size come from the tuning table (spx_autotune_batched). With
+ * SPX_FP64, or SPX_SPLIT with SPX_BATCH_KERNELS, the schedule is the sequence of
+ * per-slab kernels of spx_chi0_accumulate_dev. Unless SPX_BATCH_NOGRAPH is
+ * given, the schedule is captured once into a CUDA graph, cached in the context
+ * under the batch's signature, and replayed with a single graph launch. */
 typedef struct spx_q_desc {
   int32_t nbas;             /* N_MB of this q                                         */
   int32_t variant;          /* split kernel: 0 tuned / context default, 1 one CTA per
@@ -303,6 +324,7 @@ typedef struct spx_q_desc {
 
 #define SPX_BATCH_AUTOTUNE 1  /* measure (N, P) buckets missing from the table first  */
 #define SPX_BATCH_NOGRAPH  2  /* enqueue the schedule directly, without a graph       */
+#define SPX_BATCH_KERNELS  4  /* split precision as per-slab kernels, not persistent  */
 
 /* omega: device (nw). Ordered on `stream`; returns once enqueued unless stats. */
 int spx_chi0_batched(spx_ctx* ctx, int32_t nq, const spx_q_desc* q, int32_t nw,
@@ -310,14 +332,17 @@ int spx_chi0_batched(spx_ctx* ctx, int32_t nq, const spx_q_desc* q, int32_t nw,
                      spx_chi0_stats* stats);
 
 /* Split-path tuning table of a context: per (N_MB bucket, pair bucket, nw) the
- * kernel variant and slab size that measured fastest on a probe of that shape. */
+ * kernel variant and slab size that measured fastest on a probe of that shape,
+ * for single calls (variant 1 or 2) and for the persistent batched schedule
+ * (variant 3, with its tile shape). */
 typedef struct spx_tune_entry {
   int32_t nbas_bucket;      /* ceil(nbas / 128)                                        */
   int32_t npair_bucket;     /* 0: npair <= 16384, 1: <= 32768, 2: more                 */
   int32_t nw;
-  int32_t variant;          /* 1 one CTA per tile, 2 CTA pair                          */
+  int32_t variant;          /* 1 one CTA per tile, 2 CTA pair, 3 persistent batched    */
   int32_t slab_pairs;
-  int32_t reserved;
+  int32_t tile;             /* variant 3: tile columns (64 or 32) + 256 * pipeline
+                               stages (3 or 4); 0 otherwise                           */
   double  tflops;           /* measured throughput of the chosen configuration        */
 } spx_tune_entry;
 
@@ -328,6 +353,13 @@ int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
 /* SPX_OK and *out if the bucket of (nbas, npair, nw) is in the table, else SPX_ENOTSUP. */
 int spx_tune_lookup(const spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
                     spx_tune_entry* out);
+/* The same for the persistent batched schedule: measures its tile shapes (64 or 32
+ * complex columns per tile, 3 or 4 pipeline stages) and slab sizes on a seeded
+ * probe of one q, stores the fastest (variant 3), and looks entries up. */
+int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
+                         spx_tune_entry* out);
+int spx_tune_lookup_batched(const spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
+                            spx_tune_entry* out);
 /* The table as a JSON file, and back (entries are merged into the table). */
 int spx_tune_save(const spx_ctx* ctx, const char* path);
 int spx_tune_load(spx_ctx* ctx, const char* path);

@@ -351,3 +351,29 @@ def dielec(susceph, coul, invert=True, head=None, wing=None):
     if wing is not None:
         res.append(-np.sqrt(4 * np.pi) * sq[None, :, None] * np.asarray(wing))
     return res if len(res) > 1 else out
+
+
+def chi0_realfreq(cprod, wr, wi, suscepc=None) -> np.ndarray:
+    """suscepc(i, j, f) of src/susceptibility.f:1182-1235 (full-matrix layout) for real
+    frequencies: per pair (i <= j) re/im = cprod(:,i) conj(cprod(:,j)) (:1199), the four
+    ddots of spectral_function with wghtSr / wghtSi (:1829-1838, here the effective pair
+    weights wr, wi), then
+      suscepc(i,j) += cmplx(sus1, susc1) + cmplx(-susc2, sus2)
+      suscepc(j,i) += cmplx(sus1, susc1) - cmplx(-susc2, sus2)   (i /= j)
+    Vectorised over i for each j (numpy); returns (nbas, nbas, nw) complex."""
+    cprod = np.asarray(cprod, dtype=np.complex128)
+    wr = np.asarray(wr, dtype=np.float64)
+    wi = np.asarray(wi, dtype=np.float64)
+    npair, nbas = cprod.shape
+    nw = wr.shape[1]
+    if suscepc is None:
+        suscepc = np.zeros((nbas, nbas, nw), dtype=np.complex128, order="F")
+    for j in range(nbas):
+        x = cprod[:, : j + 1] * np.conj(cprod[:, j])[:, None]      # (npair, j+1): i <= j
+        re, im = x.real, x.imag
+        sus1, sus2 = re.T @ wr, im.T @ wr                           # (j+1, nw)
+        susc1, susc2 = re.T @ wi, im.T @ wi
+        suscepc[: j + 1, j, :] += (sus1 - susc2) + 1j * (susc1 + sus2)
+        lower = (sus1 + susc2) + 1j * (susc1 - sus2)
+        suscepc[j, :j, :] += lower[:j]
+    return suscepc

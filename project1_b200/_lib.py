@@ -80,12 +80,12 @@ class spx_q_desc(C.Structure):
 class spx_tune_entry(C.Structure):
     _fields_ = [
         ("nbas_bucket", C.c_int32), ("npair_bucket", C.c_int32), ("nw", C.c_int32),
-        ("variant", C.c_int32), ("slab_pairs", C.c_int32), ("reserved", C.c_int32),
+        ("variant", C.c_int32), ("slab_pairs", C.c_int32), ("tile", C.c_int32),
         ("tflops", C.c_double),
     ]
 
 
-SPX_BATCH_AUTOTUNE, SPX_BATCH_NOGRAPH = 1, 2
+SPX_BATCH_AUTOTUNE, SPX_BATCH_NOGRAPH, SPX_BATCH_KERNELS = 1, 2, 4
 
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
@@ -125,15 +125,21 @@ SIGNATURES = {
         C.c_int, [_P, _I64, _I32, _P, _I64, C.c_double, _I32, _P, C.c_double, _P, _I64, _P]),
     "spx_chi0_accumulate_w_dev": (
         C.c_int, [_P, _P, _I64, _I64, _I32, _P, _I64, _I32, _I32, _P, _P, C.POINTER(spx_chi0_stats)]),
+    "spx_chi0_accumulate_c_dev": (
+        C.c_int, [_P, _P, _I64, _I64, _I32, _P, _P, _I64, _I32, _I32, _P, _I64, _P,
+                  C.POINTER(spx_chi0_stats)]),
     "spx_headwings_dev": (
         C.c_int, [_P, _P, _I64, _I64, _I32, _P, _I64, _P, _I64, _I32, _P, _P, _P]),
     "spx_dielec_dev": (C.c_int, [_P, _I32, _I32, _P, _P, _I32, _P, _P, _P]),
     "spx_selftest_wait_dev": (C.c_int, [_P, _I32]),
+    "spx_measure_dmma_peak": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "spx_trafo_dev": (C.c_int, [_P, _P, _I64, _I64, _I32, _P, _I64, _I32, _P, _I64, _P]),
     "spx_chi0_batched": (
         C.c_int, [_P, _I32, C.POINTER(spx_q_desc), _I32, _P, _I32, _I32, _P, C.POINTER(spx_chi0_stats)]),
     "spx_autotune_split": (C.c_int, [_P, _I32, _I64, _I32, C.POINTER(spx_tune_entry)]),
     "spx_tune_lookup": (C.c_int, [_P, _I32, _I64, _I32, C.POINTER(spx_tune_entry)]),
+    "spx_autotune_batched": (C.c_int, [_P, _I32, _I64, _I32, C.POINTER(spx_tune_entry)]),
+    "spx_tune_lookup_batched": (C.c_int, [_P, _I32, _I64, _I32, C.POINTER(spx_tune_entry)]),
     "spx_tune_save": (C.c_int, [_P, C.c_char_p]),
     "spx_tune_load": (C.c_int, [_P, C.c_char_p]),
     "spx_gen_normal_host": (None, [C.c_uint64, C.c_uint32, _I64, _I64, C.c_double, _P]),

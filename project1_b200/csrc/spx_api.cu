@@ -286,6 +286,7 @@ extern "C" int spx_ctx_destroy(spx_ctx* ctx) {
   for (auto& g : ctx->graphs) {
     cudaGraphExecDestroy(g.exec);
     cudaGraphDestroy(g.graph);
+    if (g.mem) cudaFree(g.mem);
   }
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -657,6 +658,41 @@ extern "C" int spx_weights_hilbert_dev(spx_ctx* ctx, int64_t npair, int32_t nfrq
                                 pick_stream(ctx, stream));
 }
 
+// Adds sum_p M(p,i) conj(M(p,j)) w(p,f) with caller weights (any sign) into the
+// packed `out`, using `scratch` (accumulate_w_scratch bytes) for the padded weight
+// copy and the split path's planes.
+static size_t accumulate_w_scratch(int64_t npair, int nbas, int nw, int precision) {
+  const int64_t ldi = (int64_t)align_up((size_t)npair, 16);
+  return align_up(sizeof(double) * (size_t)ldi * nw, 256) +
+         (precision == SPX_SPLIT ? split_workspace_bytes(npair, nbas, nw) : 0);
+}
+
+static int accumulate_w_into(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
+                             int nbas, const double* w, int64_t ldw, int nw, int precision,
+                             double* out, char* scratch, cudaStream_t s, int* launches) {
+  // the kernels read the weights with 16-pair bulk copies: an aligned, padded copy
+  const int64_t ldi = (int64_t)align_up((size_t)npair, 16);
+  const size_t wbytes = align_up(sizeof(double) * (size_t)ldi * nw, 256);
+  const size_t sbytes = precision == SPX_SPLIT ? split_workspace_bytes(npair, nbas, nw) : 0;
+  double* W = (double*)scratch;
+  void* sws = scratch + wbytes;
+  int rc;
+  if ((rc = check_cuda(ctx, cudaMemsetAsync(W, 0, wbytes, s), "zero weights")) ||
+      (rc = check_cuda(ctx, cudaMemcpy2DAsync(W, sizeof(double) * ldi, w, sizeof(double) * ldw,
+                                              sizeof(double) * npair, nw, cudaMemcpyDeviceToDevice, s),
+                       "copy weights")))
+    return rc;
+  if (precision == SPX_FP64) {
+    timing_mark(ctx, s, 1);
+    rc = launch_chi0_fp64(ctx, reinterpret_cast<const double2*>(cprod), ldc, npair, nbas, W, ldi, nw,
+                          reinterpret_cast<double2*>(out), s, 8);
+    ++*launches;
+    return rc;
+  }
+  return split_chi0_slab(ctx, reinterpret_cast<const double2*>(cprod), ldc, npair, nbas, W, ldi, nw,
+                         reinterpret_cast<double2*>(out), sws, sbytes, s, launches, 0, 0);
+}
+
 extern "C" int spx_chi0_accumulate_w_dev(spx_ctx* ctx, const double* cprod, int64_t ldc,
                                          int64_t npair, int32_t nbas, const double* w, int64_t ldw,
                                          int32_t nw, int32_t precision, double* susceph,
@@ -674,35 +710,74 @@ extern "C" int spx_chi0_accumulate_w_dev(spx_ctx* ctx, const double* cprod, int6
   }
   if (npair == 0 || nbas == 0 || nw == 0) return SPX_OK;
   cudaStream_t s = pick_stream(ctx, stream);
-  // the kernels read the weights with 16-pair bulk copies: an aligned, padded copy
-  const int64_t ldi = (int64_t)align_up((size_t)npair, 16);
-  const size_t wbytes = align_up(sizeof(double) * (size_t)ldi * nw, 256);
-  const size_t sbytes = precision == SPX_SPLIT ? split_workspace_bytes(npair, nbas, nw) : 0;
-  if ((rc = ensure_workspace(ctx, wbytes + sbytes))) return rc;
-  double* W = (double*)ctx->ws;
-  void* sws = (char*)ctx->ws + wbytes;
-  if ((rc = check_cuda(ctx, cudaMemsetAsync(W, 0, wbytes, s), "zero weights")) ||
-      (rc = check_cuda(ctx, cudaMemcpy2DAsync(W, sizeof(double) * ldi, w, sizeof(double) * ldw,
-                                              sizeof(double) * npair, nw, cudaMemcpyDeviceToDevice, s),
-                       "copy weights")))
-    return rc;
+  if ((rc = ensure_workspace(ctx, accumulate_w_scratch(npair, nbas, nw, precision)))) return rc;
   int launches = 0;
   ctx->timing = stats != nullptr;
   ctx->nmarks = 0;
-  if (precision == SPX_FP64) {
-    timing_mark(ctx, s, 1);
-    rc = launch_chi0_fp64(ctx, reinterpret_cast<const double2*>(cprod), ldc, npair, nbas, W, ldi, nw,
-                          reinterpret_cast<double2*>(susceph), s, 8);
-    ++launches;
-  } else {
-    rc = split_chi0_slab(ctx, reinterpret_cast<const double2*>(cprod), ldc, npair, nbas, W, ldi, nw,
-                         reinterpret_cast<double2*>(susceph), sws, sbytes, s, &launches, 0, 0);
-  }
+  rc = accumulate_w_into(ctx, cprod, ldc, npair, nbas, w, ldw, nw, precision, susceph,
+                         (char*)ctx->ws, s, &launches);
   timing_mark(ctx, s, 2);
   ctx->timing = false;
   if (rc) return rc;
   if (stats) {
     rc = collect_status(ctx, s, "chi0_accumulate_w_dev");
+    if (rc) return rc;
+    timing_collect(ctx, &stats->ms_prep, &stats->ms_gram);
+    stats->kernel_launches = launches;
+    stats->ms_total =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return SPX_OK;
+}
+
+namespace spx {
+int launch_suscepc_combine(spx_ctx*, int, int, const double2*, const double2*, double2*, int64_t,
+                           cudaStream_t);
+}
+
+extern "C" int spx_chi0_accumulate_c_dev(spx_ctx* ctx, const double* cprod, int64_t ldc,
+                                         int64_t npair, int32_t nbas, const double* wr,
+                                         const double* wi, int64_t ldw, int32_t nw,
+                                         int32_t precision, double* suscepc, int64_t ldo,
+                                         void* stream, spx_chi0_stats* stats) {
+  int rc = check_chi0_args(ctx, cprod, ldc, npair, nbas, wr, nw, wr, precision, suscepc);
+  if (rc) return rc;
+  if (npair > 0 && nw > 0 && (!wi || ldw < npair)) return set_error(ctx, SPX_EINVAL, "wi NULL or ldw < npair");
+  if (nbas > 0 && ldo < nbas) return set_error(ctx, SPX_EINVAL, "ldo < nbas");
+  cudaSetDevice(ctx->device);
+  auto t0 = std::chrono::steady_clock::now();
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->precision = precision;
+    stats->flops = 2 * 8.0 * (double)nbas * nbas * (double)npair * nw;
+  }
+  if (npair == 0 || nbas == 0 || nw == 0) return SPX_OK;
+  cudaStream_t s = pick_stream(ctx, stream);
+  // two packed Hermitian sums S1 (weights wr) and S2 (weights wi), then the full matrix
+  const int64_t npack = (int64_t)nbas * (nbas + 1) / 2;
+  const size_t pbytes = align_up(sizeof(double2) * (size_t)npack * nw, 256);
+  const size_t sc = accumulate_w_scratch(npair, nbas, nw, precision);
+  if ((rc = ensure_workspace(ctx, 2 * pbytes + sc))) return rc;
+  double* S1 = (double*)ctx->ws;
+  double* S2 = (double*)((char*)ctx->ws + pbytes);
+  char* scratch = (char*)ctx->ws + 2 * pbytes;
+  int launches = 0;
+  ctx->timing = stats != nullptr;
+  ctx->nmarks = 0;
+  if ((rc = check_cuda(ctx, cudaMemsetAsync(S1, 0, 2 * pbytes, s), "zero partial sums"))) return rc;
+  rc = accumulate_w_into(ctx, cprod, ldc, npair, nbas, wr, ldw, nw, precision, S1, scratch, s, &launches);
+  if (!rc) rc = accumulate_w_into(ctx, cprod, ldc, npair, nbas, wi, ldw, nw, precision, S2, scratch, s, &launches);
+  if (!rc) {
+    timing_mark(ctx, s, 0);
+    rc = launch_suscepc_combine(ctx, nbas, nw, (const double2*)S1, (const double2*)S2,
+                                reinterpret_cast<double2*>(suscepc), ldo, s);
+    ++launches;
+  }
+  timing_mark(ctx, s, 2);
+  ctx->timing = false;
+  if (rc) return rc;
+  if (stats) {
+    rc = collect_status(ctx, s, "chi0_accumulate_c_dev");
     if (rc) return rc;
     timing_collect(ctx, &stats->ms_prep, &stats->ms_gram);
     stats->kernel_launches = launches;

@@ -40,6 +40,12 @@ int launch_gen_cmatrix_rows(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, int6
 int launch_gen_normal(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, double, double*,
                       cudaStream_t);
 
+struct PbConfig {
+  int bn, stages;
+};
+int pb_run(spx_ctx* ctx, int nq, const spx_q_desc* q, int nw, const double* omega, int flags,
+           cudaStream_t s, int* launches, const PbConfig* force, int force_slab);
+
 constexpr int kDefaultVariant = 2;
 constexpr int kDefaultSlab = 32768;
 constexpr int64_t kChunkSlabs = 8;   // pairs per generated / weighted chunk, in slabs
@@ -51,13 +57,14 @@ static int npair_bucket(int64_t P) { return P <= 16384 ? 0 : (P <= 32768 ? 1 : 2
 static const spx_tune_entry* find_tune(const spx_ctx* ctx, int N, int64_t P, int nw) {
   const int nb = nbas_bucket(N), pb = npair_bucket(P);
   for (const auto& e : ctx->tune)
-    if (e.nbas_bucket == nb && e.npair_bucket == pb && e.nw == nw) return &e;
+    if (e.variant != 3 && e.nbas_bucket == nb && e.npair_bucket == pb && e.nw == nw) return &e;
   return nullptr;
 }
 
 static void store_tune(spx_ctx* ctx, const spx_tune_entry& t) {
   for (auto& e : ctx->tune)
-    if (e.nbas_bucket == t.nbas_bucket && e.npair_bucket == t.npair_bucket && e.nw == t.nw) {
+    if ((e.variant == 3) == (t.variant == 3) && e.nbas_bucket == t.nbas_bucket &&
+        e.npair_bucket == t.npair_bucket && e.nw == t.nw) {
       e = t;
       return;
     }
@@ -184,6 +191,33 @@ extern "C" int spx_chi0_batched(spx_ctx* ctx, int32_t nq, const spx_q_desc* q, i
   }
   if (nq == 0 || nw == 0) return SPX_OK;
   int rc;
+  const bool persistent = precision == SPX_SPLIT && !(flags & SPX_BATCH_KERNELS);
+  if (persistent) {
+    if (flags & SPX_BATCH_AUTOTUNE)
+      for (int i = 0; i < nq; ++i) {
+        spx_tune_entry t;
+        if (q[i].npair > 0 && q[i].nbas > 0 && q[i].slab_pairs == 0 &&
+            spx_tune_lookup_batched(ctx, q[i].nbas, q[i].npair, nw, &t) != SPX_OK &&
+            (rc = spx_autotune_batched(ctx, q[i].nbas, q[i].npair, nw, nullptr)))
+          return rc;
+      }
+    cudaStream_t s = pick_stream(ctx, stream);
+    cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+    if (stats) cudaEventRecord(e0, s);
+    int launches = 0;
+    if ((rc = pb_run(ctx, nq, q, nw, omega, flags, s, &launches, nullptr, 0))) return rc;
+    if (stats) {
+      cudaEventRecord(e1, s);
+      if ((rc = collect_status(ctx, s, "chi0_batched"))) return rc;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      stats->ms_gram = ms;
+      stats->kernel_launches = launches;
+      stats->ms_total =
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return SPX_OK;
+  }
   // tune the buckets the table lacks, before anything is captured
   if ((flags & SPX_BATCH_AUTOTUNE) && precision == SPX_SPLIT) {
     for (int i = 0; i < nq; ++i)
@@ -248,9 +282,10 @@ extern "C" int spx_chi0_batched(spx_ctx* ctx, int32_t nq, const spx_q_desc* q, i
                                     });
         cudaGraphExecDestroy(old->exec);
         cudaGraphDestroy(old->graph);
+        if (old->mem) cudaFree(old->mem);
         ctx->graphs.erase(old);
       }
-      ctx->graphs.push_back({key, graph, exec, 0});
+      ctx->graphs.push_back({key, graph, exec, 0, nullptr});
       hit = &ctx->graphs.back();
       launches = cap_launches;
     }
@@ -383,8 +418,9 @@ extern "C" int spx_tune_save(const spx_ctx* ctx, const char* path) {
     const spx_tune_entry& e = ctx->tune[i];
     fprintf(f,
             "%s\n    {\"nbas_bucket\": %d, \"npair_bucket\": %d, \"nw\": %d, \"variant\": %d, "
-            "\"slab_pairs\": %d, \"tflops\": %.3f}",
-            i ? "," : "", e.nbas_bucket, e.npair_bucket, e.nw, e.variant, e.slab_pairs, e.tflops);
+            "\"slab_pairs\": %d, \"tile\": %d, \"tflops\": %.3f}",
+            i ? "," : "", e.nbas_bucket, e.npair_bucket, e.nw, e.variant, e.slab_pairs, e.tile,
+            e.tflops);
   }
   fprintf(f, "\n  ]\n}\n");
   return fclose(f) == 0 ? SPX_OK : SPX_EINVAL;
@@ -417,13 +453,15 @@ extern "C" int spx_tune_load(spx_ctx* ctx, const char* path) {
     const size_t e = txt.find('}', p);
     if (e == std::string::npos) break;
     const std::string obj = txt.substr(p, e - p + 1);
-    double nb, pb, nw, var, sl, tf = 0;
+    double nb, pb, nw, var, sl, tf = 0, tile = 0;
     if (!json_field(obj, "nbas_bucket", &nb) || !json_field(obj, "npair_bucket", &pb) ||
         !json_field(obj, "nw", &nw) || !json_field(obj, "variant", &var) ||
         !json_field(obj, "slab_pairs", &sl))
       return set_error(ctx, SPX_EINVAL, "malformed tuning entry");
     json_field(obj, "tflops", &tf);
-    if (var < 1 || var > 2 || sl < 64 || sl > 32768 || nb < 1 || nw < 1 || pb < 0 || pb > 2)
+    json_field(obj, "tile", &tile);
+    if (var < 1 || var > 3 || sl < 64 || sl > 32768 || nb < 1 || nw < 1 || pb < 0 || pb > 2 ||
+        tile < 0 || tile > 4 * 256 + 64)
       return set_error(ctx, SPX_EINVAL, "tuning entry out of range");
     spx_tune_entry t{};
     t.nbas_bucket = (int)nb;
@@ -431,6 +469,7 @@ extern "C" int spx_tune_load(spx_ctx* ctx, const char* path) {
     t.nw = (int)nw;
     t.variant = (int)var;
     t.slab_pairs = (int)sl;
+    t.tile = (int)tile;
     t.tflops = tf;
     got.push_back(t);
     p = e;

@@ -1,0 +1,951 @@
+// K7: the split-precision polarisation of many q points as ONE persistent launch.
+//
+// The reference computes one q point per call of `susceptibility`
+// (src/correlation.f:293-339), each q with its own mixed basis and band window and
+// its pairs split into packets (src/susceptibility.f:632-642). Here the whole batch
+// is one kernel: one CTA per SM, each CTA running two independent workers over
+// two device work queues.
+//
+//   * The accumulation pipeline (warp 0 TMA, warp 1 tcgen05 MMA, warps 2-5
+//     epilogue) takes items (slab k, tile, frequency) from the accumulation queue:
+//     the same 6-product int8 accumulation of the folded digit planes as the
+//     one-call kernel, 64 complex rows x BN complex columns per item.
+//   * Six preparation warps take items from the preparation queue: for slab k
+//     (a) generate M (or read the caller's) and take the column maxima, (b) the
+//     HILBERT NONE weights of one frequency, their maximum, sign and folded
+//     factors, (c) the digit planes of 8 columns.
+//
+// Slabs are ordered q by q, the q with most work first, and live in a ring of
+// NSLOT operand buffers. Dependencies are counters in device memory, each waited
+// on with a bounded spin: an accumulation item waits until its slab's planes are
+// ready; a preparation item waits until the slab that last used its buffer has
+// been fully accumulated, and a quantizer item until its slab's maxima and
+// factors exist. Every wait is on items already handed to a running CTA (a queue
+// hands items out only to CTAs that run), so the schedule cannot deadlock, whether
+// or not all CTAs are resident. The epilogue of slab s of a q adds into an output
+// tile only after slab s-1 has added into it (a per-(q, tile, frequency) counter),
+// so the sums happen in the same order as per-q calls and give the same bits.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "spx_philox.h"
+#include "spx_split.cuh"
+
+namespace spx {
+
+constexpr int PB_THREADS = 384;   // warps 0-5 accumulation, 6-11 preparation
+constexpr int PB_PREP0 = 192;     // first preparation thread
+constexpr int PB_NPREP = 192;
+constexpr int PB_RING = 4;        // item descriptors in flight between the pipeline roles
+constexpr int PB_ACOLS = 6;       // columns per (a) item: one per preparation warp
+constexpr int PB_QCOLS = 8;       // columns per (c) item
+
+struct PbQ {            // one q point
+  int N, nblk, ntile, npad, S, nslab;
+  int64_t P, npack, R;
+  const double2* M;     // caller's cprod (ldc) or NULL: generated
+  int64_t ldc;
+  uint64_t seed;
+  uint32_t sid;
+  double mscale;
+  const double* ediff;
+  const double* wscale;
+  double scale_all;
+  double* out;
+  int* seq;             // ntile * nw ordering counters
+};
+
+struct PbSlab {         // one slab of one q, in queue order
+  int q, s, slot;
+  int len, lenp, nk;
+  int64_t p0;
+  int64_t g0;           // first accumulation item
+  int64_t r0;           // first preparation item
+  int na, nb, nc;       // preparation items of kinds a, b, c
+  int ngram;
+};
+
+struct PbSlot {         // one operand buffer of the ring
+  int8_t* F;
+  double* G;
+  double* sA;
+  double* wmax;
+  int* wsgn;
+  double2* Mbuf;
+};
+
+struct PbParams {
+  const PbQ* q;
+  const PbSlab* slab;
+  const PbSlot* slot;
+  const CUtensorMap* maps;   // per (q, slot): A box (128 rows), B box (2 BN rows)
+  int nslab, nslot, nw;
+  int64_t ngram, nprep;
+  const double* omega;
+  unsigned long long* heads;  // [0] accumulation queue, [1] preparation queue
+  int* ab;                    // per slab: finished (a) + (b) items
+  int* ready;                 // per slab: finished (c) items
+  int* gdone;                 // per slab: finished accumulation items
+  int* status;
+  uint64_t timeout_ns;
+};
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void red_release_add(int* p, int v) {
+  asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+// Bounded wait until *ctr >= target (acquire). False on timeout (status set) or
+// when another worker has already given up.
+__device__ __noinline__ bool gwait(const int* ctr, int target, uint64_t timeout_ns, int* status) {
+  if (ld_acquire(ctr) >= target) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t n = 1;; ++n) {
+    __nanosleep(64);
+    if (ld_acquire(ctr) >= target) return true;
+    if ((n & 31) == 0) {
+      if (global_ns() - t0 > timeout_ns) {
+        atomicCAS(status, 0, (int)kStatusTimeout);
+        return false;
+      }
+      if (*((volatile int*)status) != 0) return false;
+    }
+  }
+}
+// The last index k with key(k) <= v over a nondecreasing array (first entry <= v).
+__device__ __forceinline__ int pb_find(const PbSlab* sl, int n, int64_t v, bool prep) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if ((prep ? sl[mid].r0 : sl[mid].g0) <= v) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+// Tile t of the upper region for BN-column tiles -> (bi 64-row block, bj BN-column
+// block), column-major: column block bj holds row blocks 0..(bj*BN + BN - 1)/64.
+template <int BN>
+__device__ __forceinline__ void pb_decode_tile(int t, int* bi, int* bj) {
+  if constexpr (BN == 64) {
+    split_decode_tile(t, bi, bj);
+  } else {
+    int j = 0, c = 0;
+    while (c + (j * BN + BN - 1) / 64 + 1 <= t) {
+      c += (j * BN + BN - 1) / 64 + 1;
+      ++j;
+    }
+    *bj = j;
+    *bi = t - c;
+  }
+}
+#endif
+
+template <int BN>
+constexpr int pb_ntile(int N) {
+  int nb = (N + BN - 1) / BN, c = 0;
+  for (int j = 0; j < nb; ++j) c += (j * BN + BN - 1) / 64 + 1;
+  return c;
+}
+
+template <int BN, int ST>
+struct __align__(1024) PbSmem {
+  uint8_t a[ST][SP_SF][SP_PLANE];
+  uint8_t b[ST][SP_SF][2 * BN * SP_KB];
+  double stage[SP_ROWS][BN + 1];        // epilogue: the tile's values, read out of TMEM
+  uint64_t full[ST], empty[ST];
+  uint64_t tfull, tempty, mdone;
+  uint64_t ifull[PB_RING], ifree[PB_RING];
+  int4 desc[PB_RING];                   // item: slab k, tile, frequency, flags
+  long long prep_item;
+  int eflag;
+  double red[PB_NPREP / 32];
+  int redi[2][PB_NPREP / 32];
+  uint32_t tmem_base;
+};
+
+#if defined(__CUDACC__)
+// ---------------- preparation workers (192 threads) ----------------
+__device__ __forceinline__ void pb_prep_bar() { named_bar_sync(1, PB_NPREP); }
+
+template <int BN, int ST>
+__device__ void pb_prep(PbSmem<BN, ST>& sm, const PbParams& prm, int pt) {
+  const int pw = pt >> 5, lane = pt & 31;
+  for (;;) {
+    if (pt == 0) sm.prep_item = (long long)atomicAdd(&prm.heads[1], 1ull);
+    pb_prep_bar();
+    const int64_t item = sm.prep_item;
+    pb_prep_bar();  // everyone has read it before thread 0 may overwrite it
+    if (item >= prm.nprep) return;
+    const int k = pb_find(prm.slab, prm.nslab, item, true);
+    const PbSlab& sl = prm.slab[k];
+    const PbQ& q = prm.q[sl.q];
+    const PbSlot& slot = prm.slot[sl.slot];
+    int64_t local = item - sl.r0;
+    const int kind = local < sl.na ? 0 : (local < sl.na + sl.nb ? 1 : 2);
+    local -= kind == 0 ? 0 : (kind == 1 ? sl.na : sl.na + sl.nb);
+    // the buffer must be free (the slab that used it last fully accumulated), and a
+    // quantizer item needs its slab's maxima and factors
+    int ok = 1;
+    if (pt == 0) {
+      if (k >= prm.nslot) {
+        const PbSlab& prev = prm.slab[k - prm.nslot];
+        ok = gwait(&prm.gdone[k - prm.nslot], prev.ngram, prm.timeout_ns, prm.status);
+      }
+      if (ok && kind == 2) ok = gwait(&prm.ab[k], sl.na + sl.nb, prm.timeout_ns, prm.status);
+      sm.redi[0][0] = ok;
+    }
+    pb_prep_bar();
+    ok = sm.redi[0][0];
+    pb_prep_bar();
+    if (!ok) return;
+
+    if (kind == 0) {
+      // (a) column i: M values of the slab (generated into the buffer, or the
+      // caller's) and their largest |Re|, |Im|
+      const int i = (int)local * PB_ACOLS + pw;
+      if (i < q.N) {
+        double m = 0.0;
+        if (q.M) {
+          const double2* col = q.M + (int64_t)i * q.ldc + sl.p0;
+          for (int p = lane; p < sl.len; p += 32) {
+            const double2 v = col[p];
+            m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+          }
+        } else {
+          double2* dst = slot.Mbuf + (int64_t)i * sl.lenp;
+          for (int p = lane; p < sl.len; p += 32) {
+            double z0, z1;
+            normal_pair(q.seed, q.sid, (uint64_t)(q.P * i + sl.p0 + p), &z0, &z1);
+            const double2 v = make_double2(__dmul_rn(q.mscale, z0), __dmul_rn(q.mscale, z1));
+            dst[p] = v;
+            m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+          }
+        }
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) slot.sA[i] = m;
+      }
+    } else if (kind == 1) {
+      // (b) frequency f: weights, their maximum and sign, the folded factors
+      const int f = (int)local;
+      const double om = prm.omega[f];
+      double m = 0.0;
+      int pos = 0, neg = 0;
+      for (int p = pt; p < sl.len; p += PB_NPREP) {
+        const double s = (q.wscale ? q.wscale[sl.p0 + p] : 1.0) * q.scale_all;
+        const double w = hilbert_none_weight(q.ediff[sl.p0 + p], om, s);
+        m = fmax(m, fabs(w));
+        pos |= w > 0.0;
+        neg |= w < 0.0;
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        pos |= __shfl_xor_sync(0xffffffffu, pos, o);
+        neg |= __shfl_xor_sync(0xffffffffu, neg, o);
+      }
+      if (lane == 0) sm.red[pw] = m, sm.redi[0][pw] = pos, sm.redi[1][pw] = neg;
+      pb_prep_bar();
+      m = 0.0;
+      pos = neg = 0;
+#pragma unroll
+      for (int w = 0; w < PB_NPREP / 32; ++w)
+        m = fmax(m, sm.red[w]), pos |= sm.redi[0][w], neg |= sm.redi[1][w];
+      pb_prep_bar();
+      if (pt == 0) {
+        slot.wmax[f] = m;
+        slot.wsgn[f] = (pos && neg) ? 0 : (neg ? -1 : 1);
+      }
+      double* gf = slot.G + (int64_t)f * sl.lenp;
+      for (int p = pt; p < sl.lenp; p += PB_NPREP) {
+        double g = 0.0;
+        if (p < sl.len) {
+          const double s = (q.wscale ? q.wscale[sl.p0 + p] : 1.0) * q.scale_all;
+          g = fold_factor(hilbert_none_weight(q.ediff[sl.p0 + p], om, s), m);
+        }
+        gf[p] = g;
+      }
+    } else {
+      // (c) digit planes of 8 columns: tasks (column, 16 pairs), a warp = 8 columns x
+      // the 4 quarters of one 64-pair block
+      const int nchunk = sl.lenp / 16;
+      const int64_t nkb = q.S / SP_KB;
+      const int64_t pstride = nkb * q.R * SP_KB;
+      for (int t = pt; t < PB_QCOLS * nchunk; t += PB_NPREP) {
+        const int lane8 = t & 7, quarter = (t >> 3) & 3, kb = t >> 5;
+        const int i = (int)local * PB_QCOLS + lane8;
+        const int p = kb * SP_KB + quarter * 16;
+        const bool col_ok = i < q.N;
+        const int ic = col_ok ? i : 0;
+        const double2* col =
+            q.M ? q.M + (int64_t)ic * q.ldc + sl.p0 : slot.Mbuf + (int64_t)ic * sl.lenp;
+        const int64_t o_re = ((int64_t)kb * q.R + split_row_re(i)) * SP_KB + quarter * 16;
+        quantize_task(col, col_ok, sl.len, p, col_ok ? slot.sA[i] : 0.0, o_re, pstride, prm.nw,
+                      slot.wsgn, slot.G, sl.lenp, slot.F);
+      }
+    }
+    // publish: generic stores become visible to the TMA (async proxy) and to the
+    // other CTAs before the counter moves
+    fence_proxy_async_global();
+    __threadfence();
+    pb_prep_bar();
+    if (pt == 0) red_release_add(kind == 2 ? &prm.ready[k] : &prm.ab[k], 1);
+  }
+}
+
+template <int BN, int ST>
+__global__ void __launch_bounds__(PB_THREADS, 1) pb_kernel(PbParams prm) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  using Smem = PbSmem<BN, ST>;
+  Smem& sm = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                      ~(uintptr_t)1023);
+  constexpr int BROWS = 2 * BN;                  // B rows (N of the MMA)
+  constexpr uint32_t IDESC = sp_idesc(BROWS);
+  constexpr uint32_t OSTRIDE = BROWS;            // TMEM columns per order
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], 1);
+    }
+    for (int r = 0; r < PB_RING; ++r) {
+      mbar_init(&sm.ifull[r], 1);
+      mbar_init(&sm.ifree[r], 1);
+    }
+    mbar_init(&sm.tfull, 1);
+    mbar_init(&sm.tempty, 4);
+    mbar_init(&sm.mdone, 1);
+    fence_barrier_init();
+  }
+  if (warp == 1) tmem_alloc(&sm.tmem_base, SP_TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sm.tmem_base;
+
+  if (threadIdx.x >= PB_PREP0) {
+    pb_prep<BN, ST>(sm, prm, threadIdx.x - PB_PREP0);
+  } else if (warp == 0) {
+    // ---------------- TMA producer: takes the items ----------------
+    if (lane == 0) {
+      int st = 0;
+      uint32_t ph = 0;
+      bool issued[ST];
+      uint32_t last_ph[ST];
+      for (int s = 0; s < ST; ++s) issued[s] = false, last_ph[s] = 0;
+      for (int j = 0;; ++j) {
+        const int r = j % PB_RING;
+        // the ring entry of item j - PB_RING has been retired by the epilogue
+        if (j >= PB_RING &&
+            !mbar_wait(&sm.ifree[r], (uint32_t)((j / PB_RING - 1) & 1), prm.timeout_ns, prm.status)) {
+          sm.desc[r] = make_int4(-1, 0, 0, 0);
+          mbar_arrive(&sm.ifull[r]);
+          break;
+        }
+        const int64_t g = (int64_t)atomicAdd(&prm.heads[0], 1ull);
+        if (g >= prm.ngram) {
+          sm.desc[r] = make_int4(-1, 0, 0, 0);
+          mbar_arrive(&sm.ifull[r]);
+          break;
+        }
+        const int k = pb_find(prm.slab, prm.nslab, g, false);
+        const PbSlab& sl = prm.slab[k];
+        const PbQ& q = prm.q[sl.q];
+        const int local = (int)(g - sl.g0);
+        const int f = local / q.ntile, tile = local % q.ntile;
+        int bi, bj;
+        pb_decode_tile<BN>(tile, &bi, &bj);
+        // the slab's planes must be ready before the first copy
+        const bool okr = gwait(&prm.ready[k], sl.nc, prm.timeout_ns, prm.status);
+        const int sg = okr ? prm.slot[sl.slot].wsgn[f] : 1;
+        const bool same = BN == SP_TILE && sg != 0 && bi == bj;
+        sm.desc[r] = make_int4(okr ? k : -1, tile, f, same ? 1 : 0);
+        mbar_arrive(&sm.ifull[r]);
+        if (!okr) break;
+        fence_proxy_async_global();
+        const CUtensorMap* mA = prm.maps + 2 * ((int64_t)sl.q * prm.nslot + sl.slot);
+        const CUtensorMap* mB = mA + 1;
+        const int za = f * SP_SLOT, zb = za + (sg == 0 ? SP_SF : 0);
+        bool ok = true;
+        for (int ks = 0; ks < sl.nk; ++ks) {
+          if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&sm.full[st], (uint32_t)(SP_SF * (SP_PLANE + (same ? 0 : BROWS * SP_KB))));
+          tma_load_4d(&sm.a[st][0][0], mA, 0, bi * SP_ROWS, ks, za, &sm.full[st]);
+          if (!same) tma_load_4d(&sm.b[st][0][0], mB, 0, bj * BROWS, ks, zb, &sm.full[st]);
+          issued[st] = true;
+          last_ph[st] = ph;
+          if (++st == ST) st = 0, ph ^= 1u;
+        }
+        if (!ok) break;
+      }
+      for (int s = 0; s < ST; ++s)
+        if (issued[s]) mbar_drain(&sm.full[s], last_ph[s], prm.timeout_ns);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      int st = 0;
+      uint32_t ph = 0;
+      bool committed = false;
+      for (int j = 0;; ++j) {
+        const int r = j % PB_RING;
+        if (!mbar_wait_idle(&sm.ifull[r], (uint32_t)((j / PB_RING) & 1), prm.timeout_ns, prm.status)) break;
+        const int4 d = sm.desc[r];
+        if (d.x < 0) break;
+        const int nk = prm.slab[d.x].nk;
+        const bool same = d.w != 0;
+        if (!mbar_wait(&sm.tempty, (uint32_t)(j & 1) ^ 1u, prm.timeout_ns, prm.status)) break;
+        tc_fence_after();
+        bool ok = true;
+        for (int ks = 0; ks < nk; ++ks) {
+          if (!mbar_wait(&sm.full[st], ph, prm.timeout_ns, prm.status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll
+          for (int kk = 0; kk < SP_NKS; ++kk) {
+            uint64_t da[SP_SF], db[SP_SF];
+#pragma unroll
+            for (int t = 0; t < SP_SF; ++t) {
+              da[t] = desc_sw64(&sm.a[st][t][0]) + (uint64_t)(kk * 2);
+              db[t] = same ? da[t] : desc_sw64(&sm.b[st][t][0]) + (uint64_t)(kk * 2);
+            }
+            const uint32_t k0 = (ks > 0 || kk > 0);
+            mma_i8<1>(tmem + 0 * OSTRIDE, da[0], db[0], IDESC, k0);
+            mma_i8<2>(tmem + 1 * OSTRIDE, da[0], db[1], IDESC, k0);
+            mma_i8<3>(tmem + 2 * OSTRIDE, da[0], db[2], IDESC, k0);
+            mma_i8<1>(tmem + 1 * OSTRIDE, da[1], db[0], IDESC, 1u);
+            mma_i8<3>(tmem + 2 * OSTRIDE, da[1], db[1], IDESC, 1u);
+            mma_i8<0>(tmem + 2 * OSTRIDE, da[2], db[0], IDESC, 1u);
+          }
+          tc_commit(&sm.empty[st]);
+          committed = true;
+          if (++st == ST) st = 0, ph ^= 1u;
+        }
+        if (!ok) break;
+        tc_commit(&sm.tfull);
+      }
+      if (committed) {
+        tc_commit(&sm.mdone);
+        mbar_drain(&sm.mdone, 0u, prm.timeout_ns);
+      }
+    }
+  } else {
+    // ---------------- epilogue: warps 2-5, TMEM lane quarter warp % 4 ----------------
+    const int qd = warp & 3;
+    const int row = 32 * qd + lane;          // TMEM lane = real-stacked row of the tile
+    const int c = lane & 1;
+    const uint32_t tl = tmem + ((uint32_t)(32 * qd) << 16);
+    const int et = threadIdx.x - 64;         // 0..127
+    for (int j = 0;; ++j) {
+      const int r = j % PB_RING;
+      if (!mbar_wait_idle(&sm.ifull[r], (uint32_t)((j / PB_RING) & 1), prm.timeout_ns, prm.status)) break;
+      const int4 d = sm.desc[r];
+      if (d.x < 0) break;
+      if (!mbar_wait_idle(&sm.tfull, (uint32_t)(j & 1), prm.timeout_ns, prm.status)) break;
+      tc_fence_after();
+      const PbSlab& sl = prm.slab[d.x];
+      const PbQ& q = prm.q[sl.q];
+      const PbSlot& slot = prm.slot[sl.slot];
+      int bi, bj;
+      pb_decode_tile<BN>(d.y, &bi, &bj);
+      const int f = d.z;
+      // the accumulator, combined into complex values, into shared memory
+#pragma unroll 1
+      for (int cc = 0; cc < BROWS / 16; ++cc) {
+        double T[16];
+        load_fold16(tl + (uint32_t)(16 * cc), OSTRIDE, T);
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          const double pb = __shfl_xor_sync(0xffffffffu, T[2 * jj + 1], 1);
+          sm.stage[row][8 * cc + jj] = c == 0 ? T[2 * jj] + pb : T[2 * jj] - pb;
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.tempty);  // the MMAs of the next item may start
+      // slab s of this q adds into the tile after slab s-1 did (the order of per-q calls)
+      int* seq = q.seq + (int64_t)f * q.ntile + d.y;
+      if (et == 0) sm.eflag = sl.s == 0 || gwait(seq, sl.s, prm.timeout_ns, prm.status);
+      named_bar_sync(2, 128);
+      const int ok = sm.eflag;
+      const int gil = bi * SP_TILE + row / 2;
+      if (ok && gil < q.N) {
+        const double fac = fold_row_factor(slot.wsgn[f], slot.sA[gil], slot.wmax[f]);
+        double* ob = q.out + 2 * (int64_t)f * q.npack + 2 * gil + c;
+        for (int jj = 0; jj < BN; ++jj) {
+          const int gj = bj * BN + jj;
+          if (gil <= gj && gj < q.N)
+            atomicAdd(ob + (int64_t)gj * (gj + 1), fac * slot.sA[gj] * sm.stage[row][jj]);
+        }
+      }
+      __threadfence();
+      named_bar_sync(2, 128);
+      if (et == 0) {
+        red_release_add(seq, 1);
+        red_release_add(&prm.gdone[d.x], 1);
+        mbar_arrive(&sm.ifree[r]);
+      }
+      if (!ok) break;
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc(tmem, SP_TMEM_COLS);
+}
+#endif
+
+// ---------------------------------------------------------------------------
+// host side
+
+int make_tmap_u8_4d(spx_ctx* ctx, CUtensorMap* map, const void* base, const uint64_t dims[4],
+                    const uint64_t strides[3], const uint32_t box[4], CUtensorMapSwizzle swz);
+
+struct PbConfig {
+  int bn, stages;
+};
+
+static size_t pb_smem(PbConfig c) {
+  if (c.bn == 64) return sizeof(PbSmem<64, 3>) + 1024;
+  return c.stages == 4 ? sizeof(PbSmem<32, 4>) + 1024 : sizeof(PbSmem<32, 3>) + 1024;
+}
+
+// The schedule of one batch on the device: descriptors, ring buffers, counters.
+struct PbPlan {
+  std::vector<PbQ> q;
+  std::vector<PbSlab> slab;
+  std::vector<PbSlot> slot;
+  std::vector<CUtensorMap> maps;
+  int64_t ngram = 0, nprep = 0;
+  size_t slot_bytes = 0, ctr_bytes = 0, seq_ints = 0;
+};
+
+// Bytes of the ring and the device descriptors for `nq` q points at slab sizes S_q.
+size_t pb_plan_bytes(int nq, const spx_q_desc* qd, const int* S, int nw, int nslot) {
+  size_t per_slot = 0, seq = 0;
+  int64_t nslab = 0;
+  for (int i = 0; i < nq; ++i) {
+    const int N = qd[i].nbas;
+    if (N <= 0 || qd[i].npair <= 0) continue;
+    const int nblk = (N + 63) / 64;
+    const int64_t R = (int64_t)((nblk + 1) / 2 * 2) * SP_ROWS;
+    size_t b = align_up((size_t)SP_SLOT * nw * R * S[i], 1024) + align_up(sizeof(double) * (size_t)nw * S[i], 256) +
+               align_up(sizeof(double) * (size_t)R, 256) + 2 * align_up(sizeof(double) * (size_t)nw, 256) +
+               (qd[i].cprod ? 0 : align_up(sizeof(double2) * (size_t)N * S[i], 256));
+    per_slot = std::max(per_slot, b);
+    seq += (size_t)pb_ntile<32>(N) * nw;   // the larger of the two tilings
+    nslab += (qd[i].npair + S[i] - 1) / S[i];
+  }
+  const size_t desc = align_up(sizeof(PbQ) * nq, 256) + align_up(sizeof(PbSlab) * nslab, 256) +
+                      align_up(sizeof(PbSlot) * nslot, 256) +
+                      align_up(sizeof(CUtensorMap) * 2 * (size_t)nq * nslot, 256);
+  const size_t ctr = align_up(sizeof(unsigned long long) * 2 + sizeof(int) * (3 * nslab + seq), 256);
+  return per_slot * nslot + desc + ctr + 4096;
+}
+
+// Builds the schedule into `mem` (device, pb_plan_bytes large): descriptors are
+// copied there synchronously; the counters (the first `*ctr_bytes` bytes at
+// *ctr) must be zeroed before every launch.
+int pb_build(spx_ctx* ctx, int nq, const spx_q_desc* qd, const int* S, int nw, int nslot,
+             PbConfig cfg, const double* omega, char* mem, size_t mem_bytes, PbParams* out,
+             void** ctr, size_t* ctr_bytes) {
+  (void)mem_bytes;
+  // q order: most work first
+  std::vector<int> order;
+  for (int i = 0; i < nq; ++i)
+    if (qd[i].nbas > 0 && qd[i].npair > 0) order.push_back(i);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return (double)qd[a].nbas * qd[a].nbas * (double)qd[a].npair >
+           (double)qd[b].nbas * qd[b].nbas * (double)qd[b].npair;
+  });
+  std::vector<PbQ> q(nq);
+  std::vector<PbSlab> slabs;
+  int64_t g0 = 0, r0 = 0;
+  size_t seq_total = 0;
+  std::vector<size_t> seq_off(nq, 0);
+  for (int i = 0; i < nq; ++i) {
+    const spx_q_desc& d = qd[i];
+    PbQ& x = q[i];
+    std::memset(&x, 0, sizeof(x));
+    x.N = d.nbas;
+    x.P = d.npair;
+    if (x.N <= 0 || x.P <= 0) continue;
+    x.nblk = (x.N + 63) / 64;
+    x.ntile = cfg.bn == 64 ? pb_ntile<64>(x.N) : pb_ntile<32>(x.N);
+    x.R = (int64_t)((x.nblk + 1) / 2 * 2) * SP_ROWS;
+    x.npad = (int)(x.R / 2);
+    x.S = S[i];
+    x.nslab = (int)((x.P + x.S - 1) / x.S);
+    x.npack = (int64_t)x.N * (x.N + 1) / 2;
+    x.M = reinterpret_cast<const double2*>(d.cprod);
+    x.ldc = d.ldc;
+    x.seed = d.seed;
+    x.sid = d.stream_id;
+    x.mscale = d.m_scale;
+    x.ediff = d.ediff;
+    x.wscale = d.wscale;
+    x.scale_all = d.scale_all;
+    x.out = d.susceph;
+    seq_off[i] = seq_total;
+    seq_total += (size_t)x.ntile * nw;
+  }
+  for (int i : order) {
+    const PbQ& x = q[i];
+    for (int s = 0; s < x.nslab; ++s) {
+      PbSlab sl;
+      std::memset(&sl, 0, sizeof(sl));
+      sl.q = i;
+      sl.s = s;
+      sl.slot = (int)(slabs.size() % nslot);
+      sl.p0 = (int64_t)s * x.S;
+      sl.len = (int)std::min<int64_t>(x.S, x.P - sl.p0);
+      sl.lenp = (int)align_up((size_t)sl.len, SP_KB);
+      sl.nk = sl.lenp / SP_KB;
+      sl.g0 = g0;
+      sl.r0 = r0;
+      sl.na = (x.N + PB_ACOLS - 1) / PB_ACOLS;
+      sl.nb = nw;
+      sl.nc = x.npad / PB_QCOLS;
+      sl.ngram = x.ntile * nw;
+      g0 += sl.ngram;
+      r0 += sl.na + sl.nb + sl.nc;
+      slabs.push_back(sl);
+    }
+  }
+  const int nslab = (int)slabs.size();
+  Carve cv{mem, mem_bytes};
+  // counters first (one memset per launch): heads, ab, ready, gdone, seq
+  char* c0 = cv.p;
+  unsigned long long* heads = cv.take<unsigned long long>(2);
+  int* ab = cv.take<int>(nslab);
+  int* ready = cv.take<int>(nslab);
+  int* gdone = cv.take<int>(nslab);
+  int* seq = cv.take<int>(seq_total);
+  *ctr = c0;
+  *ctr_bytes = (size_t)(cv.p - c0);
+  for (int i = 0; i < nq; ++i) q[i].seq = seq + seq_off[i];
+  PbQ* dq = cv.take<PbQ>(nq);
+  PbSlab* dsl = cv.take<PbSlab>(nslab);
+  PbSlot* dslot = cv.take<PbSlot>(nslot);
+  CUtensorMap* dmaps = reinterpret_cast<CUtensorMap*>(cv.take<char>(sizeof(CUtensorMap) * 2 * (size_t)nq * nslot));
+  // ring buffers sized for the largest q
+  size_t fb = 0, gb = 0, sb = 0, mb = 0;
+  for (int i = 0; i < nq; ++i) {
+    if (q[i].N <= 0) continue;
+    fb = std::max(fb, (size_t)SP_SLOT * nw * q[i].R * q[i].S);
+    gb = std::max(gb, (size_t)nw * q[i].S);
+    sb = std::max(sb, (size_t)q[i].R);
+    if (!q[i].M) mb = std::max(mb, (size_t)q[i].N * q[i].S);
+  }
+  std::vector<PbSlot> slot(nslot);
+  for (int b = 0; b < nslot; ++b) {
+    slot[b].F = reinterpret_cast<int8_t*>(cv.take<char>(fb));
+    slot[b].G = cv.take<double>(gb);
+    slot[b].sA = cv.take<double>(sb);
+    slot[b].wmax = cv.take<double>(nw);
+    slot[b].wsgn = cv.take<int>(nw);
+    slot[b].Mbuf = mb ? cv.take<double2>(mb) : nullptr;
+  }
+  if (!cv.ok) return set_error(ctx, SPX_ENOMEM, "persistent batch: scratch too small");
+  // tensor maps per (q, slot): planes [6 nw][nkb][R][64 B]
+  std::vector<CUtensorMap> maps(2 * (size_t)nq * nslot);
+  for (int i = 0; i < nq; ++i) {
+    if (q[i].N <= 0) continue;
+    const uint64_t nkb = (uint64_t)(q[i].S / SP_KB);
+    const uint64_t st[3] = {SP_KB, (uint64_t)q[i].R * SP_KB, nkb * q[i].R * SP_KB};
+    const uint64_t dims[4] = {SP_KB, (uint64_t)q[i].R, nkb, (uint64_t)SP_SLOT * nw};
+    const uint32_t ba[4] = {SP_KB, SP_ROWS, 1, SP_SF};
+    const uint32_t bb[4] = {SP_KB, (uint32_t)(2 * cfg.bn), 1, SP_SF};
+    for (int b = 0; b < nslot; ++b) {
+      int rc = make_tmap_u8_4d(ctx, &maps[2 * ((size_t)i * nslot + b)], slot[b].F, dims, st, ba,
+                               CU_TENSOR_MAP_SWIZZLE_64B);
+      if (!rc)
+        rc = make_tmap_u8_4d(ctx, &maps[2 * ((size_t)i * nslot + b) + 1], slot[b].F, dims, st, bb,
+                             CU_TENSOR_MAP_SWIZZLE_64B);
+      if (rc) return rc;
+    }
+  }
+  int rc;
+  if ((rc = check_cuda(ctx, cudaMemcpy(dq, q.data(), sizeof(PbQ) * nq, cudaMemcpyHostToDevice), "plan copy")) ||
+      (rc = check_cuda(ctx, cudaMemcpy(dsl, slabs.data(), sizeof(PbSlab) * nslab, cudaMemcpyHostToDevice), "plan copy")) ||
+      (rc = check_cuda(ctx, cudaMemcpy(dslot, slot.data(), sizeof(PbSlot) * nslot, cudaMemcpyHostToDevice), "plan copy")) ||
+      (rc = check_cuda(ctx, cudaMemcpy(dmaps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice), "plan copy")))
+    return rc;
+  PbParams& p = *out;
+  std::memset(&p, 0, sizeof(p));
+  p.q = dq;
+  p.slab = dsl;
+  p.slot = dslot;
+  p.maps = dmaps;
+  p.nslab = nslab;
+  p.nslot = nslot;
+  p.nw = nw;
+  p.ngram = g0;
+  p.nprep = r0;
+  p.omega = omega;
+  p.heads = heads;
+  p.ab = ab;
+  p.ready = ready;
+  p.gdone = gdone;
+  p.status = ctx->d_status;
+  p.timeout_ns = (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
+  return SPX_OK;
+}
+
+// Enqueues one launch of the schedule on `s` (the counters are zeroed first).
+int pb_launch(spx_ctx* ctx, const PbParams& prm, PbConfig cfg, void* ctr, size_t ctr_bytes,
+              cudaStream_t s) {
+  int rc = check_cuda(ctx, cudaMemsetAsync(ctr, 0, ctr_bytes, s), "counters");
+  if (rc) return rc;
+  const size_t smem = pb_smem(cfg);
+  const int grid = ctx->num_sms;
+  if (cfg.bn == 64) {
+    cudaFuncSetAttribute(pb_kernel<64, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    pb_kernel<64, 3><<<grid, PB_THREADS, smem, s>>>(prm);
+  } else if (cfg.stages == 4) {
+    cudaFuncSetAttribute(pb_kernel<32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    pb_kernel<32, 4><<<grid, PB_THREADS, smem, s>>>(prm);
+  } else {
+    cudaFuncSetAttribute(pb_kernel<32, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    pb_kernel<32, 3><<<grid, PB_THREADS, smem, s>>>(prm);
+  }
+  return check_cuda(ctx, cudaGetLastError(), "persistent batch launch");
+}
+
+constexpr int PB_NSLOT = 3;
+constexpr int PB_DEFAULT_SLAB = 16384;
+constexpr PbConfig PB_DEFAULT_CFG = {64, 3};
+constexpr size_t PB_MAX_GRAPHS = 8;
+
+static int pb_nbas_bucket(int N) { return (N + 127) / 128; }
+static int pb_npair_bucket(int64_t P) { return P <= 16384 ? 0 : (P <= 32768 ? 1 : 2); }
+
+static const spx_tune_entry* pb_find_tune(const spx_ctx* ctx, int N, int64_t P, int nw) {
+  for (const auto& e : ctx->tune)
+    if (e.variant == 3 && e.nbas_bucket == pb_nbas_bucket(N) && e.npair_bucket == pb_npair_bucket(P) &&
+        e.nw == nw)
+      return &e;
+  return nullptr;
+}
+
+static PbConfig pb_cfg_of(int tile) {
+  const int bn = tile & 255, st = tile >> 8;
+  if (bn == 32 && (st == 3 || st == 4)) return {32, st};
+  return PB_DEFAULT_CFG;
+}
+
+static uint64_t pb_fnv(uint64_t h, const void* p, size_t n) {
+  const unsigned char* b = (const unsigned char*)p;
+  for (size_t i = 0; i < n; ++i) {
+    h ^= b[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+// One persistent launch for the whole batch (split precision). Slab sizes: the
+// descriptor's, else the tuned, else 16384; tile shape: the tuned shape of the q
+// with most work, else 64 x 64 with 3 stages (`force` overrides both when set).
+int pb_run(spx_ctx* ctx, int nq, const spx_q_desc* q, int nw, const double* omega, int flags,
+           cudaStream_t s, int* launches, const PbConfig* force, int force_slab) {
+  std::vector<int> S(nq, PB_DEFAULT_SLAB);
+  PbConfig cfg = PB_DEFAULT_CFG;
+  double most = -1;
+  for (int i = 0; i < nq; ++i) {
+    if (q[i].nbas <= 0 || q[i].npair <= 0) continue;
+    const spx_tune_entry* t = pb_find_tune(ctx, q[i].nbas, q[i].npair, nw);
+    int sl = q[i].slab_pairs > 0 ? q[i].slab_pairs : (t ? t->slab_pairs : PB_DEFAULT_SLAB);
+    if (force_slab > 0) sl = force_slab;
+    S[i] = std::max(SP_KB, std::min(SP_SLAB, sl / SP_KB * SP_KB));
+    const double work = (double)q[i].nbas * q[i].nbas * (double)q[i].npair;
+    if (work > most) {
+      most = work;
+      cfg = t ? pb_cfg_of(t->tile) : PB_DEFAULT_CFG;
+    }
+  }
+  if (force) cfg = *force;
+  const size_t bytes = pb_plan_bytes(nq, q, S.data(), nw, PB_NSLOT);
+  PbParams prm;
+  void* ctr = nullptr;
+  size_t ctr_bytes = 0;
+  int rc;
+  if (flags & SPX_BATCH_NOGRAPH) {
+    if ((rc = ensure_workspace(ctx, bytes))) return rc;
+    if ((rc = pb_build(ctx, nq, q, S.data(), nw, PB_NSLOT, cfg, omega, (char*)ctx->ws, ctx->ws_bytes,
+                       &prm, &ctr, &ctr_bytes)))
+      return rc;
+    if ((rc = pb_launch(ctx, prm, cfg, ctr, ctr_bytes, s))) return rc;
+    *launches = 1;
+    return SPX_OK;
+  }
+  uint64_t key = 0x9e3779b97f4a7c15ull;
+  key = pb_fnv(key, "persistent", 10);
+  key = pb_fnv(key, &nq, sizeof(nq));
+  key = pb_fnv(key, q, sizeof(spx_q_desc) * nq);
+  key = pb_fnv(key, S.data(), sizeof(int) * nq);
+  key = pb_fnv(key, &cfg, sizeof(cfg));
+  key = pb_fnv(key, &nw, sizeof(nw));
+  key = pb_fnv(key, &omega, sizeof(omega));
+  spx_ctx::BatchGraph* hit = nullptr;
+  for (auto& g : ctx->graphs)
+    if (g.key == key) hit = &g;
+  if (!hit) {
+    void* mem = nullptr;
+    if (cudaMalloc(&mem, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(ctx, SPX_ENOMEM, "persistent batch: cannot allocate " + std::to_string(bytes) + " bytes");
+    }
+    rc = pb_build(ctx, nq, q, S.data(), nw, PB_NSLOT, cfg, omega, (char*)mem, bytes, &prm, &ctr, &ctr_bytes);
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if (!rc) rc = check_cuda(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed), "begin capture");
+    if (!rc) {
+      rc = pb_launch(ctx, prm, cfg, ctr, ctr_bytes, ctx->stream);
+      cudaError_t ee = cudaStreamEndCapture(ctx->stream, &graph);
+      if (!rc) rc = check_cuda(ctx, ee, "end capture");
+      if (!rc) rc = check_cuda(ctx, cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+    }
+    if (rc) {
+      cudaGetLastError();
+      if (graph) cudaGraphDestroy(graph);
+      cudaFree(mem);
+      return rc;
+    }
+    if (ctx->graphs.size() >= PB_MAX_GRAPHS) {
+      auto old = std::min_element(ctx->graphs.begin(), ctx->graphs.end(),
+                                  [](const spx_ctx::BatchGraph& a, const spx_ctx::BatchGraph& b) {
+                                    return a.last_use < b.last_use;
+                                  });
+      cudaGraphExecDestroy(old->exec);
+      cudaGraphDestroy(old->graph);
+      if (old->mem) cudaFree(old->mem);
+      ctx->graphs.erase(old);
+    }
+    ctx->graphs.push_back({key, graph, exec, 0, mem});
+    hit = &ctx->graphs.back();
+  }
+  hit->last_use = ++ctx->graph_clock;
+  *launches = 1;
+  return check_cuda(ctx, cudaGraphLaunch(hit->exec, s), "graph launch");
+}
+
+}  // namespace spx
+
+using namespace spx;
+
+namespace spx {
+int launch_gen_normal(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, double, double*, cudaStream_t);
+}
+
+// Times the persistent schedule's tile shapes and slab sizes on a seeded probe of one
+// q (M generated on the device), keeps the fastest as a variant-3 entry.
+extern "C" int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
+                                    spx_tune_entry* out) {
+  if (!ctx) return SPX_EINVAL;
+  if (nbas <= 0 || npair <= 0 || nw <= 0) return set_error(ctx, SPX_EINVAL, "empty probe");
+  if (nbas > 46340) return set_error(ctx, SPX_EINVAL, "nbas too large");
+  cudaSetDevice(ctx->device);
+  const int slabs[2] = {16384, 32768};
+  const PbConfig cfgs[3] = {{64, 3}, {32, 3}, {32, 4}};
+  const int64_t P = std::min<int64_t>(npair, 4 * (int64_t)SP_SLAB);
+  const int64_t npack = (int64_t)nbas * (nbas + 1) / 2;
+  // probe arrays in a private allocation (the schedule itself uses the workspace)
+  const size_t e_bytes = align_up(sizeof(double) * (size_t)P, 256);
+  const size_t o_bytes = align_up(sizeof(double2) * (size_t)npack * nw, 256);
+  const size_t om_bytes = align_up(sizeof(double) * (size_t)nw, 256);
+  char* buf = nullptr;
+  if (cudaMalloc(&buf, e_bytes + o_bytes + om_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(ctx, SPX_ENOMEM, "autotune probe");
+  }
+  double* E = (double*)buf;
+  double* O = (double*)(buf + e_bytes);
+  double* OM = (double*)(buf + e_bytes + o_bytes);
+  cudaStream_t s = ctx->stream;
+  std::vector<double> om(nw);
+  for (int f = 0; f < nw; ++f) om[f] = 1.0 + f;
+  int rc = launch_gen_normal(ctx, 0x5eed, 78, 0, P, 3.0, E, s);
+  if (!rc) rc = check_cuda(ctx, cudaMemcpyAsync(OM, om.data(), sizeof(double) * nw, cudaMemcpyHostToDevice, s), "probe");
+  if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(s), "probe");
+  spx_tune_entry best{};
+  best.nbas_bucket = pb_nbas_bucket(nbas);
+  best.npair_bucket = pb_npair_bucket(npair);
+  best.nw = nw;
+  best.variant = 3;
+  best.tflops = -1;
+  spx_q_desc d;
+  std::memset(&d, 0, sizeof(d));
+  d.nbas = nbas;
+  d.npair = P;
+  d.seed = 0x5eed;
+  d.stream_id = 77;
+  d.m_scale = 1.0 / std::sqrt((double)nbas);
+  d.ediff = E;
+  d.scale_all = 1.0;
+  d.susceph = O;
+  const double flops = 8.0 * (double)nbas * nbas * (double)P * nw;
+  cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+  for (int ci = 0; ci < 3 && !rc; ++ci)
+    for (int sl : slabs) {
+      if (sl == 32768 && P <= 16384) continue;
+      float best_ms = 1e30f;
+      for (int rep = 0; rep < 2 && !rc; ++rep) {
+        int launches = 0;
+        cudaEventRecord(e0, s);
+        rc = pb_run(ctx, 1, &d, nw, OM, SPX_BATCH_NOGRAPH, s, &launches, &cfgs[ci], sl);
+        if (rc) break;
+        cudaEventRecord(e1, s);
+        if ((rc = collect_status(ctx, s, "batched autotune"))) break;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep) best_ms = std::min(best_ms, ms);
+      }
+      if (rc) break;
+      const double tf = flops / (best_ms * 1e-3) / 1e12;
+      if (tf > best.tflops) {
+        best.tflops = tf;
+        best.slab_pairs = sl;
+        best.tile = cfgs[ci].bn + 256 * cfgs[ci].stages;
+      }
+    }
+  cudaFree(buf);
+  if (rc) return rc;
+  bool stored = false;
+  for (auto& e : ctx->tune)
+    if (e.variant == 3 && e.nbas_bucket == best.nbas_bucket && e.npair_bucket == best.npair_bucket &&
+        e.nw == nw) {
+      e = best;
+      stored = true;
+    }
+  if (!stored) ctx->tune.push_back(best);
+  if (out) *out = best;
+  return SPX_OK;
+}
+
+extern "C" int spx_tune_lookup_batched(const spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
+                                       spx_tune_entry* out) {
+  if (!ctx) return SPX_EINVAL;
+  const spx_tune_entry* t = pb_find_tune(ctx, nbas, npair, nw);
+  if (!t) return SPX_ENOTSUP;
+  if (out) *out = *t;
+  return SPX_OK;
+}

@@ -12,33 +12,32 @@
 // Layout and pipeline:
 //   * one work item = (frequency, upper tile); persistent CTAs stride over items;
 //   * warp 0 streams 16-pair slabs of the two 64-column panels of M
-//     (p-contiguous columns, exactly the Fortran cprod layout) into shared
-//     memory with 1-D bulk TMA copies, one per column, plus the 16 weights,
-//     one stage ahead of the math; each warp releases a stage on an mbarrier
-//     when it is done with it, and only warp 0 waits for that before refilling;
+//     (p-contiguous columns, exactly the Fortran cprod layout) into shared memory
+//     with 2-D TMA boxes of 8 pairs x 64 columns (128-byte rows, SWIZZLE_128B, so
+//     fragment loads of eight rows hit eight different bank groups), three stages
+//     ahead (five copy instructions per stage); pairs and columns past the slab's
+//     end arrive as zeros, and a diagonal tile loads its one panel once;
 //   * four warps each own a 32x32 complex sub-tile and run
-//     mma.sync m16n8kKI f64 on re/im planes: re += ar*(w br) + ai*(w bi),
-//     im += ai*(w br) - ar*(w bi);
-//   * shared rows are padded to 20 complex (320 B) so the 16-byte fragment
-//     loads of a quarter-warp hit eight distinct bank groups;
+//     mma.sync m16n8k8 f64 on re/im parts: re += ar*(w br) + ai*(w bi),
+//     im += ai*(w br) - ar*(w bi); each warp releases a stage on an mbarrier;
 //   * the epilogue adds the tile into the packed upper triangle
 //     susceph(j*(j+1)/2 + i, f) (src/susceptibility.f:1210).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "spx_common.cuh"
+#include "spx_tcgen05.cuh"
 
 namespace spx {
 
 constexpr int F64_B = 64;                 // tile edge in complex rows / columns
 constexpr int F64_KC = 16;                // band pairs per pipeline stage
-constexpr int F64_ROW = F64_KC + 4;       // padded shared row, double2 units
-constexpr int F64_ST = 2;                 // pipeline stages
+constexpr int F64_KBOX = 8;               // pairs per TMA box: one 128-byte swizzled row
+constexpr int F64_ST = 3;                 // pipeline stages
 constexpr int F64_WARPS = 4;              // each owns a 32x32 complex sub-tile
 constexpr int F64_THREADS = 32 * F64_WARPS;
 
 struct F64Params {
-  const double2* M;
-  int64_t ldc;
   int64_t P;
   int N;
   const double* W;
@@ -52,12 +51,15 @@ struct F64Params {
   uint64_t timeout_ns;
 };
 
-struct __align__(16) F64Smem {
-  double2 a[F64_ST][F64_B][F64_ROW];
-  double2 b[F64_ST][F64_B][F64_ROW];
+// one panel half: 64 columns x 8 pairs, row r's 16-byte chunk c stored at c ^ (r & 7)
+typedef double2 F64Box[F64_B][F64_KBOX];
+
+struct __align__(1024) F64Smem {
+  F64Box a[F64_ST][2];
+  F64Box b[F64_ST][2];
   double w[F64_ST][F64_KC];
   uint64_t full[F64_ST];
-  uint64_t empty[F64_ST];  // every warp has finished with the stage
+  uint64_t empty[F64_ST];  // every compute warp has finished with the stage
 };
 
 // Upper-triangle tile t -> (bi, bj), bi <= bj, column-major over the triangle.
@@ -67,6 +69,15 @@ __device__ __forceinline__ void decode_tile(int t, int* bi, int* bj) {
   while ((j + 1) * (j + 2) / 2 <= t) ++j;
   *bj = j;
   *bi = t - j * (j + 1) / 2;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
 }
 
 // D(16x8) += A(16xKI) * B(KIx8), f64. Fragment order: a[2q+h] = A(g+8h, t+4q),
@@ -100,36 +111,12 @@ __device__ __forceinline__ void dmma<16>(double (&d)[4], const double* a, const 
         "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
-// Issues the bulk copies of chunk `c` (item, p0) into stage `st`: one copy per
-// panel column plus the weights. Called by all lanes of warp 0.
-__device__ __forceinline__ void f64_issue(F64Smem& sm, const F64Params& prm, int st,
-                                          int64_t item, int64_t p0, int lane) {
-  const int f = (int)(item / prm.ntile);
-  int bi, bj;
-  decode_tile((int)(item % prm.ntile), &bi, &bj);
-  const int i0 = bi * F64_B, j0 = bj * F64_B;
-  const int ni = min(F64_B, prm.N - i0), nj = min(F64_B, prm.N - j0);
-  const int len = (int)min((int64_t)F64_KC, prm.P - p0);
-  const int wlen = (len + 1) & ~1;
-  if (lane == 0) mbar_arrive_expect_tx(&sm.full[st], (uint32_t)((ni + nj) * len * 16 + wlen * 8));
-  __syncwarp();
-  for (int c = lane; c < ni; c += 32)
-    bulk_g2s(&sm.a[st][c][0], prm.M + (int64_t)(i0 + c) * prm.ldc + p0, len * 16, &sm.full[st]);
-  for (int c = lane; c < nj; c += 32)
-    bulk_g2s(&sm.b[st][c][0], prm.M + (int64_t)(j0 + c) * prm.ldc + p0, len * 16, &sm.full[st]);
-  if (lane == 0)
-    bulk_g2s(&sm.w[st][0], prm.W + (int64_t)f * prm.ldw + p0, wlen * 8, &sm.full[st]);
-}
-
-template <int KI>
-__global__ void __launch_bounds__(F64_THREADS, 2) chi0_fp64_kernel(F64Params prm) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  F64Smem& sm = *reinterpret_cast<F64Smem*>(smem_raw);
+__global__ void __launch_bounds__(F64_THREADS, 2)
+    chi0_fp64_kernel(const __grid_constant__ CUtensorMap mapM, F64Params prm) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  F64Smem& sm = *reinterpret_cast<F64Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                            ~(uintptr_t)1023);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-  // zero the stages once so that masked lanes never read uninitialised bits
-  for (int t = threadIdx.x; t < 2 * F64_ST * F64_B * F64_ROW; t += blockDim.x)
-    reinterpret_cast<double2*>(smem_raw)[t] = make_double2(0.0, 0.0);
   if (threadIdx.x == 0) {
     for (int s = 0; s < F64_ST; ++s) {
       mbar_init(&sm.full[s], 1);
@@ -148,22 +135,42 @@ __global__ void __launch_bounds__(F64_THREADS, 2) chi0_fp64_kernel(F64Params prm
   const int64_t total = my_items * nchunk;
   auto chunk_item = [&](int64_t c) { return blockIdx.x + (c / nchunk) * (int64_t)gridDim.x; };
   auto chunk_p0 = [&](int64_t c) { return (c % nchunk) * (int64_t)F64_KC; };
-  // chunks [0, issued) have their copies issued (tracked by warp 0)
-  int64_t issued = total < F64_ST - 1 ? total : (int64_t)(F64_ST - 1);
-  if (warp == 0)
-    for (int64_t c = 0; c < issued; ++c)
-      f64_issue(sm, prm, (int)(c % F64_ST), chunk_item(c), chunk_p0(c), lane);
 
+  // chunk c's copies (one thread): 2 or 4 boxes of M and the 16 weights
+  auto issue = [&](int64_t c) {
+    const int st = (int)(c % F64_ST);
+    const int64_t item = chunk_item(c), p0 = chunk_p0(c);
+    const int f = (int)(item / prm.ntile);
+    int bi, bj;
+    decode_tile((int)(item % prm.ntile), &bi, &bj);
+    const bool same = bi == bj;
+    mbar_arrive_expect_tx(&sm.full[st], (uint32_t)((same ? 2 : 4) * sizeof(F64Box) + F64_KC * 8));
+    const int x = (int)(2 * p0);
+    tma_load_2d(&sm.a[st][0][0][0], &mapM, x, bi * F64_B, &sm.full[st]);
+    tma_load_2d(&sm.a[st][1][0][0], &mapM, x + 2 * F64_KBOX, bi * F64_B, &sm.full[st]);
+    if (!same) {
+      tma_load_2d(&sm.b[st][0][0][0], &mapM, x, bj * F64_B, &sm.full[st]);
+      tma_load_2d(&sm.b[st][1][0][0], &mapM, x + 2 * F64_KBOX, bj * F64_B, &sm.full[st]);
+    }
+    bulk_g2s(&sm.w[st][0], prm.W + (int64_t)f * prm.ldw + p0, F64_KC * 8, &sm.full[st]);
+  };
+  // chunks [0, issued) have their copies issued (tracked by warp 0, lane 0)
+  int64_t issued = total < F64_ST - 1 ? total : (int64_t)(F64_ST - 1);
+  if (warp == 0 && lane == 0)
+    for (int64_t c = 0; c < issued; ++c) issue(c);
+
+  // ---------------- compute warps ----------------
   const int wi = warp & 1, wj = warp >> 1;
   const int g = lane >> 2, t = lane & 3;
-  constexpr int NQ = KI / 4;
   double accR[2][4][4], accI[2][4][4];
   bool failed = false;
   int64_t c = 0;
   for (; c < total; ++c) {
     const int st = (int)(c % F64_ST);
     const uint32_t ph = (uint32_t)((c / F64_ST) & 1);
-    const int64_t p0 = chunk_p0(c);
+    const int64_t item = chunk_item(c), p0 = chunk_p0(c);
+    int bi, bj;
+    decode_tile((int)(item % prm.ntile), &bi, &bj);
     if (p0 == 0) {
 #pragma unroll
       for (int mt = 0; mt < 2; ++mt)
@@ -177,80 +184,74 @@ __global__ void __launch_bounds__(F64_THREADS, 2) chi0_fp64_kernel(F64Params prm
     if (warp == 0 && c + F64_ST - 1 < total) {
       const int64_t prev = c - 1;
       int ok = 1;
-      if (prev >= 0 && lane == 0)
-        ok = mbar_wait(&sm.empty[(int)(prev % F64_ST)], (uint32_t)((prev / F64_ST) & 1),
-                       prm.timeout_ns, prm.status);
+      if (lane == 0) {
+        if (prev >= 0)
+          ok = mbar_wait(&sm.empty[(int)(prev % F64_ST)], (uint32_t)((prev / F64_ST) & 1),
+                         prm.timeout_ns, prm.status);
+        if (ok) issue(c + F64_ST - 1);
+      }
       if (!__shfl_sync(0xffffffffu, ok, 0)) {
         failed = true;
         break;
       }
-      f64_issue(sm, prm, (int)((c + F64_ST - 1) % F64_ST), chunk_item(c + F64_ST - 1),
-                chunk_p0(c + F64_ST - 1), lane);
       issued = c + F64_ST;
     }
     if (!mbar_wait(&sm.full[st], ph, prm.timeout_ns, prm.status)) {
       failed = true;
       break;
     }
-    const int len = (int)min((int64_t)F64_KC, prm.P - p0);
+    const F64Box* Ab = sm.a[st];
+    const F64Box* Bb = bi == bj ? sm.a[st] : sm.b[st];
 #pragma unroll
-    for (int ks = 0; ks < F64_KC / KI; ++ks) {
-      double wq[NQ];
-      bool valid[NQ];
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        const int p = ks * KI + t + 4 * q;
-        valid[q] = p < len;
-        wq[q] = valid[q] ? sm.w[st][p] : 0.0;
-      }
-      // one 16-row slice of A at a time keeps the live set small; B slices are
-      // re-read from shared memory for the second slice
+    for (int ks = 0; ks < F64_KC / F64_KBOX; ++ks) {
+      const double w0 = sm.w[st][ks * F64_KBOX + t], w1 = sm.w[st][ks * F64_KBOX + t + 4];
+      // one 16-row slice of A at a time keeps the live set small
 #pragma unroll
       for (int mt = 0; mt < 2; ++mt) {
-        double ar[2 * NQ], ai[2 * NQ];
+        double ar[4], ai[4];
 #pragma unroll
-        for (int q = 0; q < NQ; ++q)
+        for (int q = 0; q < 2; ++q)
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            const double2 v = sm.a[st][32 * wi + 16 * mt + g + 8 * h][ks * KI + t + 4 * q];
-            ar[2 * q + h] = valid[q] ? v.x : 0.0;
-            ai[2 * q + h] = valid[q] ? v.y : 0.0;
+            const int r = 32 * wi + 16 * mt + g + 8 * h;
+            const double2 v = Ab[ks][r][(t + 4 * q) ^ (r & 7)];
+            ar[2 * q + h] = v.x;
+            ai[2 * q + h] = v.y;
           }
         // two column slices at a time: the two MMAs that share an accumulator are
         // three independent MMAs apart, hiding the DMMA latency
 #pragma unroll
         for (int np = 0; np < 2; ++np) {
-          double br[2][NQ], bim[2][NQ], bneg[2][NQ];
+          double br[2][2], bim[2][2], bneg[2][2];
 #pragma unroll
           for (int h = 0; h < 2; ++h)
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-              const double2 v = sm.b[st][32 * wj + 8 * (2 * np + h) + g][ks * KI + t + 4 * q];
-              br[h][q] = wq[q] * v.x;
-              bim[h][q] = wq[q] * v.y;
+            for (int q = 0; q < 2; ++q) {
+              const int r = 32 * wj + 8 * (2 * np + h) + g;
+              const double2 v = Bb[ks][r][(t + 4 * q) ^ (r & 7)];
+              const double wq = q ? w1 : w0;
+              br[h][q] = wq * v.x;
+              bim[h][q] = wq * v.y;
               bneg[h][q] = -bim[h][q];
             }
-          dmma<KI>(accR[mt][2 * np], ar, br[0]);
-          dmma<KI>(accR[mt][2 * np + 1], ar, br[1]);
-          dmma<KI>(accI[mt][2 * np], ai, br[0]);
-          dmma<KI>(accI[mt][2 * np + 1], ai, br[1]);
-          dmma<KI>(accR[mt][2 * np], ai, bim[0]);
-          dmma<KI>(accR[mt][2 * np + 1], ai, bim[1]);
-          dmma<KI>(accI[mt][2 * np], ar, bneg[0]);
-          dmma<KI>(accI[mt][2 * np + 1], ar, bneg[1]);
+          dmma<8>(accR[mt][2 * np], ar, br[0]);
+          dmma<8>(accR[mt][2 * np + 1], ar, br[1]);
+          dmma<8>(accI[mt][2 * np], ai, br[0]);
+          dmma<8>(accI[mt][2 * np + 1], ai, br[1]);
+          dmma<8>(accR[mt][2 * np], ai, bim[0]);
+          dmma<8>(accR[mt][2 * np + 1], ai, bim[1]);
+          dmma<8>(accI[mt][2 * np], ar, bneg[0]);
+          dmma<8>(accI[mt][2 * np + 1], ar, bneg[1]);
         }
       }
     }
-    // this warp is done with stage st; only the issuing warp waits for all four
+    // this warp is done with stage st
     __syncwarp();
     if (lane == 0) mbar_arrive(&sm.empty[st]);
 
     if (p0 + F64_KC >= prm.P) {
       // last slab of this item: add the tile into the packed upper triangle
-      const int64_t item = chunk_item(c);
       const int f = (int)(item / prm.ntile);
-      int bi, bj;
-      decode_tile((int)(item % prm.ntile), &bi, &bj);
       double2* outf = prm.out + (int64_t)f * prm.npack;
 #pragma unroll
       for (int mt = 0; mt < 2; ++mt)
@@ -270,23 +271,28 @@ __global__ void __launch_bounds__(F64_THREADS, 2) chi0_fp64_kernel(F64Params prm
           }
     }
   }
-  if (failed && warp == 0) {
-    // never leave with bulk copies still landing in this CTA's shared memory
+  if (failed && warp == 0 && lane == 0) {
+    // never leave with copies still landing in this CTA's shared memory
     for (int64_t k = c; k < issued; ++k)
       mbar_drain(&sm.full[(int)(k % F64_ST)], (uint32_t)((k / F64_ST) & 1), prm.timeout_ns);
   }
 }
 
-// Enqueues K1 over one slab of band pairs. W holds the weights of exactly these
-// pairs (leading dimension ldw, padding zeroed).
-int launch_chi0_fp64(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N,
-                     const double* W, int64_t ldw, int nw, double2* out, cudaStream_t stream,
-                     int ki) {
-  if (P <= 0 || N <= 0 || nw <= 0) return SPX_OK;
+// Tensor map of M as a 2-D FP64 array: pairs (re, im interleaved) contiguous,
+// columns ldc complex apart; boxes of 8 pairs x 64 columns, SWIZZLE_128B.
+static int f64_map(CUtensorMap* map, const double2* M, int64_t ldc, int64_t P, int N) {
+  const uint64_t dims[2] = {(uint64_t)(2 * P), (uint64_t)N};
+  const uint64_t strides[1] = {(uint64_t)ldc * 16};
+  const uint32_t box[2] = {2 * F64_KBOX, F64_B};
+  return encode_tmap(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, M, dims, strides, box,
+                     CU_TENSOR_MAP_SWIZZLE_128B);
+}
+
+static int f64_launch(int num_sms, const double2* M, int64_t ldc, int64_t P, int N, const double* W,
+                      int64_t ldw, int nw, double2* out, int* status, uint64_t timeout_ns,
+                      cudaStream_t stream) {
   const int nblk = (N + F64_B - 1) / F64_B;
   F64Params prm;
-  prm.M = M;
-  prm.ldc = ldc;
   prm.P = P;
   prm.N = N;
   prm.W = W;
@@ -296,30 +302,33 @@ int launch_chi0_fp64(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int
   prm.npack = (int64_t)N * (N + 1) / 2;
   prm.ntile = nblk * (nblk + 1) / 2;
   prm.nitems = (int64_t)prm.ntile * nw;
-  prm.status = ctx->d_status;
-  prm.timeout_ns = (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
-  const size_t smem = sizeof(F64Smem);
-  int grid = (int)std::min<int64_t>(prm.nitems, (int64_t)2 * ctx->num_sms);
-  cudaError_t e;
-  switch (ki) {
-    case 4:
-      cudaFuncSetAttribute(chi0_fp64_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-      chi0_fp64_kernel<4><<<grid, F64_THREADS, smem, stream>>>(prm);
-      break;
-    case 16:
-      cudaFuncSetAttribute(chi0_fp64_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-      chi0_fp64_kernel<16><<<grid, F64_THREADS, smem, stream>>>(prm);
-      break;
-    default:
-      cudaFuncSetAttribute(chi0_fp64_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-      chi0_fp64_kernel<8><<<grid, F64_THREADS, smem, stream>>>(prm);
-      break;
-  }
-  e = cudaGetLastError();
-  return check_cuda(ctx, e, "chi0_fp64_kernel launch");
+  prm.status = status;
+  prm.timeout_ns = timeout_ns;
+  CUtensorMap map;
+  const int e = f64_map(&map, M, ldc, P, N);
+  if (e) return e;
+  const size_t smem = sizeof(F64Smem) + 1024;
+  if (cudaFuncSetAttribute(chi0_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return -2;
+  const int grid = (int)std::min<int64_t>(prm.nitems, (int64_t)2 * num_sms);
+  chi0_fp64_kernel<<<grid, F64_THREADS, smem, stream>>>(map, prm);
+  return 0;
+}
+
+// Enqueues K1 over one slab of band pairs. W holds the weights of exactly these
+// pairs (leading dimension ldw, a multiple of 16, padding zeroed).
+int launch_chi0_fp64(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N,
+                     const double* W, int64_t ldw, int nw, double2* out, cudaStream_t stream,
+                     int ki) {
+  (void)ki;
+  if (P <= 0 || N <= 0 || nw <= 0) return SPX_OK;
+  const uint64_t timeout_ns =
+      (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
+  const int e = f64_launch(ctx->num_sms, M, ldc, P, N, W, ldw, nw, out, ctx->d_status, timeout_ns, stream);
+  if (e) return set_error(ctx, SPX_ECUDA, "chi0_fp64_kernel: tensor map or attribute failed (" +
+                                              std::to_string(e) + ")");
+  return check_cuda(ctx, cudaGetLastError(), "chi0_fp64_kernel launch");
 }
 
 }  // namespace spx
@@ -333,28 +342,69 @@ int launch_chi0_fp64_noctx(int num_sms, int* status, uint64_t timeout_ns, const 
                            int64_t ldc, int64_t P, int N, const double* W, int64_t ldw, int nw,
                            double2* out, cudaStream_t stream) {
   if (P <= 0 || N <= 0 || nw <= 0) return SPX_OK;
-  const int nblk = (N + F64_B - 1) / F64_B;
-  F64Params prm;
-  prm.M = M;
-  prm.ldc = ldc;
-  prm.P = P;
-  prm.N = N;
-  prm.W = W;
-  prm.ldw = ldw;
-  prm.nw = nw;
-  prm.out = out;
-  prm.npack = (int64_t)N * (N + 1) / 2;
-  prm.ntile = nblk * (nblk + 1) / 2;
-  prm.nitems = (int64_t)prm.ntile * nw;
-  prm.status = status;
-  prm.timeout_ns = timeout_ns;
-  const size_t smem = sizeof(F64Smem);
-  if (cudaFuncSetAttribute(chi0_fp64_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
-    return SPX_ECUDA;
-  const int grid = (int)std::min<int64_t>(prm.nitems, (int64_t)2 * num_sms);
-  chi0_fp64_kernel<8><<<grid, F64_THREADS, smem, stream>>>(prm);
+  if (f64_launch(num_sms, M, ldc, P, N, W, ldw, nw, out, status, timeout_ns, stream)) return SPX_ECUDA;
   return cudaGetLastError() == cudaSuccess ? SPX_OK : SPX_ECUDA;
 }
 
 }  // namespace spx
+
+namespace spx {
+
+// FP64 tensor-pipe peak: every warp issues back-to-back m16n8k8 DMMAs on register
+// operands into eight independent accumulators (no memory traffic in the loop),
+// so the rate is the DMMA pipe's own. The sums go to `sink` so nothing is elided.
+__global__ void __launch_bounds__(128) dmma_peak_kernel(int iters, double* sink) {
+  const int lane = threadIdx.x & 31;
+  double a[4], b[2];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) a[k] = 1.0 + 1e-3 * (lane + k);
+  b[0] = 0.5 - 1e-3 * lane;
+  b[1] = 0.25 + 1e-3 * lane;
+  double d[8][4];
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) d[k][r] = 0.0;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) dmma<8>(d[k], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) s += d[k][r];
+  sink[blockIdx.x * (int64_t)blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace spx
+
+// Measured FP64 tensor (DMMA) peak of the context's device in TFLOP/s (2 flops
+// per MAC), timed with CUDA events on the context stream: one warm-up launch, then
+// one launch of 4 CTAs x 4 warps per SM. No counterpart in the reference.
+extern "C" int spx_measure_dmma_peak(spx_ctx* ctx, double* tflops) {
+  if (!ctx || !tflops) return SPX_EINVAL;
+  cudaSetDevice(ctx->device);
+  const int blocks = 4 * ctx->num_sms, threads = 128, iters = 20000;
+  int rc = spx::ensure_workspace(ctx, sizeof(double) * (size_t)blocks * threads);
+  if (rc) return rc;
+  double* sink = reinterpret_cast<double*>(ctx->ws);
+  cudaEvent_t e0, e1;
+  if ((rc = spx::check_cuda(ctx, cudaEventCreate(&e0), "event")) ||
+      (rc = spx::check_cuda(ctx, cudaEventCreate(&e1), "event")))
+    return rc;
+  spx::dmma_peak_kernel<<<blocks, threads, 0, ctx->stream>>>(iters / 10, sink);
+  cudaEventRecord(e0, ctx->stream);
+  spx::dmma_peak_kernel<<<blocks, threads, 0, ctx->stream>>>(iters, sink);
+  cudaEventRecord(e1, ctx->stream);
+  rc = spx::check_cuda(ctx, cudaGetLastError(), "dmma_peak_kernel launch");
+  if (!rc) rc = spx::check_cuda(ctx, cudaEventSynchronize(e1), "dmma_peak_kernel");
+  float ms = 0.f;
+  if (!rc) rc = spx::check_cuda(ctx, cudaEventElapsedTime(&ms, e0, e1), "event time");
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  const double macs = 16.0 * 8 * 8 * 8 * (double)iters * (blocks * threads / 32);
+  *tflops = 2.0 * macs / (ms * 1e-3) / 1e12;
+  return SPX_OK;
+}

@@ -2,72 +2,58 @@
 //
 // The sum chi_f(i, j) = sum_p M(p, i) conj(M(p, j)) w(p, f) (src/susceptibility.f:
 // 1182-1240 with the HILBERT NONE weights of :950-975) is evaluated as an exact
-// integer contraction of 8-bit digit slices (an Ozaki-type error-free split):
+// integer contraction of 8-bit digit slices (an Ozaki-type error-free split) of
+// the weight-folded operand
 //
-//   x = s/127 * (d0 + d1/256 + d2/256^2 + d3/256^3 + r/256^3),  |d0| <= 127,
-//   d1..d3 in [-128, 127], |r| <= 1/2,
+//   A(p, i) = sqrt(|w(p, f)|) M(p, i),   chi_f = A^T diag(sgn w) conj(A),
 //
-// with s the largest |Re|, |Im| of the column over a slab of band pairs. The
-// digits are the balanced base-256 bytes of one integer, round(x*127/s * 2^24),
-// so a single FP64 -> int32 rounding per value produces all of them. The
-// unweighted operand A = M keeps 3 slices, the weighted operand B = w_f M keeps 4
-// (its column scale is s_j * max_p |w(p,f)|, so its relative resolution must
-// absorb the spread of the weights). Digit products with t + u <= 3 are summed on
-// tcgen05.mma kind::i8 into four int32 accumulators in tensor memory, one per
-// order g = t + u, which is exact: no rounding happens inside the contraction.
-// Once per slab of 32768 pairs (the int32 headroom: 3 * 128^2 * 32768 < 2^31) the
-// epilogue forms ((D0*256 + D1)*256 + D2)*256 + D3 exactly in int64 and adds
-// s_i s_j wmax_f / (127^2 2^24) times it to the FP64 output. The weights and
-// the scale factors stay FP64 throughout; near-degenerate pairs therefore keep
-// their FP64 weights.
+// one operand per frequency for both sides of the product. For every frequency
+// whose weights have one sign over the slab (all imaginary-axis HILBERT NONE
+// weights) the Gram is A^T conj(A) times that sign, a Hermitian rank-P update
+// whose two operands are the same digit planes. Frequencies with weights of both
+// signs take B(p, j) = sgn(w(p, f)) A(p, j) as the second operand (its own planes).
+// Each value becomes three balanced base-256 digits of one rounded integer,
 //
-// Error (per element, relative to sqrt|chi_ii chi_jj|): slicing of A (half a unit of
-// its third digit, 2^-17/127 of the column scale per value) <= 2^-17/127 times the
-// column crest factor max|x| sqrt(P)/||x||, slicing of B <= 2^-25/127 times the
-// weighted crest factor, dropped orders g >= 4 below that; see the accuracy tests.
+//   A = s sqrt(wmax)/127 * 2^-16 * (d0 2^16 + d1 2^8 + d2),  |d0| <= 127,
 //
-// Tile layout: a 64 x 64 complex tile is a 128 x 128 real-stacked product: A rows
-// are (Re M_i | Im M_i) for 64 mixed-basis functions, B rows likewise for the
-// 64 columns j; D[(c,i)][(c',j)] holds the four real products, combined in the
-// epilogue as re = D[re_i][re_j] + D[im_i][im_j], im = D[im_i][re_j] - D[re_i][im_j]
-// (the two halves live in different TMEM lane quarters and meet in shared memory).
+// with s the largest |Re|, |Im| of the column M(:, i) over the slab of band pairs
+// and wmax = max_p |w(p, f)|. The six digit products with t + u <= 2 are summed on
+// tcgen05.mma kind::i8 into three int32 accumulators in tensor memory, one per
+// order g = t + u, exactly (3 * 128^2 * 32768 < 2^31). Once per slab the epilogue
+// forms (D0*256 + D1)*256 + D2 exactly and adds s_i s_j wmax / (127^2 2^16) times
+// it (times the sign) to the FP64 output. Weights and scales stay FP64 throughout,
+// so near-degenerate pairs keep their FP64 weights.
+//
+// Error (per element, relative to sqrt(sum_p |w| |M_pi|^2 sum_p |w| |M_pj|^2), which
+// is sqrt|chi_ii chi_jj| for one-signed weights): rounding of each operand is half a
+// unit of its third digit, 2^-17/127 of its column scale, and the dropped orders
+// g >= 3 are of the same size; both enter with the crest factor max|A| sqrt(P)/||A||
+// of the folded columns.
+//
+// Tile layout: a 64 x 64 complex tile is a 128 x 128 real-stacked product whose rows
+// interleave the parts of each mixed-basis function: row 2i holds Re A_i and row
+// 2i+1 holds Im A_i (likewise the columns for j). D[2i+c][2j+c'] then holds the four
+// real products of (i, j) in two adjacent TMEM lanes, and the epilogue combines
+// re = D[2i][2j] + D[2i+1][2j+1], im = D[2i+1][2j] - D[2i][2j+1] by one warp shuffle.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <vector>
 
-#include "spx_common.cuh"
-#include "spx_tcgen05.cuh"
+#include "spx_split.cuh"
 
 namespace spx {
 
-constexpr int SP_TILE = 64;            // complex rows / columns per tile
-constexpr int SP_ROWS = 128;           // real-stacked rows per tile (re | im)
-constexpr int SP_KB = 64;              // band pairs (bytes) per pipeline stage: two MMA K steps
-constexpr int SP_KSTEP = 32;           // int8 MMA K
-constexpr int SP_NKS = SP_KB / SP_KSTEP;
-constexpr int SP_SA = 3;               // digit slices of the unweighted operand
-constexpr int SP_SB = 4;               // digit slices of the weighted operand
-constexpr int SP_ST = 3;               // pipeline stages
-constexpr int SP_SLAB = 32768;         // band pairs per exact int32 accumulation
+constexpr int SP_ST = 4;               // pipeline stages (one CTA per tile)
 constexpr int SP_THREADS = 192;        // warp 0 TMA, warp 1 MMA + TMEM, warps 2-5 epilogue
-constexpr int SP_PLANE = SP_ROWS * SP_KB;  // bytes of one slice of one stage
-constexpr int SP_TMEM_COLS = 512;      // 4 orders x 128 columns of int32
-
-
-// idesc for kind::i8: D s32 (bits 4-5 = 2), A/B signed int8 (bits 7-9, 10-12 = 1),
-// K-major A and B, N = 128 (bits 17-22 = N/8), M = 128 (bits 24-28 = M/16).
-constexpr uint32_t SP_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(SP_ROWS / 8) << 17) |
-                              ((uint32_t)(SP_ROWS / 16) << 24);
 
 struct __align__(1024) SplitSmem {
-  uint8_t a[SP_ST][SP_SA][SP_PLANE];
-  uint8_t b[SP_ST][SP_SB][SP_PLANE];
-  long long xchg[2][SP_TILE][33];      // epilogue exchange of the (row, Im col) halves
+  uint8_t a[SP_ST][SP_SF][SP_PLANE];
+  uint8_t b[SP_ST][SP_SF][SP_PLANE];
   uint64_t full[SP_ST];
   uint64_t empty[SP_ST];
-  uint64_t tfull, tempty, xfull, xfree, mdone;
+  uint64_t tfull, tempty, mdone;
   uint32_t tmem_base;
 };
 
@@ -76,43 +62,52 @@ struct SplitParams {
   int ntile;
   int nw;
   int nitems;
-  int nk;                 // pipeline stages per item (pairs of the slab / 32)
+  int nk;                 // pipeline stages per item (pairs of the slab / 64)
   const double* sA;       // column scales of the slab
   const double* wmax;     // max |w(p, f)| of the slab
+  const int* wsgn;        // per frequency: +1 / -1 one-signed weights, 0 both signs
   double* out;            // packed complex output, as doubles
   int64_t npack;
   int* status;
   uint64_t timeout_ns;
 };
 
-__device__ __forceinline__ void split_decode_tile(int t, int* bi, int* bj) {
-  int j = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
-  while (j * (j + 1) / 2 > t) --j;
-  while ((j + 1) * (j + 2) / 2 <= t) ++j;
-  *bj = j;
-  *bi = t - j * (j + 1) / 2;
-}
-
-// T = ((D0*256 + D1)*256 + D2)*256 + D3 for 32 columns starting at `taddr`, where
-// D_g sits 128 g columns further: the exact integer value of the slab's sum.
-__device__ __forceinline__ void load_orders(uint32_t taddr, long long (&T)[32]) {
-  int32_t r[32];
-  tmem_ld32(taddr, r);
-  tmem_wait_ld();
+// The epilogue of one tile, run by the four epilogue warps (warp q reads TMEM lanes
+// 32q..32q+31, i.e. rows i = 16q + lane/2, part c = lane & 1). The whole accumulator
+// is read into registers first and released to the MMA warp, so the next item's
+// MMAs overlap this tile's reductions into the output.
+template <class Release>
+__device__ __forceinline__ void fold_epilogue(uint32_t tl, int q, int lane, int bi, int bj, int f,
+                                              const SplitParams& prm, Release release) {
+  const int c = lane & 1;
+  double o[SP_TILE];
 #pragma unroll
-  for (int k = 0; k < 32; ++k) T[k] = r[k];
+  for (int cc = 0; cc < SP_TILE / 8; ++cc) {
+    double T[16];
+    load_fold16(tl + (uint32_t)(16 * cc), 128u, T);
 #pragma unroll
-  for (int g = 1; g < 4; ++g) {
-    tmem_ld32(taddr + (uint32_t)(g * 128), r);
-    tmem_wait_ld();
+    for (int jj = 0; jj < 8; ++jj) {
+      // both lanes of a row pair send their (., Im_j) product to the other one
+      const double pb = __shfl_xor_sync(0xffffffffu, T[2 * jj + 1], 1);
+      o[8 * cc + jj] = c == 0 ? T[2 * jj] + pb : T[2 * jj] - pb;
+    }
+  }
+  release();
+  const int gil = bi * SP_TILE + 16 * q + lane / 2;
+  if (gil >= prm.N) return;
+  const double fac = fold_row_factor(prm.wsgn[f], prm.sA[gil], prm.wmax[f]);
+  double* ob = prm.out + 2 * (int64_t)f * prm.npack + 2 * gil + c;
 #pragma unroll
-    for (int k = 0; k < 32; ++k) T[k] = T[k] * 256 + r[k];
+  for (int jj = 0; jj < SP_TILE; ++jj) {
+    const int gj = bj * SP_TILE + jj;
+    // one add per element per launch: launches are stream-ordered, so the sum is
+    // deterministic, and the reduction needs no read round trip
+    if (gil <= gj && gj < prm.N) atomicAdd(ob + (int64_t)gj * (gj + 1), fac * prm.sA[gj] * o[jj]);
   }
 }
 
 __global__ void __launch_bounds__(SP_THREADS, 1)
-    split_gram_kernel(const __grid_constant__ CUtensorMap mapA,
-                      const __grid_constant__ CUtensorMap mapB, SplitParams prm) {
+    split_gram_kernel(const __grid_constant__ CUtensorMap mapF, SplitParams prm) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   SplitSmem& sm = *reinterpret_cast<SplitSmem*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -125,8 +120,6 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
     }
     mbar_init(&sm.tfull, 1);
     mbar_init(&sm.tempty, 4);
-    mbar_init(&sm.xfull, 4);
-    mbar_init(&sm.xfree, 4);
     mbar_init(&sm.mdone, 1);
     fence_barrier_init();
   }
@@ -149,14 +142,18 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
         const int f = item / prm.ntile;
         int bi, bj;
         split_decode_tile(item % prm.ntile, &bi, &bj);
+        const int sg = prm.wsgn[f];
+        // a diagonal tile of a one-signed frequency multiplies A by itself
+        const bool same = sg != 0 && bi == bj;
+        const int za = f * SP_SLOT, zb = za + (sg == 0 ? SP_SF : 0);
         for (int ks = 0; ks < prm.nk; ++ks) {
           if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) {
             ok = false;
             break;
           }
-          mbar_arrive_expect_tx(&sm.full[st], (uint32_t)((SP_SA + SP_SB) * SP_PLANE));
-          tma_load_4d(&sm.a[st][0][0], &mapA, 0, bi * SP_ROWS, ks, 0, &sm.full[st]);
-          tma_load_4d(&sm.b[st][0][0], &mapB, 0, bj * SP_ROWS, ks, f * SP_SB, &sm.full[st]);
+          mbar_arrive_expect_tx(&sm.full[st], (uint32_t)((same ? 1 : 2) * SP_SF * SP_PLANE));
+          tma_load_4d(&sm.a[st][0][0], &mapF, 0, bi * SP_ROWS, ks, za, &sm.full[st]);
+          if (!same) tma_load_4d(&sm.b[st][0][0], &mapF, 0, bj * SP_ROWS, ks, zb, &sm.full[st]);
           issued[st] = true;
           last_ph[st] = ph;
           if (++st == SP_ST) st = 0, ph ^= 1u;
@@ -174,6 +171,10 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       int j = 0;
       bool committed = false;
       for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j) {
+        const int f = item / prm.ntile;
+        int bi, bj;
+        split_decode_tile(item % prm.ntile, &bi, &bj);
+        const bool same = prm.wsgn[f] != 0 && bi == bj;
         // accumulators free (first item: immediately)
         if (!mbar_wait(&sm.tempty, (uint32_t)(j & 1) ^ 1u, prm.timeout_ns, prm.status)) break;
         tc_fence_after();
@@ -185,24 +186,22 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
           }
           tc_fence_after();
           // order g = t + u lives at TMEM columns [128 g, 128 g + 128); the first
-          // product of every order in a slab (t == 0, first K step) overwrites it
+          // product of every order in a slab (first K step) overwrites it
 #pragma unroll
           for (int kk = 0; kk < SP_NKS; ++kk) {
-            uint64_t da[SP_SA], db[SP_SB];
+            uint64_t da[SP_SF], db[SP_SF];
 #pragma unroll
-            for (int t = 0; t < SP_SA; ++t) da[t] = desc_sw64(&sm.a[st][t][0]) + (uint64_t)(kk * 2);
-#pragma unroll
-            for (int u = 0; u < SP_SB; ++u) db[u] = desc_sw64(&sm.b[st][u][0]) + (uint64_t)(kk * 2);
+            for (int t = 0; t < SP_SF; ++t) {
+              da[t] = desc_sw64(&sm.a[st][t][0]) + (uint64_t)(kk * 2);
+              db[t] = same ? da[t] : desc_sw64(&sm.b[st][t][0]) + (uint64_t)(kk * 2);
+            }
             const uint32_t k0 = (ks > 0 || kk > 0);
             mma_i8<1>(tmem + 0 * 128, da[0], db[0], SP_IDESC, k0);
             mma_i8<2>(tmem + 1 * 128, da[0], db[1], SP_IDESC, k0);
-            mma_i8<2>(tmem + 2 * 128, da[0], db[2], SP_IDESC, k0);
-            mma_i8<3>(tmem + 3 * 128, da[0], db[3], SP_IDESC, k0);
+            mma_i8<3>(tmem + 2 * 128, da[0], db[2], SP_IDESC, k0);
             mma_i8<1>(tmem + 1 * 128, da[1], db[0], SP_IDESC, 1u);
-            mma_i8<2>(tmem + 2 * 128, da[1], db[1], SP_IDESC, 1u);
-            mma_i8<3>(tmem + 3 * 128, da[1], db[2], SP_IDESC, 1u);
-            mma_i8<1>(tmem + 2 * 128, da[2], db[0], SP_IDESC, 1u);
-            mma_i8<3>(tmem + 3 * 128, da[2], db[1], SP_IDESC, 1u);
+            mma_i8<3>(tmem + 2 * 128, da[1], db[1], SP_IDESC, 1u);
+            mma_i8<0>(tmem + 2 * 128, da[2], db[0], SP_IDESC, 1u);
           }
           tc_commit(&sm.empty[st]);  // stage free once these MMAs have read it
           committed = true;
@@ -220,61 +219,20 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
     }
   } else {
     // ---------------- epilogue: 4 warps, one TMEM lane quarter each ----------------
-    const int q = warp & 3;                 // lane quarter
-    const bool is_re = q < 2;               // lanes 0-63: Re rows, 64-127: Im rows
-    const int ii = (q & 1) * 32 + lane;     // complex row within the tile
+    const int q = warp & 3;
     const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16);
     int j = 0;
-    uint32_t xseq = 0;
     for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j) {
       if (!mbar_wait_idle(&sm.tfull, (uint32_t)(j & 1), prm.timeout_ns, prm.status)) break;
       tc_fence_after();
       const int f = item / prm.ntile;
       int bi, bj;
       split_decode_tile(item % prm.ntile, &bi, &bj);
-      const int gi = bi * SP_TILE + ii;
-      const double si = gi < prm.N ? prm.sA[gi] : 0.0;
-      const double fac =
-          si * prm.wmax[f] * (1.0 / (127.0 * 127.0 * 16777216.0));
-      double* outf = prm.out + 2 * (int64_t)f * prm.npack;
-      bool ok = true;
-      for (int js = 0; js < 2 && ok; ++js, ++xseq) {
-        long long tre[32], tim[32];  // T[row][Re col], T[row][Im col] for 32 columns j
-        load_orders(tl + (uint32_t)(js * 32), tre);
-        load_orders(tl + (uint32_t)(64 + js * 32), tim);
-        // exchange the Im-column halves between the Re and Im rows of each i
-        if (!mbar_wait(&sm.xfree, (xseq & 1u) ^ 1u, prm.timeout_ns, prm.status)) {
-          ok = false;
-          break;
-        }
-#pragma unroll
-        for (int k = 0; k < 32; ++k) sm.xchg[is_re ? 0 : 1][ii][k] = tim[k];
+      fold_epilogue(tl, q, lane, bi, bj, f, prm, [&] {
+        tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.xfull);
-        if (!mbar_wait(&sm.xfull, xseq & 1u, prm.timeout_ns, prm.status)) {
-          ok = false;
-          break;
-        }
-        // Re rows: chi_re = T[re_i][re_j] + T[im_i][im_j]; Im rows: chi_im = T[im_i][re_j] - T[re_i][im_j]
-#pragma unroll
-        for (int k = 0; k < 32; ++k) {
-          const int gj = bj * SP_TILE + js * 32 + k;
-          const long long partner = sm.xchg[is_re ? 1 : 0][ii][k];
-          const long long v = is_re ? tre[k] + partner : tre[k] - partner;
-          if (gi <= gj && gj < prm.N) {
-            // one add per element per launch: launches are ordered, so the sum is
-            // deterministic, and the reduction needs no read round trip
-            double* o = outf + 2 * ((int64_t)gj * (gj + 1) / 2 + gi) + (is_re ? 0 : 1);
-            atomicAdd(o, fac * prm.sA[gj] * (double)v);
-          }
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.xfree);
-      }
-      if (!ok) break;
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&sm.tempty);
+        if (lane == 0) mbar_arrive(&sm.tempty);
+      });
     }
   }
 
@@ -287,28 +245,25 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
 // ---------------------------------------------------------------------------
 // CTA-pair form: one tcgen05.mma.cta_group::2 (M = 256) covers two 64 x 64 complex
 // tiles stacked in i. Each CTA of the cluster stages its own A tile (128 rows) and
-// half of the shared B tile (64 rows: CTA 0 the Re rows, CTA 1 the Im rows of the
-// 64 columns j); the leader CTA issues the MMAs, which read both CTAs' shared
-// memory and write each CTA's own TMEM. Per SM and stage this moves 20 KB instead
-// of 28 KB from L2 for the same tensor work. Every completion that crosses the
-// pair is an explicit remote arrive or commit (no multicast).
+// half of the shared B tile (64 rows: CTA 0 the columns j of the first 32, CTA 1
+// the next 32); the leader CTA issues the MMAs, which read both CTAs' shared memory
+// and write each CTA's own TMEM. Every completion that crosses the pair is an
+// explicit remote arrive or commit (no multicast).
 
 constexpr int SP2_ST = 5;
-constexpr int SP2_XC = 16;                      // columns per epilogue exchange
 constexpr int SP2_BROWS = SP_ROWS / 2;          // B rows staged per CTA
-constexpr int SP2_BPLANE = SP2_BROWS * SP_KB;   // 2048 bytes
+constexpr int SP2_BPLANE = SP2_BROWS * SP_KB;   // 4096 bytes
 constexpr uint32_t SP2_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(SP_ROWS / 8) << 17) |
                                ((uint32_t)(2 * SP_ROWS / 16) << 24);   // M = 256, N = 128
 
 struct __align__(1024) Split2Smem {
-  uint8_t a[SP2_ST][SP_SA][SP_PLANE];
-  uint8_t b[SP2_ST][SP_SB][SP2_BPLANE];
-  long long xchg[2][SP_TILE][SP2_XC + 1];
+  uint8_t a[SP2_ST][SP_SF][SP_PLANE];
+  uint8_t b[SP2_ST][SP_SF][SP2_BPLANE];
   uint64_t full[SP2_ST];   // leader: both CTAs' bytes of a stage have landed
   uint64_t empty[SP2_ST];  // each CTA: the MMAs have read the stage
   uint64_t tfull;          // each CTA: accumulators ready
   uint64_t tempty;         // leader: both CTAs' epilogues have drained TMEM (8 warps)
-  uint64_t xfull, xfree, mdone;
+  uint64_t mdone;
   uint32_t tmem_base;
 };
 
@@ -324,25 +279,9 @@ __device__ __forceinline__ void pair_decode_tile(int t, int* bI, int* bJ) {
   *bI = t - c;
 }
 
-// T = ((D0*256 + D1)*256 + D2)*256 + D3 for 16 columns starting at `taddr`.
-__device__ __forceinline__ void load_orders16(uint32_t taddr, long long (&T)[16]) {
-  int32_t r[16];
-  tmem_ld16(taddr, r);
-  tmem_wait_ld();
-#pragma unroll
-  for (int k = 0; k < 16; ++k) T[k] = r[k];
-#pragma unroll
-  for (int g = 1; g < 4; ++g) {
-    tmem_ld16(taddr + (uint32_t)(g * 128), r);
-    tmem_wait_ld();
-#pragma unroll
-    for (int k = 0; k < 16; ++k) T[k] = T[k] * 256 + r[k];
-  }
-}
-
 __global__ void __launch_bounds__(SP_THREADS, 1)
-    split_gram2_kernel(const __grid_constant__ CUtensorMap mapA,
-                       const __grid_constant__ CUtensorMap mapB, SplitParams prm) {
+    split_gram2_kernel(const __grid_constant__ CUtensorMap mapF,
+                       const __grid_constant__ CUtensorMap mapFh, SplitParams prm) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   Split2Smem& sm = *reinterpret_cast<Split2Smem*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -357,8 +296,6 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
     }
     mbar_init(&sm.tfull, 1);
     mbar_init(&sm.tempty, 8);
-    mbar_init(&sm.xfull, 4);
-    mbar_init(&sm.xfree, 4);
     mbar_init(&sm.mdone, 1);
     fence_barrier_init();
   }
@@ -380,14 +317,16 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       // Cursor over this cluster's (item, stage) sequence; it advances by increments
       // and decodes a tile only when it enters a new item.
       struct Cursor {
-        int item, ks, ya, yb, zf;
+        int item, ks, ya, yb, za, zb;
       };
       auto enter = [&](Cursor& u) {
         int bI, bJ;
         pair_decode_tile(u.item % prm.ntile, &bI, &bJ);
+        const int f = u.item / prm.ntile;
         u.ya = (2 * bI + (int)rank) * SP_ROWS;
         u.yb = bJ * SP_ROWS + (int)rank * SP2_BROWS;
-        u.zf = (u.item / prm.ntile) * SP_SB;
+        u.za = f * SP_SLOT;
+        u.zb = u.za + (prm.wsgn[f] == 0 ? SP_SF : 0);
       };
       auto advance = [&](Cursor& u) {
         if (++u.ks == prm.nk) {
@@ -396,7 +335,7 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
           if (u.item < prm.nitems) enter(u);
         }
       };
-      Cursor ld{cid, 0, 0, 0, 0};
+      Cursor ld{cid, 0, 0, 0, 0, 0};
       if (cid < prm.nitems) enter(ld);
       while (ld.item < prm.nitems) {
         if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) {
@@ -405,15 +344,15 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
         }
         const uint32_t lead_full = mapa_shared(smem_u32(&sm.full[st]), 0);
         if (rank == 0)
-          mbar_arrive_expect_tx(&sm.full[st],
-                                (uint32_t)(2 * (SP_SA * SP_PLANE + SP_SB * SP2_BPLANE)));
-        tma_load_4d_pair(&sm.a[st][0][0], &mapA, 0, ld.ya, ld.ks, 0, lead_full);
-        tma_load_4d_pair(&sm.b[st][0][0], &mapB, 0, ld.yb, ld.ks, ld.zf, lead_full);
+          mbar_arrive_expect_tx(&sm.full[st], (uint32_t)(2 * SP_SF * (SP_PLANE + SP2_BPLANE)));
+        tma_load_4d_pair(&sm.a[st][0][0], &mapF, 0, ld.ya, ld.ks, ld.za, lead_full);
+        tma_load_4d_pair(&sm.b[st][0][0], &mapFh, 0, ld.yb, ld.ks, ld.zb, lead_full);
         advance(ld);
         issued[st] = true;
         last_ph[st] = ph;
         if (++st == SP2_ST) st = 0, ph ^= 1u;
       }
+      (void)ok;
       if (rank == 0) {
         // the leader's stage barriers count both CTAs' bytes
         for (int q = 0; q < SP2_ST; ++q)
@@ -446,21 +385,19 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
           tc_fence_after();
 #pragma unroll
           for (int kk = 0; kk < SP_NKS; ++kk) {
-            uint64_t da[SP_SA], db[SP_SB];
+            uint64_t da[SP_SF], db[SP_SF];
 #pragma unroll
-            for (int t = 0; t < SP_SA; ++t) da[t] = desc_sw64(&sm.a[st][t][0]) + (uint64_t)(kk * 2);
-#pragma unroll
-            for (int u = 0; u < SP_SB; ++u) db[u] = desc_sw64(&sm.b[st][u][0]) + (uint64_t)(kk * 2);
+            for (int t = 0; t < SP_SF; ++t) {
+              da[t] = desc_sw64(&sm.a[st][t][0]) + (uint64_t)(kk * 2);
+              db[t] = desc_sw64(&sm.b[st][t][0]) + (uint64_t)(kk * 2);
+            }
             const uint32_t k0 = (ks > 0 || kk > 0);
             mma2_i8<1>(tmem + 0 * 128, da[0], db[0], SP2_IDESC, k0);
             mma2_i8<2>(tmem + 1 * 128, da[0], db[1], SP2_IDESC, k0);
-            mma2_i8<2>(tmem + 2 * 128, da[0], db[2], SP2_IDESC, k0);
-            mma2_i8<3>(tmem + 3 * 128, da[0], db[3], SP2_IDESC, k0);
+            mma2_i8<3>(tmem + 2 * 128, da[0], db[2], SP2_IDESC, k0);
             mma2_i8<1>(tmem + 1 * 128, da[1], db[0], SP2_IDESC, 1u);
-            mma2_i8<2>(tmem + 2 * 128, da[1], db[1], SP2_IDESC, 1u);
-            mma2_i8<3>(tmem + 3 * 128, da[1], db[2], SP2_IDESC, 1u);
-            mma2_i8<1>(tmem + 2 * 128, da[2], db[0], SP2_IDESC, 1u);
-            mma2_i8<3>(tmem + 3 * 128, da[2], db[1], SP2_IDESC, 1u);
+            mma2_i8<3>(tmem + 2 * 128, da[1], db[1], SP2_IDESC, 1u);
+            mma2_i8<0>(tmem + 2 * 128, da[2], db[0], SP2_IDESC, 1u);
           }
           // the stage is free in both CTAs once these MMAs have read it
           tc_commit2(smem_u32(&sm.empty[st]));
@@ -480,12 +417,9 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
   } else {
     // ---------------- epilogue (both CTAs): this CTA's 64 x 64 tile ----------------
     const int q = warp & 3;
-    const bool is_re = q < 2;
-    const int ii = (q & 1) * 32 + lane;
     const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16);
     const uint32_t lead_tempty = mapa_shared(smem_u32(&sm.tempty), 0);
     int j = 0;
-    uint32_t xseq = 0;
     for (int item = cid; item < prm.nitems; item += ncl, ++j) {
       if (!mbar_wait_idle(&sm.tfull, (uint32_t)(j & 1), prm.timeout_ns, prm.status)) break;
       tc_fence_after();
@@ -493,50 +427,17 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       int bI, bJ;
       pair_decode_tile(item % prm.ntile, &bI, &bJ);
       const int bi = 2 * bI + (int)rank;
-      bool ok = true;
-      // a tile wholly below the diagonal or past N has nothing to store
-      if (bi <= bJ && bi * SP_TILE < prm.N) {
-        const int gi = bi * SP_TILE + ii;
-        const double si = gi < prm.N ? prm.sA[gi] : 0.0;
-        const double fac = si * prm.wmax[f] * (1.0 / (127.0 * 127.0 * 16777216.0));
-        double* outf = prm.out + 2 * (int64_t)f * prm.npack;
-        for (int js = 0; js < SP_TILE / SP2_XC && ok; ++js, ++xseq) {
-          long long tre[SP2_XC], tim[SP2_XC];
-          load_orders16(tl + (uint32_t)(js * SP2_XC), tre);
-          load_orders16(tl + (uint32_t)(64 + js * SP2_XC), tim);
-          if (!mbar_wait(&sm.xfree, (xseq & 1u) ^ 1u, prm.timeout_ns, prm.status)) {
-            ok = false;
-            break;
-          }
-#pragma unroll
-          for (int k = 0; k < SP2_XC; ++k) sm.xchg[is_re ? 0 : 1][ii][k] = tim[k];
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&sm.xfull);
-          if (!mbar_wait(&sm.xfull, xseq & 1u, prm.timeout_ns, prm.status)) {
-            ok = false;
-            break;
-          }
-#pragma unroll
-          for (int k = 0; k < SP2_XC; ++k) {
-            const int gj = bJ * SP_TILE + js * SP2_XC + k;
-            const long long partner = sm.xchg[is_re ? 1 : 0][ii][k];
-            const long long v = is_re ? tre[k] + partner : tre[k] - partner;
-            if (gi <= gj && gj < prm.N) {
-              double* o = outf + 2 * ((int64_t)gj * (gj + 1) / 2 + gi) + (is_re ? 0 : 1);
-              atomicAdd(o, fac * prm.sA[gj] * (double)v);
-            }
-          }
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&sm.xfree);
+      auto release = [&] {
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) {
+          if (rank == 0) mbar_arrive(&sm.tempty);
+          else mbar_arrive_cluster(lead_tempty);
         }
-      }
-      if (!ok) break;
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) {
-        if (rank == 0) mbar_arrive(&sm.tempty);
-        else mbar_arrive_cluster(lead_tempty);
-      }
+      };
+      // a tile wholly below the diagonal or past N has nothing to store
+      if (bi <= bJ && bi * SP_TILE < prm.N) fold_epilogue(tl, q, lane, bi, bJ, f, prm, release);
+      else release();
     }
   }
 
@@ -571,67 +472,73 @@ __global__ void split_colmax_kernel(const double2* __restrict__ M, int64_t ldc, 
   }
 }
 
-// wmax[f] = max_p |w(p, f)| over the slab.
-__global__ void split_wmax_kernel(const double* __restrict__ W, int64_t ldw, int64_t p0, int len,
-                                  double* __restrict__ wmax) {
+// Per frequency f over the slab: wmax[f] = max_p |w(p, f)|, the sign code wsgn[f]
+// (+1 all weights >= 0, -1 all <= 0, 0 both signs), and the folded factors
+// G[f][p] = sgn(w) sqrt(|w| / wmax) * 127 * 2^16 (0 past the slab's end).
+__global__ void split_wstat_kernel(const double* __restrict__ W, int64_t ldw, int64_t p0, int len,
+                                   int lenp, double* __restrict__ wmax, int* __restrict__ wsgn,
+                                   double* __restrict__ G) {
   const int f = blockIdx.x;
   const double* wf = W + (int64_t)f * ldw + p0;
   double m = 0.0;
-  for (int p = threadIdx.x; p < len; p += blockDim.x) m = fmax(m, fabs(wf[p]));
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  int pos = 0, neg = 0;
+  for (int p = threadIdx.x; p < len; p += blockDim.x) {
+    const double w = wf[p];
+    m = fmax(m, fabs(w));
+    pos |= w > 0.0;
+    neg |= w < 0.0;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    pos |= __shfl_xor_sync(0xffffffffu, pos, o);
+    neg |= __shfl_xor_sync(0xffffffffu, neg, o);
+  }
   __shared__ double red[32];
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __shared__ int rpos[32], rneg[32];
+  __shared__ double wm_s;
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = m;
+    rpos[threadIdx.x >> 5] = pos;
+    rneg[threadIdx.x >> 5] = neg;
+  }
   __syncthreads();
   if (threadIdx.x < 32) {
-    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (threadIdx.x == 0) wmax[f] = m;
+    const bool v = threadIdx.x < (blockDim.x >> 5);
+    m = v ? red[threadIdx.x] : 0.0;
+    pos = v ? rpos[threadIdx.x] : 0;
+    neg = v ? rneg[threadIdx.x] : 0;
+    for (int o = 16; o > 0; o >>= 1) {
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      pos |= __shfl_xor_sync(0xffffffffu, pos, o);
+      neg |= __shfl_xor_sync(0xffffffffu, neg, o);
+    }
+    if (threadIdx.x == 0) {
+      wmax[f] = m;
+      wsgn[f] = (pos && neg) ? 0 : (neg ? -1 : 1);
+      wm_s = m;
+    }
   }
-}
-
-// Round-to-nearest integer of a*b (|a*b| < 2^31) through the FP64 magic constant
-// 1.5*2^52: one fused multiply-add, the low word of the sum is the integer.
-__device__ __forceinline__ uint32_t round_mul(double a, double b) {
-  return (uint32_t)__double2loint(__fma_rn(a, b, 6755399441055744.0));
-}
-
-// Four values Y (two's complement words) -> their balanced base-256 digit planes.
-// With U = Y + 0x808080, bytes 0..2 of U are the lower digits plus 128 and byte 3
-// is the top digit (|top| <= 127 because |Y| <= 127 * 2^24). out[t] holds digit t
-// (t = 0 most significant) of the four values, one per byte.
-template <int S>
-__device__ __forceinline__ void digit_planes(const uint32_t (&Y)[4], uint32_t (&out)[S]) {
-  const uint32_t bias = S == 4 ? 0x00808080u : 0x00008080u;
-  const uint32_t u0 = Y[0] + bias, u1 = Y[1] + bias, u2 = Y[2] + bias, u3 = Y[3] + bias;
-  const uint32_t lo01 = __byte_perm(u0, u1, 0x5140), lo23 = __byte_perm(u2, u3, 0x5140);
-  const uint32_t hi01 = __byte_perm(u0, u1, 0x7362), hi23 = __byte_perm(u2, u3, 0x7362);
-  const uint32_t b0 = __byte_perm(lo01, lo23, 0x5410) ^ 0x80808080u;  // byte 0 of each
-  const uint32_t b1 = __byte_perm(lo01, lo23, 0x7632) ^ 0x80808080u;  // byte 1
-  const uint32_t b2 = __byte_perm(hi01, hi23, 0x5410);                // byte 2
-  if constexpr (S == 4) {
-    out[0] = __byte_perm(hi01, hi23, 0x7632);  // byte 3: top digit
-    out[1] = b2 ^ 0x80808080u;
-    out[2] = b1;
-    out[3] = b0;
-  } else {
-    out[0] = b2;  // byte 2: top digit of a 3-digit value
-    out[1] = b1;
-    out[2] = b0;
+  __syncthreads();
+  const double wm = wm_s;
+  double* gf = G + (int64_t)f * lenp;
+  for (int p = threadIdx.x; p < lenp; p += blockDim.x) {
+    gf[p] = p < len ? fold_factor(wf[p], wm) : 0.0;
   }
 }
 
 // One thread = one complex column i and 16 consecutive pairs of the slab. Digit
 // planes are stored [plane][k-block of 64 pairs][row][64 bytes]; a warp holds 8
-// consecutive columns x the four quarters of one k-block, so every store
-// instruction writes 8 adjacent rows x 64 bytes = 512 contiguous bytes, and the TMA
-// box (64 B, rows, 1 k-block, planes) lands as [plane][row][64 B] in shared memory.
-// Rows are real-stacked: block b of 64 columns -> rows 128 b + {0..63 Re, 64..127 Im}.
+// consecutive columns x the four quarters of one k-block, so its stores cover 16
+// adjacent rows x 64 bytes, and the TMA box (64 B, rows, 1 k-block, planes) lands as
+// [plane][row][64 B] in shared memory. Rows interleave the parts: column i -> rows
+// 128 (i / 64) + 2 (i % 64) (Re) and the next one (Im). For frequency f the planes
+// f*6 + t hold the digits t of round(x |G| / s) (the folded operand), and, when the
+// frequency's weights have both signs, planes f*6 + 3 + t those of round(x G / s).
 __global__ void __launch_bounds__(128)
     split_quantize_kernel(const double2* __restrict__ M, int64_t ldc, int64_t p0, int len,
-                          int nchunk, int N, int npad, int64_t R, int64_t Ps,
-                          const double* __restrict__ W, int64_t ldw, int nw,
-                          const double* __restrict__ sA, const double* __restrict__ wmax,
-                          int8_t* __restrict__ A, int8_t* __restrict__ B) {
+                          int nchunk, int N, int npad, int64_t R, int64_t Ps, int nw,
+                          const double* __restrict__ sA, const int* __restrict__ wsgn,
+                          const double* __restrict__ G, int8_t* __restrict__ F) {
   const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (tid >= (int64_t)npad * nchunk) return;
   // tid -> (k-block, column group of 8, quarter of the k-block, column in group)
@@ -641,80 +548,13 @@ __global__ void __launch_bounds__(128)
   const int i = (int)(rest % ngroup) * 8 + lane8;
   const int64_t kb = rest / ngroup;
   const int p = (int)(kb * SP_KB) + quarter * 16;
-  const int64_t r_re = (int64_t)(i / SP_TILE) * SP_ROWS + (i % SP_TILE);
-  const int64_t r_im = r_re + SP_TILE;
   const int64_t nkb = Ps / SP_KB;
-  // byte offsets of (plane 0, k-block, row) for this thread's 16 pairs; planes are
-  // nkb * R * 32 bytes apart
+  // planes are nkb * R * 64 bytes apart
   const int64_t pstride = nkb * R * SP_KB;
-  const int64_t a_re = (kb * R + r_re) * SP_KB + quarter * 16;
-  const int64_t a_im = (kb * R + r_im) * SP_KB + quarter * 16;
-  const int64_t b_re = a_re, b_im = a_im;
-  double xr[16], xi[16];
+  const int64_t o_re = (kb * R + split_row_re(i)) * SP_KB + quarter * 16;
   const bool col_ok = i < N;
-#pragma unroll
-  for (int k = 0; k < 16; ++k) {
-    double2 v = make_double2(0.0, 0.0);
-    if (col_ok && p + k < len) v = M[(int64_t)i * ldc + p0 + p + k];
-    xr[k] = v.x;
-    xi[k] = v.y;
-  }
-  const double s = col_ok ? sA[i] : 0.0;
-  // unweighted operand: 3 digits of round(x * 127/s * 2^16)
-  {
-    const double inv = s > 0.0 ? 127.0 * 65536.0 / s : 0.0;
-    uint32_t wr[SP_SA][4], wi[SP_SA][4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      uint32_t yr[4], yi[4], pr[SP_SA], pi[SP_SA];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        yr[k] = round_mul(xr[4 * q + k], inv);
-        yi[k] = round_mul(xi[4 * q + k], inv);
-      }
-      digit_planes<SP_SA>(yr, pr);
-      digit_planes<SP_SA>(yi, pi);
-#pragma unroll
-      for (int t = 0; t < SP_SA; ++t) wr[t][q] = pr[t], wi[t][q] = pi[t];
-    }
-#pragma unroll
-    for (int t = 0; t < SP_SA; ++t) {
-      *reinterpret_cast<uint4*>(A + a_re + t * pstride) =
-          make_uint4(wr[t][0], wr[t][1], wr[t][2], wr[t][3]);
-      *reinterpret_cast<uint4*>(A + a_im + t * pstride) =
-          make_uint4(wi[t][0], wi[t][1], wi[t][2], wi[t][3]);
-    }
-  }
-  // weighted operand, one frequency at a time: 4 digits of round(x w 127/(wmax s) 2^24)
-  for (int f = 0; f < nw; ++f) {
-    const double wm = wmax[f];
-    const double g = (s > 0.0 && wm > 0.0) ? 127.0 * 16777216.0 / (wm * s) : 0.0;
-    const double* wf = W + (int64_t)f * ldw + p0 + p;
-    uint32_t wr[SP_SB][4], wi[SP_SB][4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      uint32_t yr[4], yi[4], pr[SP_SB], pi[SP_SB];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int kk = 4 * q + k;
-        const double wk = (p + kk < len) ? wf[kk] * g : 0.0;
-        yr[k] = round_mul(xr[kk], wk);
-        yi[k] = round_mul(xi[kk], wk);
-      }
-      digit_planes<SP_SB>(yr, pr);
-      digit_planes<SP_SB>(yi, pi);
-#pragma unroll
-      for (int u = 0; u < SP_SB; ++u) wr[u][q] = pr[u], wi[u][q] = pi[u];
-    }
-#pragma unroll
-    for (int u = 0; u < SP_SB; ++u) {
-      const int64_t plane = (int64_t)f * SP_SB + u;
-      *reinterpret_cast<uint4*>(B + b_re + plane * pstride) =
-          make_uint4(wr[u][0], wr[u][1], wr[u][2], wr[u][3]);
-      *reinterpret_cast<uint4*>(B + b_im + plane * pstride) =
-          make_uint4(wi[u][0], wi[u][1], wi[u][2], wi[u][3]);
-    }
-  }
+  quantize_task(M + (int64_t)(col_ok ? i : 0) * ldc + p0, col_ok, len, p, col_ok ? sA[i] : 0.0,
+                o_re, pstride, nw, wsgn, G, nchunk * 16, F);
 }
 
 // ---------------------------------------------------------------------------
@@ -736,6 +576,26 @@ static EncodeTiledFn get_encode() {
       fn = (EncodeTiledFn)p;
   }
   return fn;
+}
+
+// Generic tiled tensor map (no context): 0 on success, -1 without the driver entry
+// point, else the driver's error code.
+int encode_tmap(CUtensorMap* map, CUtensorMapDataType type, int rank, const void* base,
+                const uint64_t* dims, const uint64_t* strides, const uint32_t* box,
+                CUtensorMapSwizzle swz) {
+  auto enc = get_encode();
+  if (!enc) return -1;
+  cuuint64_t d[5], st[4];
+  cuuint32_t b[5], es[5];
+  for (int i = 0; i < rank; ++i) {
+    d[i] = dims[i];
+    b[i] = box[i];
+    es[i] = 1;
+    if (i + 1 < rank) st[i] = strides[i];
+  }
+  return (int)enc(map, type, (cuuint32_t)rank, const_cast<void*>(base), d, st, b, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
 
 int make_tmap_u8_3d(spx_ctx* ctx, CUtensorMap* map, const void* base, uint64_t d0, uint64_t d1,
@@ -774,7 +634,7 @@ int make_tmap_u8_4d(spx_ctx* ctx, CUtensorMap* map, const void* base, const uint
 struct SplitLayout {
   int64_t Ps, R;
   int nblk;
-  size_t a_bytes, b_bytes, s_bytes, w_bytes;
+  size_t f_bytes, g_bytes, s_bytes, w_bytes, sg_bytes;
 };
 
 // slab: band pairs per exact int32 slab, a multiple of SP_KB in [SP_KB, SP_SLAB]
@@ -784,10 +644,11 @@ static SplitLayout split_layout(int64_t P, int N, int nw, int slab = SP_SLAB) {
   L.nblk = (N + SP_TILE - 1) / SP_TILE;
   // an even number of 64-blocks, so a CTA pair's second A tile always exists
   L.R = (int64_t)((L.nblk + 1) / 2 * 2) * SP_ROWS;
-  L.a_bytes = align_up((size_t)SP_SA * L.R * L.Ps, 1024);
-  L.b_bytes = align_up((size_t)SP_SB * nw * L.R * L.Ps, 1024);
+  L.f_bytes = align_up((size_t)SP_SLOT * nw * L.R * L.Ps, 1024);
+  L.g_bytes = align_up(sizeof(double) * (size_t)nw * L.Ps, 256);
   L.s_bytes = align_up(sizeof(double) * (size_t)std::max(N, 1), 256);
   L.w_bytes = align_up(sizeof(double) * (size_t)std::max(nw, 1), 256);
+  L.sg_bytes = align_up(sizeof(int) * (size_t)std::max(nw, 1), 256);
   return L;
 }
 
@@ -803,7 +664,7 @@ static int clamp_slab(int slab) {
 size_t split_workspace_bytes(int64_t P, int N, int nw, int slab) {
   slab = clamp_slab(slab);
   SplitLayout L = split_layout(P, N, nw, slab);
-  return split_nbuf(P, slab) * (L.a_bytes + L.b_bytes + L.s_bytes + L.w_bytes) + 1024;
+  return split_nbuf(P, slab) * (L.f_bytes + L.g_bytes + L.s_bytes + L.w_bytes + L.sg_bytes) + 1024;
 }
 size_t split_workspace_bytes(int64_t P, int N, int nw) {
   return split_workspace_bytes(P, N, nw, SP_SLAB);
@@ -823,34 +684,35 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
     return set_error(ctx, SPX_EINVAL, "split workspace too small");
   uint8_t* base = (uint8_t*)align_up((size_t)ws, 1024);
   const int nbuf = split_nbuf(P, slab);
-  const size_t set_bytes = L.a_bytes + L.b_bytes + L.s_bytes + L.w_bytes;
-  int8_t* A[2];
-  int8_t* B[2];
+  const size_t set_bytes = L.f_bytes + L.g_bytes + L.s_bytes + L.w_bytes + L.sg_bytes;
+  int8_t* F[2];
+  double* G[2];
   double* sA[2];
   double* wmax[2];
+  int* wsgn[2];
   for (int b = 0; b < 2; ++b) {
     uint8_t* s0 = base + (size_t)(b < nbuf ? b : 0) * set_bytes;
-    A[b] = (int8_t*)s0;
-    B[b] = (int8_t*)(s0 + L.a_bytes);
-    sA[b] = (double*)(s0 + L.a_bytes + L.b_bytes);
-    wmax[b] = (double*)(s0 + L.a_bytes + L.b_bytes + L.s_bytes);
+    F[b] = (int8_t*)s0;
+    G[b] = (double*)(s0 + L.f_bytes);
+    sA[b] = (double*)(s0 + L.f_bytes + L.g_bytes);
+    wmax[b] = (double*)(s0 + L.f_bytes + L.g_bytes + L.s_bytes);
+    wsgn[b] = (int*)(s0 + L.f_bytes + L.g_bytes + L.s_bytes + L.w_bytes);
   }
 
   // planes in HBM: [plane][k-block][row][K bytes]; TMA dims (K, row, k-block, plane)
-  // with increasing strides; a box (K, rows, 1, planes) lands as [plane][row][K]
+  // with increasing strides; a box (K, rows, 1, 3 planes) lands as [plane][row][K]
   const uint64_t nkb = (uint64_t)(L.Ps / SP_KB);
   if (variant == 0) variant = ctx->opt.split_variant;
   const bool pair = variant != 1;  // 0 (auto) and 2 select the CTA pair
-  CUtensorMap mapA[2], mapB[2];
+  CUtensorMap mapF[2], mapFh[2];
   for (int b = 0; b < nbuf; ++b) {
-    const uint64_t sta[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};
-    const uint64_t da[4] = {SP_KB, (uint64_t)L.R, nkb, SP_SA};
-    const uint32_t ba[4] = {SP_KB, SP_ROWS, 1, SP_SA};
-    int rc0 = make_tmap_u8_4d(ctx, &mapA[b], A[b], da, sta, ba, CU_TENSOR_MAP_SWIZZLE_64B);
+    const uint64_t st[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};
+    const uint64_t d[4] = {SP_KB, (uint64_t)L.R, nkb, (uint64_t)SP_SLOT * nw};
+    const uint32_t bx[4] = {SP_KB, SP_ROWS, 1, SP_SF};
+    int rc0 = make_tmap_u8_4d(ctx, &mapF[b], F[b], d, st, bx, CU_TENSOR_MAP_SWIZZLE_64B);
     if (rc0) return rc0;
-    const uint64_t db[4] = {SP_KB, (uint64_t)L.R, nkb, (uint64_t)SP_SB * nw};
-    const uint32_t bb[4] = {SP_KB, (uint32_t)(pair ? SP2_BROWS : SP_ROWS), 1, SP_SB};
-    rc0 = make_tmap_u8_4d(ctx, &mapB[b], B[b], db, sta, bb, CU_TENSOR_MAP_SWIZZLE_64B);
+    const uint32_t bh[4] = {SP_KB, SP2_BROWS, 1, SP_SF};
+    rc0 = make_tmap_u8_4d(ctx, &mapFh[b], F[b], d, st, bh, CU_TENSOR_MAP_SWIZZLE_64B);
     if (rc0) return rc0;
   }
   int rc = SPX_OK;
@@ -894,7 +756,7 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
     cfg.gridDim = dim3(2 * nclusters);
   }
 
-  // Preparation (column scales, weight maxima, digit planes) of slab s+1 runs on
+  // Preparation (column scales, weight statistics, digit planes) of slab s+1 runs on
   // the preparation stream while slab s accumulates on `stream`; buffer b = s % 2.
   const int64_t nslab = (P + L.Ps - 1) / L.Ps;
   cudaStream_t ps = ctx->prep_stream;
@@ -908,10 +770,10 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
     const int lenp = (int)align_up((size_t)len, SP_KB);
     const int nchunk = lenp / 16;  // 16-pair chunks; npad is a multiple of 64
     split_colmax_kernel<<<N, 256, 0, ps>>>(M, ldc, p0, len, sA[b]);
-    split_wmax_kernel<<<nw, 256, 0, ps>>>(W, ldw, p0, len, wmax[b]);
+    split_wstat_kernel<<<nw, 256, 0, ps>>>(W, ldw, p0, len, lenp, wmax[b], wsgn[b], G[b]);
     const int64_t nthr = (int64_t)npad * nchunk;
     split_quantize_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, ps>>>(
-        M, ldc, p0, len, nchunk, N, npad, L.R, L.Ps, W, ldw, nw, sA[b], wmax[b], A[b], B[b]);
+        M, ldc, p0, len, nchunk, N, npad, L.R, L.Ps, nw, sA[b], wsgn[b], G[b], F[b]);
     int r = check_cuda(ctx, cudaGetLastError(), "split operand preparation");
     if (r) return r;
     *launches += 3;
@@ -942,16 +804,17 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
     prm.nk = lenp / SP_KB;
     prm.sA = sA[b];
     prm.wmax = wmax[b];
+    prm.wsgn = wsgn[b];
     prm.out = reinterpret_cast<double*>(out);
     prm.npack = (int64_t)N * (N + 1) / 2;
     prm.status = ctx->d_status;
     prm.timeout_ns =
         (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
     if (pair) {
-      rc = check_cuda(ctx, cudaLaunchKernelEx(&cfg, split_gram2_kernel, mapA[b], mapB[b], prm),
+      rc = check_cuda(ctx, cudaLaunchKernelEx(&cfg, split_gram2_kernel, mapF[b], mapFh[b], prm),
                       "split_gram2_kernel launch");
     } else {
-      split_gram_kernel<<<grid, SP_THREADS, smem, stream>>>(mapA[b], mapB[b], prm);
+      split_gram_kernel<<<grid, SP_THREADS, smem, stream>>>(mapF[b], prm);
       rc = check_cuda(ctx, cudaGetLastError(), "split_gram_kernel launch");
     }
     if (rc) return rc;

@@ -42,6 +42,7 @@ struct spx_ctx {
     cudaGraph_t graph;
     cudaGraphExec_t exec;
     uint64_t last_use;
+    void* mem;  // device memory the graph's persistent schedule owns (or NULL)
   };
   std::vector<BatchGraph> graphs;
   uint64_t graph_clock = 0;

@@ -234,6 +234,12 @@ __device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
 }
 #endif
 
+// Host: a tiled tensor map of `rank` dims (dims[0] contiguous, strides[] the byte
+// strides of dims 1..rank-1) without a context: 0, -1 (no driver entry), or the
+// driver's error code.
+int encode_tmap(CUtensorMap* map, CUtensorMapDataType type, int rank, const void* base,
+                const uint64_t* dims, const uint64_t* strides, const uint32_t* box,
+                CUtensorMapSwizzle swz);
 // Host: builds a 3-D uint8 tiled tensor map (dims innermost first, byte strides of
 // dims 1 and 2) through the driver entry point. Returns 0 on success.
 int make_tmap_u8_3d(spx_ctx* ctx, CUtensorMap* map, const void* base, uint64_t d0, uint64_t d1,

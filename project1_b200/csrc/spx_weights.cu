@@ -3,6 +3,7 @@
 
 #include "spx_common.cuh"
 #include "spx_philox.h"
+#include "spx_split.cuh"
 
 namespace spx {
 
@@ -22,10 +23,8 @@ __global__ void weights_kernel(int64_t P, int64_t ldw, const double* __restrict_
     const int f = (int)(t / ldw);
     double v = 0.0;
     if (p < P) {
-      const double d = ediff[p];
-      const double om = omega[f];
       const double s = (wscale ? wscale[p] : 1.0) * scale_all;
-      v = -2.0 * d / (om * om + d * d) * s;
+      v = hilbert_none_weight(ediff[p], omega[f], s);
     }
     w[t] = v;
   }
@@ -39,6 +38,46 @@ int launch_weights(spx_ctx* ctx, int64_t P, int64_t ldw, const double* ediff,
   int grid = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 16);
   weights_kernel<<<grid, 256, 0, stream>>>(P, ldw, ediff, wscale, scale_all, nw, omega, w);
   return check_cuda(ctx, cudaGetLastError(), "weights_kernel launch");
+}
+
+// suscepc(i, j, f) += S1 + i S2 and suscepc(j, i, f) += conj(S1) + i conj(S2) for the
+// packed Hermitian sums S1 (weights wr) and S2 (weights wi) of element (i <= j): the
+// non-Hermitian real-frequency polarisation of src/susceptibility.f:1229-1235 (one
+// thread per packed element and frequency; each output element has one writer).
+__global__ void suscepc_combine_kernel(int N, int nw, const double2* __restrict__ S1,
+                                       const double2* __restrict__ S2, double2* __restrict__ out,
+                                       int64_t ldo) {
+  const int64_t npack = (int64_t)N * (N + 1) / 2;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < npack * nw;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int f = (int)(t / npack);
+    const int64_t p = t - (int64_t)f * npack;
+    int j = (int)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
+    while ((int64_t)j * (j + 1) / 2 > p) --j;
+    while ((int64_t)(j + 1) * (j + 2) / 2 <= p) ++j;
+    const int i = (int)(p - (int64_t)j * (j + 1) / 2);
+    const double2 a = S1[t], b = S2[t];
+    double2* of = out + (int64_t)f * ldo * N;
+    double2 v = of[(int64_t)j * ldo + i];
+    v.x += a.x - b.y;
+    v.y += a.y + b.x;
+    of[(int64_t)j * ldo + i] = v;
+    if (i != j) {
+      double2 u = of[(int64_t)i * ldo + j];
+      u.x += a.x + b.y;
+      u.y += b.x - a.y;
+      of[(int64_t)i * ldo + j] = u;
+    }
+  }
+}
+
+int launch_suscepc_combine(spx_ctx* ctx, int N, int nw, const double2* S1, const double2* S2,
+                           double2* out, int64_t ldo, cudaStream_t stream) {
+  const int64_t total = (int64_t)N * (N + 1) / 2 * nw;
+  if (total <= 0) return SPX_OK;
+  const int grid = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 16);
+  suscepc_combine_kernel<<<grid, 256, 0, stream>>>(N, nw, S1, S2, out, ldo);
+  return check_cuda(ctx, cudaGetLastError(), "suscepc_combine_kernel launch");
 }
 
 __global__ void scale_kernel(double* z, int64_t n2, double factor) {

@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "spx_common.cuh"
+#include "spx_zgemm.h"
 
 namespace spx {
 
@@ -42,27 +43,7 @@ constexpr int ZG_KC = 16;            // K per pipeline stage
 constexpr int ZG_ROW = ZG_KC + 4;    // padded shared row, double2 units
 constexpr int ZG_THREADS = 128;
 
-struct ZgParams {
-  // A_b(m, k) = A[b1*sA1 + b2*sA2 + m*lda + k], or with a_mcontig
-  // A[b1*sA1 + b2*sA2 + m + k*lda] (a Fortran column-major panel)
-  const double2* A;
-  int64_t lda, sA1, sA2;
-  int a_mcontig;
-  // B_b(col, k) = B[b1*sB1 + b2*sB2 + colOff(col) + kOff(k)], col = n*ncin + c,
-  // colOff = n*sBn + (cOff ? cOff[c] : c*sBc), kOff = kOff ? kOff[k] : k
-  const double2* B;
-  int64_t sB1, sB2, sBn, sBc;
-  const int64_t* cOff;
-  const int* kOff;
-  // O_b(m, col) = O[b1*sO1 + b2*sO2 + m + n*sOn + c*sOc]
-  double2* O;
-  int64_t sO1, sO2, sOn, sOc;
-  const double2* alpha;  // per b1, or null: alpha_v
-  double2 alpha_v;
-  int M, ncol, ncin, K, nb1;
-  int K_last;  // K of the last batch when > 0 (split-K over batches)
-  int mtiles, ntiles;
-};
+// ZgParams: see spx_zgemm.h
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
@@ -216,7 +197,7 @@ __global__ void __launch_bounds__(ZG_THREADS, 2) zgemm_gather_kernel(ZgParams pr
     }
 }
 
-static int launch_zgemm(spx_ctx* ctx, ZgParams prm, int nbatch, cudaStream_t s) {
+int launch_zgemm(spx_ctx* ctx, ZgParams prm, int nbatch, cudaStream_t s) {
   if (prm.M <= 0 || prm.ncol <= 0 || prm.K <= 0 || nbatch <= 0) return SPX_OK;
   prm.mtiles = (prm.M + ZG_B - 1) / ZG_B;
   prm.ntiles = (prm.ncol + ZG_B - 1) / ZG_B;

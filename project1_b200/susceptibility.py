@@ -72,6 +72,7 @@ class Context:
             raise SpexGpuError(rc, f"spx_ctx_create: {_lib.strerror(rc)}")
         self.handle = h
         self.device = device
+        self.split_variant = split_variant
 
     def close(self) -> None:
         if getattr(self, "handle", None):
@@ -194,6 +195,23 @@ class Context:
         self._check(rc, "spx_chi0_accumulate_w_dev")
         return _stats(st) if st is not None else None
 
+    def chi0_accumulate_c_dev(self, cprod, wr, wi, suscepc, precision: str = "fp64",
+                              npair: Optional[int] = None, stream=None, stats: bool = False):
+        """Real-frequency suscepc += sum_p cprod(p,i) conj(cprod(p,j)) (wr + i wi)(p,f), full
+        matrix: suscepc complex128 (nw, nbas, ldo) row-major == Fortran (ldo, nbas, nw);
+        wr, wi (nw, ldw)."""
+        nbas, ldc = cprod.shape
+        nw, ldw = wr.shape
+        ldo = suscepc.shape[2]
+        npair = ldc if npair is None else npair
+        st = _lib.spx_chi0_stats() if stats else None
+        rc = self.lib.spx_chi0_accumulate_c_dev(self.handle, _ptr(cprod), ldc, npair, nbas, _ptr(wr),
+                                                _ptr(wi), ldw, nw, PRECISIONS[precision], _ptr(suscepc),
+                                                ldo, torch_stream(stream, suscepc),
+                                                C.byref(st) if st is not None else None)
+        self._check(rc, "spx_chi0_accumulate_c_dev")
+        return _stats(st) if st is not None else None
+
     # ---- q -> 0 head and wings -------------------------------------------------------
 
     def headwings_dev(self, cprod, dcprod, w, head, wing, npair: Optional[int] = None,
@@ -268,6 +286,12 @@ class Context:
         self._check(rc, "spx_chi0_batched")
         return _stats(st) if st is not None else None
 
+    def measure_dmma_peak(self) -> float:
+        """The device's FP64 tensor (DMMA) peak in TFLOP/s, measured by the library."""
+        v = C.c_double()
+        self._check(self.lib.spx_measure_dmma_peak(self.handle, C.byref(v)), "spx_measure_dmma_peak")
+        return v.value
+
     def autotune_split(self, nbas: int, npair: int, nw: int) -> dict:
         e = _lib.spx_tune_entry()
         self._check(self.lib.spx_autotune_split(self.handle, nbas, npair, nw, C.byref(e)),
@@ -277,6 +301,17 @@ class Context:
     def tune_lookup(self, nbas: int, npair: int, nw: int) -> Optional[dict]:
         e = _lib.spx_tune_entry()
         rc = self.lib.spx_tune_lookup(self.handle, nbas, npair, nw, C.byref(e))
+        return _stats(e) if rc == 0 else None
+
+    def autotune_batched(self, nbas: int, npair: int, nw: int) -> dict:
+        e = _lib.spx_tune_entry()
+        self._check(self.lib.spx_autotune_batched(self.handle, nbas, npair, nw, C.byref(e)),
+                    "spx_autotune_batched")
+        return _stats(e)
+
+    def tune_lookup_batched(self, nbas: int, npair: int, nw: int) -> Optional[dict]:
+        e = _lib.spx_tune_entry()
+        rc = self.lib.spx_tune_lookup_batched(self.handle, nbas, npair, nw, C.byref(e))
         return _stats(e) if rc == 0 else None
 
     def tune_save(self, path: str) -> None:

@@ -1,4 +1,5 @@
-"""Many q points in one graph launch (K7) and the split-path autotuner."""
+"""Many q points in one launch (K7): the persistent split schedule, the per-slab
+kernel schedule, and the autotuners."""
 import json
 
 import numpy as np
@@ -67,7 +68,10 @@ def test_batched_equals_per_q_calls(ctx, generated, precision):
     omega = torch.from_numpy(inputs.frequencies(3)).to(DEV)
     qs = [_q(n, p, 3, i, generated) for i, (n, p) in enumerate(SHAPES)]
     st = ctx.chi0_batched(qs, omega, precision=precision, stats=True)
-    assert st["kernel_launches"] > len(qs)
+    if precision == "split":
+        assert st["kernel_launches"] == 1       # one persistent kernel for the whole batch
+    else:
+        assert st["kernel_launches"] > len(qs)
     for q in qs:
         ref = _per_q_reference(ctx, q, omega, precision)
         assert torch.equal(q["susceph"], ref), (q["nbas"], q["npair"])
@@ -149,7 +153,8 @@ def test_autotuned_batch(ctx):
     qs = [_q(n, p, 2, 40 + i, True, variant=0, slab=0) for i, (n, p) in enumerate([(260, 20000), (520, 9000)])]
     ctx.chi0_batched(qs, omega, flags=_lib.SPX_BATCH_AUTOTUNE, stats=True)
     for q in qs:
-        assert ctx.tune_lookup(q["nbas"], q["npair"], 2) is not None
+        t = ctx.tune_lookup_batched(q["nbas"], q["npair"], 2)
+        assert t is not None and t["variant"] == 3 and t["tile"] in (64 + 3 * 256, 32 + 3 * 256, 32 + 4 * 256)
         assert torch.isfinite(torch.view_as_real(q["susceph"])).all()
         assert q["susceph"].abs().max() > 0
 
@@ -163,3 +168,58 @@ def test_batched_rejects_bad_descriptors(ctx):
         ctx.chi0_batched([dict(q, npair=200)], omega)       # ldc 105 < npair
     with pytest.raises(SpexGpuError):
         ctx.chi0_batched([dict(q, nbas=50000)], omega)
+
+
+def _force_tile(c, tmp_path, qs, nw, tile, slab):
+    """Loads a tuning table that assigns `tile` and `slab` to the buckets of `qs`."""
+    ents = []
+    for q in qs:
+        n, p = q["nbas"], q["npair"]
+        ents.append({"nbas_bucket": (n + 127) // 128, "npair_bucket": 0 if p <= 16384 else (1 if p <= 32768 else 2),
+                     "nw": nw, "variant": 3, "slab_pairs": slab, "tile": tile, "tflops": 1.0})
+    path = tmp_path / f"tile{tile}.json"
+    path.write_text(json.dumps({"format": "spexgpu-tune-1", "entries": ents}))
+    c.tune_load(path)
+
+
+@pytest.mark.parametrize("tile", [64 + 3 * 256, 32 + 3 * 256, 32 + 4 * 256])
+def test_persistent_tile_shapes_equal_per_q_calls(tmp_path, tile):
+    """Every tile shape of the persistent schedule gives the per-q result bit for bit,
+    with the slab ring reused many times (4096-pair slabs, 3 buffers) and a q whose
+    weights change sign (negative energy differences)."""
+    omega = torch.from_numpy(inputs.frequencies(3)).to(DEV)
+    with spx.Context(0) as c:
+        qs = [_q(n, p, 3, 60 + i, gen, slab=0) for i, (n, p, gen) in
+              enumerate([(130, 60000, True), (65, 9000, False), (200, 20000, True)])]
+        qs[1]["ediff"][::7] *= -1.0
+        _force_tile(c, tmp_path, qs, 3, tile, 4096)
+        st = c.chi0_batched(qs, omega, stats=True)
+        assert st["kernel_launches"] == 1
+        for q in qs:
+            ref = torch.zeros_like(q["susceph"])
+            cp = q.get("cprod")
+            if cp is None:
+                cp = torch.empty((q["nbas"], q["npair"]), dtype=torch.complex128, device=DEV)
+                c.gen_cmatrix_dev(q["seed"], q["stream_id"], cp, q["npair"], scale=q["m_scale"])
+            c.synchronize()
+            torch.cuda.synchronize()
+            with spx.Context(0, split_variant=1) as c1:
+                for p0 in range(0, q["npair"], 4096):
+                    # slab by slab, as the persistent schedule cuts them
+                    n = min(4096, q["npair"] - p0)
+                    c1.chi0_accumulate_dev(cp[:, p0:p0 + n].contiguous(), q["ediff"][p0:p0 + n].contiguous(),
+                                           omega, ref, scale_all=q["scale_all"], precision="split", stats=True)
+            assert torch.equal(q["susceph"], ref), (tile, q["nbas"], q["npair"])
+
+
+def test_persistent_and_kernel_schedules_agree(ctx):
+    omega = torch.from_numpy(inputs.frequencies(2)).to(DEV)
+    qs = [_q(n, p, 2, 80 + i, True) for i, (n, p) in enumerate([(90, 40000), (300, 5000)])]
+    ctx.chi0_batched(qs, omega, stats=True)
+    a = [q["susceph"].clone() for q in qs]
+    for q in qs:
+        q["susceph"].zero_()
+    st = ctx.chi0_batched(qs, omega, flags=_lib.SPX_BATCH_KERNELS, stats=True)
+    assert st["kernel_launches"] > 1
+    for q, x in zip(qs, a):
+        assert torch.equal(q["susceph"], x)

@@ -177,3 +177,12 @@ def test_bounded_wait_reports_timeout_and_context_survives():
         c.chi0_accumulate(m, d, om, out)
         emax, _ = normalized_error(out, ref, 40)
         assert emax <= FP64_TOL
+
+
+def test_measured_dmma_peak_is_plausible():
+    """The FP64 tensor peak the bench divides by: B200's DMMA path is rated about
+    40 TFLOP/s, so the measured value must lie in a plausible band."""
+    with spx.Context(0) as c:
+        v = c.measure_dmma_peak()
+    print(f"measured DMMA peak: {v:.1f} TFLOP/s")
+    assert 10.0 < v < 120.0, v

@@ -35,7 +35,8 @@ def _d(a):
     return torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
 
 
-@pytest.mark.parametrize("nbas,nw,invert", [(50, 2, False), (50, 2, True), (300, 3, True), (1, 1, True), (129, 1, True)])
+@pytest.mark.parametrize("nbas,nw,invert", [(50, 2, False), (50, 2, True), (300, 3, True), (1, 1, True), (129, 1, True),
+                                            (64, 2, True), (700, 4, True)])
 def test_dielec_matches_oracle(ctx, nbas, nw, invert):
     chi, coul = _chi(nbas, nw, seed=nbas)
     ref = oracle.dielec(chi, coul, invert)
@@ -68,3 +69,15 @@ def test_dielec_rejects_indefinite(ctx):
     sus = _d(chi.T)
     with pytest.raises(SpexGpuError, match="frequency 0"):
         ctx.dielec_dev(sus, _d(np.ones(nbas)), invert=True)
+
+
+def test_dielec_reports_the_indefinite_frequency(ctx):
+    """Only the second frequency's eps is indefinite (its pivot fails in a later block):
+    the error names that frequency."""
+    nbas = 150
+    chi, coul = _chi(nbas, 2, seed=5)
+    chi[:, 1] = 0.0
+    for j in range(nbas):
+        chi[j * (j + 1) // 2 + j, 1] = 0.0 if j < 100 else 3.0 / coul[j]     # eps_jj = 1 - 3 for j >= 100
+    with pytest.raises(SpexGpuError, match="frequency 1"):
+        ctx.dielec_dev(_d(chi.T), _d(coul), invert=True)

@@ -84,3 +84,35 @@ def test_hilbert_path_reproduces_hilbert_none(ctx):
     ctx.chi0_accumulate_dev(_d(m.T), _d(ediff), _d(omega), b, scale_all=1.0 / w.nk, stats=True)
     emax, _ = normalized_error(a.cpu().numpy().T, b.cpu().numpy().T, w.nbas)
     assert emax <= 5e-3, emax
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("split", 1e-6)])
+def test_real_frequency_suscepc_matches_oracle(ctx, precision, tol):
+    """Real frequencies (suscepc): Hilbert weights wghtSr / wghtSi of real frequencies
+    from getwghtS, contracted with tetrahedron weights on the device, then the full
+    non-Hermitian matrix against the reference loop restated (:1182-1235)."""
+    rng = np.random.default_rng(21)
+    nbas, P, nw = 70, 3001, 4
+    frqs = np.concatenate([[0.0], np.geomspace(0.05, 60.0, 120)])
+    frqc = np.array([0.0, 1.3, 7.7, 25.0]) + 0j            # real frequencies
+    wsr, wsi = oracle.getwghtS(frqc, frqs, 0.01, 0, 0)
+    assert np.abs(wsi).max() > 0                            # the imaginary part matters
+    wt = rng.uniform(0, 1, (P, frqs.size)) * (rng.uniform(0, 1, (P, frqs.size)) > 0.9)
+    wr_ref = oracle.hilbert_weights(wt, wsr, scale_all=0.5)
+    wi_ref = oracle.hilbert_weights(wt, wsi, scale_all=0.5)
+    m = np.asfortranarray((rng.standard_normal((P, nbas)) + 1j * rng.standard_normal((P, nbas))) / np.sqrt(nbas))
+    ref = oracle.chi0_realfreq(m, wr_ref, wi_ref)            # (nbas, nbas, nw)
+    wrd = torch.zeros((nw, P), dtype=torch.float64, device=DEV)
+    wid = torch.zeros((nw, P), dtype=torch.float64, device=DEV)
+    ctx.weights_hilbert_dev(_d(wt.T), _d(wsr.T), wrd, scale_all=0.5)
+    ctx.weights_hilbert_dev(_d(wt.T), _d(wsi.T), wid, scale_all=0.5)
+    ldo = nbas + 3
+    out = torch.zeros((nw, nbas, ldo), dtype=torch.complex128, device=DEV)
+    st = ctx.chi0_accumulate_c_dev(_d(m.T), wrd, wid, out, precision=precision, stats=True)
+    assert st["kernel_launches"] >= 3
+    got = np.transpose(out.cpu().numpy()[:, :, :nbas], (2, 1, 0))   # (i, j, f)
+    scale = np.sqrt(np.einsum("pi,pf->if", np.abs(m) ** 2, np.abs(wr_ref) + np.abs(wi_ref)))
+    err = np.abs(got - ref) / (scale[:, None, :] * scale[None, :, :])
+    assert err.max() <= tol, err.max()
+    # the padding rows of suscepc are untouched
+    assert out[:, :, nbas:].abs().max().item() == 0.0

@@ -99,3 +99,15 @@ def test_hilbert_weights_threshold():
     a = oracle.hilbert_weights(wt, ws, thr=0.3, scale_all=0.5)
     b = 0.5 * np.where(wt > 0.3, wt, 0) @ ws
     assert np.allclose(a, b)
+
+
+def test_realfreq_restatement_is_the_complex_weighted_gram():
+    """The suscepc loop of the reference (two real sums per weight part, combined into
+    (i,j) and (j,i)) equals sum_p M_i conj(M_j) (wr + i wi) for every i, j."""
+    rng = np.random.default_rng(0)
+    P, N, nw = 60, 9, 3
+    m = rng.standard_normal((P, N)) + 1j * rng.standard_normal((P, N))
+    wr, wi = rng.standard_normal((P, nw)), rng.standard_normal((P, nw))
+    got = oracle.chi0_realfreq(m, wr, wi)
+    direct = np.einsum("pi,pj,pf->ijf", m, np.conj(m), wr + 1j * wi)
+    assert np.abs(got - direct).max() <= 1e-12 * np.abs(direct).max()
