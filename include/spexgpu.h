@@ -130,6 +130,17 @@ int spx_chi0_accumulate_dev(spx_ctx* ctx, const double* cprod, int64_t ldc,
                             int32_t nw, const double* omega, int32_t precision,
                             double* susceph, void* stream, spx_chi0_stats* stats);
 
+/* The -DINV build (spex.inv: MCOMPLEX_dp = real_dp, src/cppmacro.h:53-64): real
+ * cprod (ldc, nbas) and real packed susceph (nbas(nbas+1)/2, nw), with
+ * re(k) = cprod(k,i) * cprod(k,j) (src/susceptibility.f:1197),
+ *   susceph(ij, f) += sum_p cprod(p, i) cprod(p, j) w(p, f),  ij = j(j+1)/2 + i.
+ * Device arrays; the weights, precision and stream as spx_chi0_accumulate_dev. */
+int spx_chi0_accumulate_real_dev(spx_ctx* ctx, const double* cprod, int64_t ldc,
+                                 int64_t npair, int32_t nbas,
+                                 const double* ediff, const double* wscale, double scale_all,
+                                 int32_t nw, const double* omega, int32_t precision,
+                                 double* susceph, void* stream, spx_chi0_stats* stats);
+
 /* Allocation-free FP64 accumulation; no counterpart in the reference.
  * For callers that cannot call cudaMalloc, such as a Fortran host whose device
  * memory belongs to its OpenMP/OpenACC offload runtime or to a pool allocator.
@@ -272,6 +283,18 @@ int spx_headwings_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t np
 int spx_trafo_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
                   int32_t nbas, const double* ctrafo, int64_t ldt, int32_t dim,
                   double* out, int64_t ldo, void* stream);
+
+/* The same transform for the basis without FULLPW (src/susceptibility.f:814-824):
+ * wavefproducts then returns <M~ phi|phi>, so the interstitial rows of ctrafo are
+ * first multiplied by the plane-wave overlap (olapvec, src/overlap.f:298-316),
+ *   ctrafo1(nbasp + i, j) = sum_k conj(cstep(G_k - G_i)) ctrafo(nbasp + k, j),
+ * G = pw->gptm (the ngptm MPB plane waves, nbas = nbasp + ngptm), with pw->cstep on
+ * its box (differences outside it count as 0); the muffin-tin rows are unchanged,
+ * and out = conj(conj(cprod) * ctrafo1) as spx_trafo_dev. */
+int spx_trafo_olap_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
+                       int32_t nbas, int32_t nbasp, const double* ctrafo, int64_t ldt,
+                       int32_t dim, const spx_pw_desc* pw, double* out, int64_t ldo,
+                       void* stream);
 
 /* ---- dielectric matrix and its inverse (FP64) ------------------------------
  * Replaces src/correlation.f:614-636 and :703-745 for the imaginary frequencies: in

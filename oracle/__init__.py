@@ -209,6 +209,35 @@ def trafo(cprod, ctrafo, dim=None):
     return np.conj(np.conj(c) @ t[:, :dim])
 
 
+def olapvec(vec, gpt, cstep, sr):
+    """src/overlap.f:298-316: out(i) = dotprod(row, vec) with row(j) = cstep(G_j - G_i)
+    and dotprod the conjugating zdotc (src/wrapper.f:369-377); cstep on [-sr, sr]^3
+    (x fastest), zero outside."""
+    g = np.asarray(gpt)
+    cs = np.asarray(cstep).reshape((2 * sr + 1,) * 3, order="F")
+    out = np.zeros(len(g), dtype=complex)
+    for i in range(len(g)):
+        row = np.zeros(len(g), dtype=complex)
+        for j in range(len(g)):
+            d = g[j] - g[i]
+            if np.all(np.abs(d) <= sr):
+                row[j] = cs[d[0] + sr, d[1] + sr, d[2] + sr]
+        out[i] = np.vdot(row, vec)
+    return out
+
+
+def trafo_olap(cprod, ctrafo, nbasp, gptm, cstep, sr, dim=None):
+    """The non-FULLPW branch of src/susceptibility.f:814-824: ctrafo1 = ctrafo with its
+    interstitial rows replaced by olapvec of each column, then
+    cprod(:, :dim) = conj(matmul(conj(cprod), ctrafo1))."""
+    t = np.array(ctrafo, dtype=complex)
+    dim = t.shape[1] if dim is None else dim
+    t1 = t[:, :dim].copy()
+    for c in range(dim):
+        t1[nbasp:, c] = olapvec(t[nbasp:, c], gptm, cstep, sr)
+    return np.conj(np.conj(np.asarray(cprod)) @ t1)
+
+
 def _ln(z: complex) -> complex:
     """Principal logarithm as src/hilbert.f:283-296 defines it: a real negative argument
     gives +i pi whatever the sign of its zero imaginary part."""
@@ -377,3 +406,20 @@ def chi0_realfreq(cprod, wr, wi, suscepc=None) -> np.ndarray:
         lower = (sus1 + susc2) + 1j * (susc1 - sus2)
         suscepc[j, :j, :] += lower[:j]
     return suscepc
+
+
+def chi0_real(cprod, w, susceph=None) -> np.ndarray:
+    """The -DINV body loop (src/susceptibility.f:1182-1240 with MCOMPLEX_dp = real_dp):
+    re(k) = cprod(k,i) * cprod(k,j) (:1197), sus1 = ddot(re, wghtSr(:, f)) (:1781),
+    susceph(j(j+1)/2 + i, f) += sus1 (:1210), vectorised over i for each j with the
+    products summed in long double. Returns (npack, nw) float64."""
+    cprod = np.asarray(cprod, dtype=np.float64)
+    w = np.asarray(w, dtype=np.longdouble)
+    npair, nbas = cprod.shape
+    nw = w.shape[1]
+    if susceph is None:
+        susceph = np.zeros((nbas * (nbas + 1) // 2, nw), dtype=np.float64, order="F")
+    for j in range(nbas):
+        re = cprod[:, : j + 1].astype(np.longdouble) * cprod[:, j].astype(np.longdouble)[:, None]
+        susceph[j * (j + 1) // 2: j * (j + 1) // 2 + j + 1] += (re.T @ w).astype(np.float64)
+    return susceph

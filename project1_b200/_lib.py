@@ -109,6 +109,10 @@ SIGNATURES = {
         C.c_int,
         [_P, _P, _I64, _I64, _I32, _P, _P, C.c_double, _I32, _P, _I32, _P, _P, C.POINTER(spx_chi0_stats)],
     ),
+    "spx_chi0_accumulate_real_dev": (
+        C.c_int,
+        [_P, _P, _I64, _I64, _I32, _P, _P, C.c_double, _I32, _P, _I32, _P, _P, C.POINTER(spx_chi0_stats)],
+    ),
     "spx_scale_dev": (C.c_int, [_P, _P, _I64, C.c_double, _P]),
     "spx_chi0_accumulate_dev_noalloc": (
         C.c_int, [_P, _I64, _I64, _I32, _P, _P, C.c_double, _I32, _P, _P, _P]),
@@ -134,6 +138,8 @@ SIGNATURES = {
     "spx_selftest_wait_dev": (C.c_int, [_P, _I32]),
     "spx_measure_dmma_peak": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "spx_trafo_dev": (C.c_int, [_P, _P, _I64, _I64, _I32, _P, _I64, _I32, _P, _I64, _P]),
+    "spx_trafo_olap_dev": (C.c_int, [_P, _P, _I64, _I64, _I32, _I32, _P, _I64, _I32,
+                                     C.POINTER(spx_pw_desc), _P, _I64, _P]),
     "spx_chi0_batched": (
         C.c_int, [_P, _I32, C.POINTER(spx_q_desc), _I32, _P, _I32, _I32, _P, C.POINTER(spx_chi0_stats)]),
     "spx_autotune_split": (C.c_int, [_P, _I32, _I64, _I32, C.POINTER(spx_tune_entry)]),

@@ -37,6 +37,11 @@ int launch_chi0_fp64(spx_ctx*, const double2*, int64_t, int64_t, int, const doub
 int split_chi0_slab(spx_ctx*, const double2*, int64_t, int64_t, int, const double*, int64_t,
                     int, double2*, void*, size_t, cudaStream_t, int*, int variant, int slab);
 size_t split_workspace_bytes(int64_t P, int N, int nw);
+size_t split_workspace_bytes_real(int64_t P, int N, int nw);
+int split_chi0_real_slab(spx_ctx*, const double*, int64_t, int64_t, int, const double*, int64_t,
+                         int, double*, void*, size_t, cudaStream_t, int*);
+int launch_chi0_fp64_real(spx_ctx*, const double*, int64_t, int64_t, int, const double*, int64_t,
+                          int, double*, cudaStream_t);
 
 void timing_mark(spx_ctx* ctx, cudaStream_t s, int kind) {
   if (!ctx->timing) return;
@@ -385,6 +390,73 @@ extern "C" int spx_chi0_accumulate_dev(spx_ctx* ctx, const double* cprod, int64_
   if (rc) return rc;
   if (stats) {
     rc = collect_status(ctx, s, "chi0_accumulate_dev");
+    if (rc) return rc;
+    timing_collect(ctx, &stats->ms_prep, &stats->ms_gram);
+    stats->kernel_launches = launches;
+    stats->ms_total =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return SPX_OK;
+}
+
+// -DINV build: real cprod and real packed susceph (MCOMPLEX_dp = real_dp,
+// src/cppmacro.h:53-64; re(k) = cprod(k,i)*cprod(k,j), src/susceptibility.f:1197).
+extern "C" int spx_chi0_accumulate_real_dev(spx_ctx* ctx, const double* cprod, int64_t ldc,
+                                            int64_t npair, int32_t nbas, const double* ediff,
+                                            const double* wscale, double scale_all, int32_t nw,
+                                            const double* omega, int32_t precision,
+                                            double* susceph, void* stream, spx_chi0_stats* stats) {
+  int rc = check_chi0_args(ctx, cprod, ldc, npair, nbas, ediff, nw, omega, precision, susceph);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  auto t0 = std::chrono::steady_clock::now();
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->precision = precision;
+    stats->flops = 2.0 * (double)nbas * nbas * (double)npair * nw;
+  }
+  if (npair == 0 || nbas == 0 || nw == 0) return SPX_OK;
+  cudaStream_t s = pick_stream(ctx, stream);
+  const int64_t ldw = (int64_t)align_up((size_t)npair, 16);
+  const size_t wbytes = align_up(sizeof(double) * (size_t)ldw * nw, 256);
+  const size_t sbytes = precision == SPX_SPLIT ? split_workspace_bytes_real(npair, nbas, nw) : 0;
+  // the FP64 kernel streams M with 2-D tensor copies: columns must start on 16 bytes,
+  // otherwise M goes through an aligned copy first
+  const bool realign = precision == SPX_FP64 && ((ldc & 1) || ((uintptr_t)cprod & 15));
+  const int64_t ldm = realign ? (int64_t)align_up((size_t)npair, 2) : ldc;
+  const size_t mbytes = realign ? align_up(sizeof(double) * (size_t)ldm * nbas, 256) : 0;
+  if ((rc = ensure_workspace(ctx, wbytes + sbytes + mbytes))) return rc;
+  double* W = (double*)ctx->ws;
+  void* sws = (char*)ctx->ws + wbytes;
+  const double* M = cprod;
+  if (realign) {
+    double* Mc = (double*)((char*)ctx->ws + wbytes + sbytes);
+    if ((rc = check_cuda(ctx, cudaMemcpy2DAsync(Mc, sizeof(double) * ldm, cprod, sizeof(double) * ldc,
+                                                sizeof(double) * npair, nbas, cudaMemcpyDeviceToDevice, s),
+                         "align cprod")))
+      return rc;
+    M = Mc;
+  }
+  int launches = 0;
+  ctx->timing = stats != nullptr;
+  ctx->nmarks = 0;
+  timing_mark(ctx, s, 0);
+  rc = launch_weights(ctx, npair, ldw, ediff, wscale, scale_all, nw, omega, W, s);
+  ++launches;
+  if (!rc) {
+    if (precision == SPX_FP64) {
+      timing_mark(ctx, s, 1);
+      rc = launch_chi0_fp64_real(ctx, M, ldm, npair, nbas, W, ldw, nw, susceph, s);
+      ++launches;
+    } else {
+      rc = split_chi0_real_slab(ctx, M, ldm, npair, nbas, W, ldw, nw, susceph, sws, sbytes, s, &launches);
+    }
+  }
+  timing_mark(ctx, s, 2);
+  ctx->timing = false;
+  if (rc) return rc;
+  if (stats) {
+    rc = collect_status(ctx, s, "chi0_accumulate_real_dev");
     if (rc) return rc;
     timing_collect(ctx, &stats->ms_prep, &stats->ms_gram);
     stats->kernel_launches = launches;

@@ -350,6 +350,180 @@ int launch_chi0_fp64_noctx(int num_sms, int* status, uint64_t timeout_ns, const 
 
 namespace spx {
 
+// ---------------------------------------------------------------------------
+// K1r: the -DINV build (MCOMPLEX_dp = real_dp, src/cppmacro.h:53-64), where
+// re(k) = cprod(k,i) * cprod(k,j) (src/susceptibility.f:1197) and chi is real:
+//   chi_f(i, j) += sum_p M(p, i) M(p, j) w(p, f),  i <= j,
+// on the same pipeline as K1 with one 2-D TMA box of 16 pairs x 64 columns per
+// panel and stage (128-byte rows, SWIZZLE_128B: pair k of row r sits in 16-byte
+// chunk (k/2) ^ (r & 7)), and one DMMA per 8 x 8 real product.
+typedef double F64RBox[F64_B][F64_KC];
+
+struct __align__(1024) F64RSmem {
+  F64RBox a[F64_ST];
+  F64RBox b[F64_ST];
+  double w[F64_ST][F64_KC];
+  uint64_t full[F64_ST];
+  uint64_t empty[F64_ST];
+};
+
+__device__ __forceinline__ double f64r_at(const F64RBox& box, int r, int k) {
+  return box[r][(((k >> 1) ^ (r & 7)) << 1) | (k & 1)];
+}
+
+__global__ void __launch_bounds__(F64_THREADS, 2)
+    chi0_fp64_real_kernel(const __grid_constant__ CUtensorMap mapM, F64Params prm, double* outr) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  F64RSmem& sm = *reinterpret_cast<F64RSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                              ~(uintptr_t)1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < F64_ST; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], F64_WARPS);
+    }
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const int64_t nchunk = (prm.P + F64_KC - 1) / F64_KC;
+  const int64_t my_items = prm.nitems > blockIdx.x
+                               ? (prm.nitems - blockIdx.x + gridDim.x - 1) / gridDim.x
+                               : 0;
+  const int64_t total = my_items * nchunk;
+  auto chunk_item = [&](int64_t c) { return blockIdx.x + (c / nchunk) * (int64_t)gridDim.x; };
+  auto chunk_p0 = [&](int64_t c) { return (c % nchunk) * (int64_t)F64_KC; };
+  auto issue = [&](int64_t c) {
+    const int st = (int)(c % F64_ST);
+    const int64_t item = chunk_item(c), p0 = chunk_p0(c);
+    const int f = (int)(item / prm.ntile);
+    int bi, bj;
+    decode_tile((int)(item % prm.ntile), &bi, &bj);
+    const bool same = bi == bj;
+    mbar_arrive_expect_tx(&sm.full[st], (uint32_t)((same ? 1 : 2) * sizeof(F64RBox) + F64_KC * 8));
+    tma_load_2d(&sm.a[st][0][0], &mapM, (int)p0, bi * F64_B, &sm.full[st]);
+    if (!same) tma_load_2d(&sm.b[st][0][0], &mapM, (int)p0, bj * F64_B, &sm.full[st]);
+    bulk_g2s(&sm.w[st][0], prm.W + (int64_t)f * prm.ldw + p0, F64_KC * 8, &sm.full[st]);
+  };
+  int64_t issued = total < F64_ST - 1 ? total : (int64_t)(F64_ST - 1);
+  if (warp == 0 && lane == 0)
+    for (int64_t c = 0; c < issued; ++c) issue(c);
+
+  const int wi = warp & 1, wj = warp >> 1;
+  const int g = lane >> 2, t = lane & 3;
+  double acc[2][4][4];
+  bool failed = false;
+  int64_t c = 0;
+  for (; c < total; ++c) {
+    const int st = (int)(c % F64_ST);
+    const uint32_t ph = (uint32_t)((c / F64_ST) & 1);
+    const int64_t item = chunk_item(c), p0 = chunk_p0(c);
+    int bi, bj;
+    decode_tile((int)(item % prm.ntile), &bi, &bj);
+    if (p0 == 0) {
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) acc[mt][nt][r] = 0.0;
+    }
+    if (warp == 0 && c + F64_ST - 1 < total) {
+      const int64_t prev = c - 1;
+      int ok = 1;
+      if (lane == 0) {
+        if (prev >= 0)
+          ok = mbar_wait(&sm.empty[(int)(prev % F64_ST)], (uint32_t)((prev / F64_ST) & 1),
+                         prm.timeout_ns, prm.status);
+        if (ok) issue(c + F64_ST - 1);
+      }
+      if (!__shfl_sync(0xffffffffu, ok, 0)) {
+        failed = true;
+        break;
+      }
+      issued = c + F64_ST;
+    }
+    if (!mbar_wait(&sm.full[st], ph, prm.timeout_ns, prm.status)) {
+      failed = true;
+      break;
+    }
+    const F64RBox& A = sm.a[st];
+    const F64RBox& B = bi == bj ? sm.a[st] : sm.b[st];
+#pragma unroll
+    for (int ks = 0; ks < F64_KC / 8; ++ks) {
+      const double w0 = sm.w[st][8 * ks + t], w1 = sm.w[st][8 * ks + t + 4];
+      double bq[4][2];
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int r = 32 * wj + 8 * nt + g;
+        bq[nt][0] = w0 * f64r_at(B, r, 8 * ks + t);
+        bq[nt][1] = w1 * f64r_at(B, r, 8 * ks + t + 4);
+      }
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        double a[4];
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+            a[2 * q + h] = f64r_at(A, 32 * wi + 16 * mt + g + 8 * h, 8 * ks + t + 4 * q);
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) dmma<8>(acc[mt][nt], a, bq[nt]);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sm.empty[st]);
+    if (p0 + F64_KC >= prm.P) {
+      const int f = (int)(item / prm.ntile);
+      double* of = outr + (int64_t)f * prm.npack;
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const int i = bi * F64_B + 32 * wi + 16 * mt + g + 8 * (r >> 1);
+            const int j = bj * F64_B + 32 * wj + 8 * nt + 2 * t + (r & 1);
+            if (i <= j && j < prm.N) of[(int64_t)j * (j + 1) / 2 + i] += acc[mt][nt][r];
+          }
+    }
+  }
+  if (failed && warp == 0 && lane == 0) {
+    for (int64_t k = c; k < issued; ++k)
+      mbar_drain(&sm.full[(int)(k % F64_ST)], (uint32_t)((k / F64_ST) & 1), prm.timeout_ns);
+  }
+}
+
+// Enqueues K1r over one slab of real band-pair products M (ldc, N).
+int launch_chi0_fp64_real(spx_ctx* ctx, const double* M, int64_t ldc, int64_t P, int N,
+                          const double* W, int64_t ldw, int nw, double* out, cudaStream_t stream) {
+  if (P <= 0 || N <= 0 || nw <= 0) return SPX_OK;
+  const int nblk = (N + F64_B - 1) / F64_B;
+  F64Params prm;
+  prm.P = P;
+  prm.N = N;
+  prm.W = W;
+  prm.ldw = ldw;
+  prm.nw = nw;
+  prm.out = nullptr;
+  prm.npack = (int64_t)N * (N + 1) / 2;
+  prm.ntile = nblk * (nblk + 1) / 2;
+  prm.nitems = (int64_t)prm.ntile * nw;
+  prm.status = ctx->d_status;
+  prm.timeout_ns = (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
+  CUtensorMap map;
+  const uint64_t dims[2] = {(uint64_t)P, (uint64_t)N};
+  const uint64_t strides[1] = {(uint64_t)ldc * 8};
+  const uint32_t box[2] = {F64_KC, F64_B};
+  const int e = encode_tmap(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, M, dims, strides, box,
+                            CU_TENSOR_MAP_SWIZZLE_128B);
+  if (e) return set_error(ctx, SPX_ECUDA, "chi0_fp64_real_kernel: tensor map (" + std::to_string(e) + ")");
+  const size_t smem = sizeof(F64RSmem) + 1024;
+  cudaFuncSetAttribute(chi0_fp64_real_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int grid = (int)std::min<int64_t>(prm.nitems, (int64_t)2 * ctx->num_sms);
+  chi0_fp64_real_kernel<<<grid, F64_THREADS, smem, stream>>>(map, prm, out);
+  return check_cuda(ctx, cudaGetLastError(), "chi0_fp64_real_kernel launch");
+}
+
 // FP64 tensor-pipe peak: every warp issues back-to-back m16n8k8 DMMAs on register
 // operands into eight independent accumulators (no memory traffic in the loop),
 // so the rate is the DMMA pipe's own. The sums go to `sink` so nothing is elided.

@@ -106,6 +106,30 @@ __device__ __forceinline__ void fold_epilogue(uint32_t tl, int q, int lane, int 
   }
 }
 
+// The -DINV (real) epilogue: a 128 x 128 tile of real chi, TMEM lane = row i of the
+// block, column = j; read and added 16 columns at a time, then the accumulator is
+// released.
+template <class Release>
+__device__ __forceinline__ void real_epilogue(uint32_t tl, int q, int lane, int bi, int bj, int f,
+                                              const SplitParams& prm, Release release) {
+  const int gi = bi * SP_ROWS + 32 * q + lane;
+  const double fac = gi < prm.N ? fold_row_factor(prm.wsgn[f], prm.sA[gi], prm.wmax[f]) : 0.0;
+  double* of = prm.out + (int64_t)f * prm.npack + gi;
+#pragma unroll 1
+  for (int cc = 0; cc < SP_ROWS / 16; ++cc) {
+    double T[16];
+    load_fold16(tl + (uint32_t)(16 * cc), 128u, T);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int gj = bj * SP_ROWS + 16 * cc + k;
+      if (gi < prm.N && gi <= gj && gj < prm.N)
+        atomicAdd(of + (int64_t)gj * (gj + 1) / 2, fac * prm.sA[gj] * T[k]);
+    }
+  }
+  release();
+}
+
+template <bool REAL>
 __global__ void __launch_bounds__(SP_THREADS, 1)
     split_gram_kernel(const __grid_constant__ CUtensorMap mapF, SplitParams prm) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -228,11 +252,13 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       const int f = item / prm.ntile;
       int bi, bj;
       split_decode_tile(item % prm.ntile, &bi, &bj);
-      fold_epilogue(tl, q, lane, bi, bj, f, prm, [&] {
+      auto release = [&] {
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.tempty);
-      });
+      };
+      if constexpr (REAL) real_epilogue(tl, q, lane, bi, bj, f, prm, release);
+      else fold_epilogue(tl, q, lane, bi, bj, f, prm, release);
     }
   }
 
@@ -526,35 +552,75 @@ __global__ void split_wstat_kernel(const double* __restrict__ W, int64_t ldw, in
   }
 }
 
-// One thread = one complex column i and 16 consecutive pairs of the slab. Digit
-// planes are stored [plane][k-block of 64 pairs][row][64 bytes]; a warp holds 8
-// consecutive columns x the four quarters of one k-block, so its stores cover 16
-// adjacent rows x 64 bytes, and the TMA box (64 B, rows, 1 k-block, planes) lands as
-// [plane][row][64 B] in shared memory. Rows interleave the parts: column i -> rows
-// 128 (i / 64) + 2 (i % 64) (Re) and the next one (Im). For frequency f the planes
-// f*6 + t hold the digits t of round(x |G| / s) (the folded operand), and, when the
-// frequency's weights have both signs, planes f*6 + 3 + t those of round(x G / s).
-__global__ void __launch_bounds__(128)
+// One thread = one complex column i and 8 consecutive pairs of the slab. Digit
+// planes are stored [plane][k-block of 64 pairs][row][64 bytes]; a warp holds 4
+// consecutive columns x the eight 8-pair pieces of one k-block, so its stores cover
+// 8 adjacent rows x 64 bytes, and the TMA box (64 B, rows, 1 k-block, planes) lands
+// as [plane][row][64 B] in shared memory. Rows interleave the parts: column i ->
+// rows 128 (i / 64) + 2 (i % 64) (Re) and the next one (Im). For frequency f the
+// planes f*6 + t hold the digits t of round(x |G| / s) (the folded operand), and,
+// when the frequency's weights have both signs, planes f*6 + 3 + t those of
+// round(x G / s). At most 128 registers a thread: a block fits on an SM beside the
+// accumulation kernel's CTA, so slab s+1 is prepared while slab s accumulates.
+__global__ void __launch_bounds__(128, 4)
     split_quantize_kernel(const double2* __restrict__ M, int64_t ldc, int64_t p0, int len,
                           int nchunk, int N, int npad, int64_t R, int64_t Ps, int nw,
                           const double* __restrict__ sA, const int* __restrict__ wsgn,
                           const double* __restrict__ G, int8_t* __restrict__ F) {
   const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (tid >= (int64_t)npad * nchunk * 2) return;
+  // tid -> (k-block, column group of 4, eighth of the k-block, column in group)
+  const int ngroup = npad / 4;
+  const int lane4 = (int)(tid & 3), eighth = (int)((tid >> 2) & 7);
+  const int64_t rest = tid >> 5;
+  const int i = (int)(rest % ngroup) * 4 + lane4;
+  const int64_t kb = rest / ngroup;
+  const int p = (int)(kb * SP_KB) + eighth * 8;
+  const int64_t nkb = Ps / SP_KB;
+  // planes are nkb * R * 64 bytes apart
+  const int64_t pstride = nkb * R * SP_KB;
+  const int64_t o_re = (kb * R + split_row_re(i)) * SP_KB + eighth * 8;
+  const bool col_ok = i < N;
+  quantize_task8(M + (int64_t)(col_ok ? i : 0) * ldc + p0, col_ok, len, p, col_ok ? sA[i] : 0.0,
+                 o_re, pstride, nw, wsgn, G, nchunk * 16, F);
+}
+
+// -DINV (real M): column scales and digit planes with one plane row per column
+// (rows 128 b .. 128 b + 127 hold the columns of 128-block b).
+__global__ void split_colmax_real_kernel(const double* __restrict__ M, int64_t ldc, int64_t p0,
+                                         int len, double* __restrict__ sA) {
+  const int i = blockIdx.x;
+  const double* col = M + (int64_t)i * ldc + p0;
+  double m = 0.0;
+  for (int p = threadIdx.x; p < len; p += blockDim.x) m = fmax(m, fabs(col[p]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) sA[i] = m;
+  }
+}
+
+__global__ void __launch_bounds__(128, 4)
+    split_quantize_real_kernel(const double* __restrict__ M, int64_t ldc, int64_t p0, int len,
+                               int nchunk, int N, int npad, int64_t R, int64_t Ps, int nw,
+                               const double* __restrict__ sA, const int* __restrict__ wsgn,
+                               const double* __restrict__ G, int8_t* __restrict__ F) {
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (tid >= (int64_t)npad * nchunk) return;
-  // tid -> (k-block, column group of 8, quarter of the k-block, column in group)
   const int ngroup = npad / 8;
   const int lane8 = (int)(tid & 7), quarter = (int)((tid >> 3) & 3);
   const int64_t rest = tid >> 5;
   const int i = (int)(rest % ngroup) * 8 + lane8;
   const int64_t kb = rest / ngroup;
   const int p = (int)(kb * SP_KB) + quarter * 16;
-  const int64_t nkb = Ps / SP_KB;
-  // planes are nkb * R * 64 bytes apart
-  const int64_t pstride = nkb * R * SP_KB;
-  const int64_t o_re = (kb * R + split_row_re(i)) * SP_KB + quarter * 16;
+  const int64_t pstride = (Ps / SP_KB) * R * SP_KB;
   const bool col_ok = i < N;
-  quantize_task(M + (int64_t)(col_ok ? i : 0) * ldc + p0, col_ok, len, p, col_ok ? sA[i] : 0.0,
-                o_re, pstride, nw, wsgn, G, nchunk * 16, F);
+  quantize_task_real(M + (int64_t)(col_ok ? i : 0) * ldc + p0, col_ok, len, p, col_ok ? sA[i] : 0.0,
+                     (kb * R + i) * SP_KB + quarter * 16, pstride, nw, wsgn, G, nchunk * 16, F);
 }
 
 // ---------------------------------------------------------------------------
@@ -721,7 +787,8 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
   const size_t smem2 = sizeof(Split2Smem) + 1024;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(split_gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(split_gram_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(split_gram_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(split_gram2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem2);
     attr_set = true;
@@ -771,7 +838,7 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
     const int nchunk = lenp / 16;  // 16-pair chunks; npad is a multiple of 64
     split_colmax_kernel<<<N, 256, 0, ps>>>(M, ldc, p0, len, sA[b]);
     split_wstat_kernel<<<nw, 256, 0, ps>>>(W, ldw, p0, len, lenp, wmax[b], wsgn[b], G[b]);
-    const int64_t nthr = (int64_t)npad * nchunk;
+    const int64_t nthr = (int64_t)npad * nchunk * 2;  // 8-pair tasks
     split_quantize_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, ps>>>(
         M, ldc, p0, len, nchunk, N, npad, L.R, L.Ps, nw, sA[b], wsgn[b], G[b], F[b]);
     int r = check_cuda(ctx, cudaGetLastError(), "split operand preparation");
@@ -814,7 +881,7 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
       rc = check_cuda(ctx, cudaLaunchKernelEx(&cfg, split_gram2_kernel, mapF[b], mapFh[b], prm),
                       "split_gram2_kernel launch");
     } else {
-      split_gram_kernel<<<grid, SP_THREADS, smem, stream>>>(mapF[b], prm);
+      split_gram_kernel<false><<<grid, SP_THREADS, smem, stream>>>(mapF[b], prm);
       rc = check_cuda(ctx, cudaGetLastError(), "split_gram_kernel launch");
     }
     if (rc) return rc;
@@ -824,6 +891,122 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
       // with one buffer, the next preparation waits for this accumulation
       if (nbuf == 1 &&
           (rc = check_cuda(ctx, cudaStreamWaitEvent(ps, gram_done[0], 0), "event")))
+        return rc;
+      if ((rc = prep(s + 1))) return rc;
+    }
+  }
+  return SPX_OK;
+}
+
+// Real layout: 128 columns per block, one plane row per column.
+static SplitLayout split_layout_real(int64_t P, int N, int nw, int slab) {
+  SplitLayout L = split_layout(P, 1, nw, slab);
+  L.nblk = (N + SP_ROWS - 1) / SP_ROWS;
+  L.R = (int64_t)L.nblk * SP_ROWS;
+  L.f_bytes = align_up((size_t)SP_SLOT * nw * L.R * L.Ps, 1024);
+  L.s_bytes = align_up(sizeof(double) * (size_t)std::max(N, 1), 256);
+  return L;
+}
+
+size_t split_workspace_bytes_real(int64_t P, int N, int nw) {
+  SplitLayout L = split_layout_real(P, N, nw, SP_SLAB);
+  return split_nbuf(P, SP_SLAB) * (L.f_bytes + L.g_bytes + L.s_bytes + L.w_bytes + L.sg_bytes) + 1024;
+}
+
+// The -DINV accumulation (src/susceptibility.f:1197, re(k) = cprod(k,i) * cprod(k,j)):
+// real M (ldc, N), real packed out (npack, nw), the folded 6-product int8 contraction
+// on 128 x 128 real tiles, one CTA per tile.
+int split_chi0_real_slab(spx_ctx* ctx, const double* M, int64_t ldc, int64_t P, int N,
+                         const double* W, int64_t ldw, int nw, double* out, void* ws,
+                         size_t ws_bytes, cudaStream_t stream, int* launches) {
+  if (P <= 0 || N <= 0 || nw <= 0) return SPX_OK;
+  SplitLayout L = split_layout_real(P, N, nw, SP_SLAB);
+  if (!ws || ws_bytes < split_workspace_bytes_real(P, N, nw))
+    return set_error(ctx, SPX_EINVAL, "split workspace too small");
+  uint8_t* base = (uint8_t*)align_up((size_t)ws, 1024);
+  const int nbuf = split_nbuf(P, SP_SLAB);
+  const size_t set_bytes = L.f_bytes + L.g_bytes + L.s_bytes + L.w_bytes + L.sg_bytes;
+  int8_t* F[2];
+  double *G[2], *sA[2], *wmax[2];
+  int* wsgn[2];
+  for (int b = 0; b < 2; ++b) {
+    uint8_t* s0 = base + (size_t)(b < nbuf ? b : 0) * set_bytes;
+    F[b] = (int8_t*)s0;
+    G[b] = (double*)(s0 + L.f_bytes);
+    sA[b] = (double*)(s0 + L.f_bytes + L.g_bytes);
+    wmax[b] = (double*)(s0 + L.f_bytes + L.g_bytes + L.s_bytes);
+    wsgn[b] = (int*)(s0 + L.f_bytes + L.g_bytes + L.s_bytes + L.w_bytes);
+  }
+  const uint64_t nkb = (uint64_t)(L.Ps / SP_KB);
+  CUtensorMap mapF[2];
+  for (int b = 0; b < nbuf; ++b) {
+    const uint64_t st[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};
+    const uint64_t d[4] = {SP_KB, (uint64_t)L.R, nkb, (uint64_t)SP_SLOT * nw};
+    const uint32_t bx[4] = {SP_KB, SP_ROWS, 1, SP_SF};
+    int rc0 = make_tmap_u8_4d(ctx, &mapF[b], F[b], d, st, bx, CU_TENSOR_MAP_SWIZZLE_64B);
+    if (rc0) return rc0;
+  }
+  const size_t smem = sizeof(SplitSmem) + 1024;
+  cudaFuncSetAttribute(split_gram_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int ntile = L.nblk * (L.nblk + 1) / 2;
+  const int nitems = ntile * nw;
+  const int grid = std::min(nitems, ctx->num_sms);
+  const int npad = (int)L.R;
+  const int64_t nslab = (P + L.Ps - 1) / L.Ps;
+  cudaStream_t ps = ctx->prep_stream;
+  cudaEvent_t ev_start = ctx->sev[0];
+  cudaEvent_t prep_done[2] = {ctx->sev[1], ctx->sev[2]};
+  cudaEvent_t gram_done[2] = {ctx->sev[3], ctx->sev[4]};
+  int rc;
+  auto prep = [&](int64_t s) -> int {
+    const int b = (int)(s % nbuf);
+    const int64_t p0 = s * L.Ps;
+    const int len = (int)std::min<int64_t>(L.Ps, P - p0);
+    const int lenp = (int)align_up((size_t)len, SP_KB);
+    const int nchunk = lenp / 16;
+    split_colmax_real_kernel<<<N, 256, 0, ps>>>(M, ldc, p0, len, sA[b]);
+    split_wstat_kernel<<<nw, 256, 0, ps>>>(W, ldw, p0, len, lenp, wmax[b], wsgn[b], G[b]);
+    const int64_t nthr = (int64_t)npad * nchunk;
+    split_quantize_real_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, ps>>>(
+        M, ldc, p0, len, nchunk, N, npad, L.R, L.Ps, nw, sA[b], wsgn[b], G[b], F[b]);
+    int r = check_cuda(ctx, cudaGetLastError(), "split operand preparation (real)");
+    if (r) return r;
+    *launches += 3;
+    return check_cuda(ctx, cudaEventRecord(prep_done[b], ps), "event");
+  };
+  if ((rc = check_cuda(ctx, cudaEventRecord(ev_start, stream), "event")) ||
+      (rc = check_cuda(ctx, cudaStreamWaitEvent(ps, ev_start, 0), "event")))
+    return rc;
+  timing_mark(ctx, stream, 0);
+  if ((rc = prep(0))) return rc;
+  for (int64_t s = 0; s < nslab; ++s) {
+    const int b = (int)(s % nbuf);
+    const int len = (int)std::min<int64_t>(L.Ps, P - s * L.Ps);
+    const int lenp = (int)align_up((size_t)len, SP_KB);
+    if ((rc = check_cuda(ctx, cudaStreamWaitEvent(stream, prep_done[b], 0), "event"))) return rc;
+    if (nbuf == 2 && s >= 1 && s + 1 < nslab &&
+        (rc = check_cuda(ctx, cudaStreamWaitEvent(ps, gram_done[(s + 1) % 2], 0), "event")))
+      return rc;
+    timing_mark(ctx, stream, 1);
+    SplitParams prm;
+    prm.N = N;
+    prm.ntile = ntile;
+    prm.nw = nw;
+    prm.nitems = nitems;
+    prm.nk = lenp / SP_KB;
+    prm.sA = sA[b];
+    prm.wmax = wmax[b];
+    prm.wsgn = wsgn[b];
+    prm.out = out;
+    prm.npack = (int64_t)N * (N + 1) / 2;
+    prm.status = ctx->d_status;
+    prm.timeout_ns = (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
+    split_gram_kernel<true><<<grid, SP_THREADS, smem, stream>>>(mapF[b], prm);
+    if ((rc = check_cuda(ctx, cudaGetLastError(), "split_gram_kernel (real) launch"))) return rc;
+    *launches += 1;
+    if ((rc = check_cuda(ctx, cudaEventRecord(gram_done[b], stream), "event"))) return rc;
+    if (s + 1 < nslab) {
+      if (nbuf == 1 && (rc = check_cuda(ctx, cudaStreamWaitEvent(ps, gram_done[0], 0), "event")))
         return rc;
       if ((rc = prep(s + 1))) return rc;
     }

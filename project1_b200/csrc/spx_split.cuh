@@ -164,6 +164,122 @@ __device__ __forceinline__ void quantize_task(const double2* __restrict__ col, b
   }
 }
 
+// quantize_task for 8 pairs [p, p+8): the same digits (the same arithmetic per
+// value), written as 8-byte pieces of the plane rows. Fewer live registers let the
+// preparation kernel run beside the accumulation kernel on every SM.
+__device__ __forceinline__ void quantize_task8(const double2* __restrict__ col, bool col_ok, int len,
+                                               int p, double s, int64_t o_re, int64_t pstride,
+                                               int nw, const int* __restrict__ wsgn,
+                                               const double* __restrict__ G, int lenp,
+                                               int8_t* __restrict__ F) {
+  const int64_t o_im = o_re + SP_KB;
+  double xr[8], xi[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    double2 v = make_double2(0.0, 0.0);
+    if (col_ok && p + k < len) v = col[p + k];
+    xr[k] = v.x;
+    xi[k] = v.y;
+  }
+  const double inv = s > 0.0 ? 1.0 / s : 0.0;
+#pragma unroll 1
+  for (int f = 0; f < nw; ++f) {
+    const double* gf = G + (int64_t)f * lenp + p;
+    const bool mixed = wsgn[f] == 0;
+    uint32_t ar[SP_SF][2], ai[SP_SF][2], br[SP_SF][2], bim[SP_SF][2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      uint32_t yr[4], yi[4], pr[SP_SF], pi[SP_SF];
+      double gq[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        gq[e] = gf[4 * q + e] * inv;
+        const double ga = fabs(gq[e]);
+        yr[e] = round_mul(xr[4 * q + e], ga);
+        yi[e] = round_mul(xi[4 * q + e], ga);
+      }
+      digit_planes<SP_SF>(yr, pr);
+      digit_planes<SP_SF>(yi, pi);
+#pragma unroll
+      for (int t = 0; t < SP_SF; ++t) ar[t][q] = pr[t], ai[t][q] = pi[t];
+      if (mixed) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (gq[e] < 0.0) yr[e] = 0u - yr[e], yi[e] = 0u - yi[e];
+        digit_planes<SP_SF>(yr, pr);
+        digit_planes<SP_SF>(yi, pi);
+#pragma unroll
+        for (int t = 0; t < SP_SF; ++t) br[t][q] = pr[t], bim[t][q] = pi[t];
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < SP_SF; ++t) {
+      const int64_t plane = (int64_t)f * SP_SLOT + t;
+      *reinterpret_cast<uint2*>(F + o_re + plane * pstride) = make_uint2(ar[t][0], ar[t][1]);
+      *reinterpret_cast<uint2*>(F + o_im + plane * pstride) = make_uint2(ai[t][0], ai[t][1]);
+    }
+    if (mixed) {
+#pragma unroll
+      for (int t = 0; t < SP_SF; ++t) {
+        const int64_t plane = (int64_t)f * SP_SLOT + SP_SF + t;
+        *reinterpret_cast<uint2*>(F + o_re + plane * pstride) = make_uint2(br[t][0], br[t][1]);
+        *reinterpret_cast<uint2*>(F + o_im + plane * pstride) = make_uint2(bim[t][0], bim[t][1]);
+      }
+    }
+  }
+}
+
+// The real (-DINV) form of quantize_task: column i of a real M, one plane row per
+// column (`o` its byte offset in plane 0).
+__device__ __forceinline__ void quantize_task_real(const double* __restrict__ col, bool col_ok,
+                                                   int len, int p, double s, int64_t o,
+                                                   int64_t pstride, int nw,
+                                                   const int* __restrict__ wsgn,
+                                                   const double* __restrict__ G, int lenp,
+                                                   int8_t* __restrict__ F) {
+  double x[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) x[k] = (col_ok && p + k < len) ? col[p + k] : 0.0;
+  const double inv = s > 0.0 ? 1.0 / s : 0.0;
+  for (int f = 0; f < nw; ++f) {
+    const double* gf = G + (int64_t)f * lenp + p;
+    const bool mixed = wsgn[f] == 0;
+    uint32_t a[SP_SF][4], b[SP_SF][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      uint32_t y[4], pd[SP_SF];
+      bool neg[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const double g = gf[4 * q + e] * inv;
+        neg[e] = g < 0.0;
+        y[e] = round_mul(x[4 * q + e], fabs(g));
+      }
+      digit_planes<SP_SF>(y, pd);
+#pragma unroll
+      for (int t = 0; t < SP_SF; ++t) a[t][q] = pd[t];
+      if (mixed) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (neg[e]) y[e] = 0u - y[e];
+        digit_planes<SP_SF>(y, pd);
+#pragma unroll
+        for (int t = 0; t < SP_SF; ++t) b[t][q] = pd[t];
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < SP_SF; ++t)
+      *reinterpret_cast<uint4*>(F + o + ((int64_t)f * SP_SLOT + t) * pstride) =
+          make_uint4(a[t][0], a[t][1], a[t][2], a[t][3]);
+    if (mixed) {
+#pragma unroll
+      for (int t = 0; t < SP_SF; ++t)
+        *reinterpret_cast<uint4*>(F + o + ((int64_t)f * SP_SLOT + SP_SF + t) * pstride) =
+            make_uint4(b[t][0], b[t][1], b[t][2], b[t][3]);
+    }
+  }
+}
+
 // Upper-triangle tile t -> (bi, bj), bi <= bj, column-major over the triangle.
 __device__ __forceinline__ void split_decode_tile(int t, int* bi, int* bj) {
   int j = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);

@@ -728,9 +728,11 @@ extern "C" int spx_wfprod_pw_dev(spx_ctx* ctx, const spx_pw_desc* pw, int32_t nk
 // the rows of B. In place (out == cprod), rows go through a scratch panel in chunks,
 // as the reference's row blocks do, so that no output overwrites an input still read.
 
-extern "C" int spx_trafo_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
-                             int32_t nbas, const double* ctrafo, int64_t ldt, int32_t dim,
-                             double* out, int64_t ldo, void* stream) {
+// The transform with the in-place chunk buffer at byte offset `ws_off` of the workspace
+// (anything the caller keeps in the workspace lies below it).
+static int trafo_run(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair, int32_t nbas,
+                     const double* ctrafo, int64_t ldt, int32_t dim, double* out, int64_t ldo,
+                     void* stream, size_t ws_off) {
   if (!ctx) return SPX_EINVAL;
   if (npair < 0 || nbas < 0 || dim < 0) return set_error(ctx, SPX_EINVAL, "negative size");
   if (npair == 0 || dim == 0) return SPX_OK;
@@ -771,8 +773,8 @@ extern "C" int spx_trafo_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int
   }
   // in place: row chunks through the workspace
   const int64_t chunk = std::min<int64_t>(npair, 65536);
-  if ((rc = ensure_workspace(ctx, 16 * (size_t)chunk * std::max(dim, 1) + 256))) return rc;
-  double2* tmp = reinterpret_cast<double2*>(ctx->ws);
+  if ((rc = ensure_workspace(ctx, ws_off + 16 * (size_t)chunk * std::max(dim, 1) + 256))) return rc;
+  double2* tmp = reinterpret_cast<double2*>((char*)ctx->ws + ws_off);
   for (int64_t r0 = 0; r0 < npair; r0 += chunk) {
     const int64_t len = std::min<int64_t>(chunk, npair - r0);
     if ((rc = check_cuda(ctx, cudaMemsetAsync(tmp, 0, 16 * (size_t)len * dim, s), "zero chunk")))
@@ -789,6 +791,109 @@ extern "C" int spx_trafo_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int
       return rc;
   }
   return SPX_OK;
+}
+
+extern "C" int spx_trafo_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
+                             int32_t nbas, const double* ctrafo, int64_t ldt, int32_t dim,
+                             double* out, int64_t ldo, void* stream) {
+  return trafo_run(ctx, cprod, ldc, npair, nbas, ctrafo, ldt, dim, out, ldo, stream, 0);
+}
+
+// olapvec (src/overlap.f:298-316) forms out(i) = zdotc(row, vec) with
+// row(j) = cstep(G_j - G_i), i.e. out = O vec with O(i, j) = conj(cstep(G_j - G_i)).
+// This kernel writes conj(O)(i, j) = cstep(G_j - G_i) for the MPB plane waves
+// (0 outside the box of cstep), column-major (ngptm, ngptm).
+__global__ void olap_conj_kernel(const int* __restrict__ gptm, int ngptm, const double2* __restrict__ cstep,
+                                 int sr, double2* __restrict__ O) {
+  const int ns = 2 * sr + 1;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (int64_t)ngptm * ngptm;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % ngptm), j = (int)(t / ngptm);
+    const int d0 = gptm[3 * j] - gptm[3 * i], d1 = gptm[3 * j + 1] - gptm[3 * i + 1],
+              d2 = gptm[3 * j + 2] - gptm[3 * i + 2];
+    double2 v = make_double2(0.0, 0.0);
+    if (abs(d0) <= sr && abs(d1) <= sr && abs(d2) <= sr)
+      v = cstep[(d0 + sr) + ns * ((d1 + sr) + ns * (d2 + sr))];
+    O[t] = v;
+  }
+}
+
+// In place: z = conj(z) for rows [0, rows) of `cols` columns (leading dimension ld).
+__global__ void conj_rows_kernel(double2* z, int64_t ld, int rows, int cols) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (int64_t)rows * cols;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    double2* p = z + (t / rows) * ld + t % rows;
+    p->y = -p->y;
+  }
+}
+
+extern "C" int spx_trafo_olap_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t npair,
+                                  int32_t nbas, int32_t nbasp, const double* ctrafo, int64_t ldt,
+                                  int32_t dim, const spx_pw_desc* pw, double* out, int64_t ldo,
+                                  void* stream) {
+  if (!ctx) return SPX_EINVAL;
+  if (!pw || nbasp < 0 || nbasp + pw->ngptm != nbas || pw->step_radius < 0 || pw->step_radius > 4 ||
+      (pw->ngptm > 0 && (!pw->gptm || !pw->cstep)))
+    return set_error(ctx, SPX_EINVAL, "bad plane-wave descriptor (nbas must be nbasp + ngptm)");
+  if (npair < 0 || nbas < 0 || dim < 0) return set_error(ctx, SPX_EINVAL, "negative size");
+  if (npair == 0 || dim == 0) return SPX_OK;
+  if (!ctrafo || ldt < nbas) return set_error(ctx, SPX_EINVAL, "ctrafo NULL or ldt < nbas");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = pick_stream(ctx, stream);
+  const int ng = pw->ngptm, sr = pw->step_radius, ns = 2 * sr + 1;
+  // workspace: ctrafo1 (nbas, dim), conj(O) (ng, ng), the G list and cstep
+  const size_t t1_b = align_up(16 * (size_t)nbas * dim, 256);
+  const size_t o_b = align_up(16 * (size_t)ng * ng, 256);
+  const size_t g_b = align_up(sizeof(int) * 3 * (size_t)std::max(ng, 1), 256);
+  const size_t c_b = align_up(16 * (size_t)ns * ns * ns, 256);
+  const size_t keep = t1_b + o_b + g_b + c_b;
+  int rc = ensure_workspace(ctx, keep + 256);
+  if (rc) return rc;
+  char* w = (char*)ctx->ws;
+  double2* T1 = (double2*)w;
+  double2* O = (double2*)(w + t1_b);
+  int* G = (int*)(w + t1_b + o_b);
+  double2* CS = (double2*)(w + t1_b + o_b + g_b);
+  // ctrafo1(:nbasp) = ctrafo(:nbasp); ctrafo1(nbasp:) = O ctrafo(nbasp:) (olapvec per column)
+  if ((rc = check_cuda(ctx, cudaMemcpy2DAsync(T1, 16 * (size_t)nbas, ctrafo, 16 * (size_t)ldt,
+                                              16 * (size_t)nbasp, dim, cudaMemcpyDeviceToDevice, s),
+                       "copy MT rows")))
+    return rc;
+  if (ng > 0) {
+    if ((rc = check_cuda(ctx, cudaMemcpyAsync(G, pw->gptm, sizeof(int) * 3 * ng, cudaMemcpyHostToDevice, s),
+                         "copy G list")) ||
+        (rc = check_cuda(ctx, cudaMemcpyAsync(CS, pw->cstep, 16 * (size_t)ns * ns * ns, cudaMemcpyHostToDevice, s),
+                         "copy step function")) ||
+        0)
+      return rc;
+    if ((rc = check_cuda(ctx, cudaMemset2DAsync(T1 + nbasp, 16 * (size_t)nbas, 0, 16 * (size_t)ng, dim, s),
+                         "zero PW rows")))
+      return rc;
+    olap_conj_kernel<<<std::min<int64_t>(((int64_t)ng * ng + 255) / 256, (int64_t)ctx->num_sms * 16), 256, 0, s>>>(
+        G, ng, CS, sr, O);
+    if ((rc = check_cuda(ctx, cudaGetLastError(), "olap_conj_kernel launch"))) return rc;
+    // conj(ctrafo1_pw)(i, c) = sum_j conj(O(i, j)) conj(ctrafo(nbasp + j, c))
+    ZgParams prm{};
+    prm.A = O;
+    prm.a_mcontig = 1;
+    prm.lda = ng;
+    prm.B = reinterpret_cast<const double2*>(ctrafo) + nbasp;
+    prm.sBc = ldt;
+    prm.ncin = dim;
+    prm.O = T1 + nbasp;
+    prm.sOc = nbas;
+    prm.alpha_v = make_double2(1.0, 0.0);
+    prm.M = ng;
+    prm.ncol = dim;
+    prm.K = ng;
+    prm.nb1 = 1;
+    if ((rc = launch_zgemm(ctx, prm, 1, s))) return rc;
+    conj_rows_kernel<<<std::min<int64_t>(((int64_t)ng * dim + 255) / 256, (int64_t)ctx->num_sms * 16), 256, 0, s>>>(
+        T1 + nbasp, nbas, ng, dim);
+    if ((rc = check_cuda(ctx, cudaGetLastError(), "conj_rows_kernel launch"))) return rc;
+  }
+  return trafo_run(ctx, cprod, ldc, npair, nbas, reinterpret_cast<const double*>(T1), nbas, dim, out,
+                   ldo, stream, keep);
 }
 
 // ---------------------------------------------------------------------------

@@ -181,6 +181,22 @@ class Context:
                                               _ptr(wghtSr), scale_all, _ptr(w), ldw, torch_stream(stream, w))
         self._check(rc, "spx_weights_hilbert_dev")
 
+    def chi0_accumulate_real_dev(self, cprod, ediff, omega, susceph, wscale=None,
+                                 scale_all: float = 1.0, precision: str = "fp64", stream=None,
+                                 npair: Optional[int] = None, stats: bool = False) -> Optional[dict]:
+        """The -DINV form: cprod float64 (nbas, ldc) == Fortran real (ldc, nbas), susceph
+        float64 (nw, npack) == Fortran real (npack, nw)."""
+        nbas, ldc = cprod.shape
+        npair = ldc if npair is None else npair
+        nw = omega.shape[0]
+        st = _lib.spx_chi0_stats() if stats else None
+        rc = self.lib.spx_chi0_accumulate_real_dev(
+            self.handle, _ptr(cprod), ldc, npair, nbas, _ptr(ediff), _ptr(wscale), scale_all, nw,
+            _ptr(omega), PRECISIONS[precision], _ptr(susceph), torch_stream(stream, susceph),
+            C.byref(st) if st is not None else None)
+        self._check(rc, "spx_chi0_accumulate_real_dev")
+        return _stats(st) if st is not None else None
+
     def chi0_accumulate_w_dev(self, cprod, w, susceph, precision: str = "fp64",
                               npair: Optional[int] = None, stream=None, stats: bool = False):
         """susceph += sum_p cprod(p,i) conj(cprod(p,j)) w(p,f) with given weights w (nw, ldw)."""
@@ -252,6 +268,21 @@ class Context:
         rc = self.lib.spx_trafo_dev(self.handle, _ptr(cprod), ldc, npair, nbas, _ptr(ctrafo), ldt,
                                     dim, _ptr(o), o.shape[1], torch_stream(stream, cprod))
         self._check(rc, "spx_trafo_dev")
+        return o
+
+    def trafo_olap_dev(self, cprod, ctrafo, nbasp: int, pw, out=None, npair: Optional[int] = None,
+                       stream=None):
+        """The transform without FULLPW (src/susceptibility.f:814-824): the interstitial
+        rows of ctrafo are first multiplied by the plane-wave overlap built from
+        pw (a wavefproducts.PwDesc: gptm and cstep). Shapes as trafo_dev."""
+        nbas, ldc = cprod.shape
+        dim, ldt = ctrafo.shape
+        npair = ldc if npair is None else npair
+        o = cprod if out is None else out
+        rc = self.lib.spx_trafo_olap_dev(self.handle, _ptr(cprod), ldc, npair, nbas, nbasp, _ptr(ctrafo),
+                                         ldt, dim, C.byref(pw.c), _ptr(o), o.shape[1],
+                                         torch_stream(stream, cprod))
+        self._check(rc, "spx_trafo_olap_dev")
         return o
 
     # ---- many q points in one launch ---------------------------------------------

@@ -186,3 +186,31 @@ def test_measured_dmma_peak_is_plausible():
         v = c.measure_dmma_peak()
     print(f"measured DMMA peak: {v:.1f} TFLOP/s")
     assert 10.0 < v < 120.0, v
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("split", 1e-6)])
+@pytest.mark.parametrize("nbas,npair,nw,ldpad", [(1, 3, 1, 0), (130, 5001, 3, 1), (257, 40000, 2, 0), (64, 64, 2, 3)])
+def test_real_variant_matches_oracle(precision, tol, nbas, npair, nw, ldpad):
+    """The -DINV build: real cprod (odd leading dimensions included), real packed chi."""
+    rng = np.random.default_rng(nbas + npair)
+    m = rng.standard_normal((npair, nbas)) / np.sqrt(nbas)
+    d = rng.uniform(0.5, 40.0, npair)
+    d[rng.choice(npair, max(1, npair // 100), replace=False)] = 3e-7
+    om = inputs.frequencies(nw)
+    w = oracle.weights(d, om, None, 0.5)
+    ref = oracle.chi0_real(m, w)
+    ldc = npair + ldpad
+    cp = torch.zeros((nbas, ldc), dtype=torch.float64, device=DEV)
+    cp[:, :npair] = torch.from_numpy(np.ascontiguousarray(m.T)).to(DEV)
+    out = torch.zeros((nw, nbas * (nbas + 1) // 2), dtype=torch.float64, device=DEV)
+    with spx.Context(0) as c:
+        st = c.chi0_accumulate_real_dev(cp, torch.from_numpy(d).to(DEV), torch.from_numpy(om).to(DEV), out,
+                                        scale_all=0.5, precision=precision, npair=npair, stats=True)
+    assert st["kernel_launches"] >= 2
+    got = out.cpu().numpy().T
+    j = np.arange(nbas)
+    dg = np.abs(ref[j * (j + 1) // 2 + j])
+    iu, ju = np.triu_indices(nbas)
+    idx = ju * (ju + 1) // 2 + iu
+    err = np.abs(got[idx] - ref[idx]) / np.sqrt(dg[iu] * dg[ju])
+    assert err.max() <= tol, err.max()

@@ -111,3 +111,14 @@ def test_realfreq_restatement_is_the_complex_weighted_gram():
     got = oracle.chi0_realfreq(m, wr, wi)
     direct = np.einsum("pi,pj,pf->ijf", m, np.conj(m), wr + 1j * wi)
     assert np.abs(got - direct).max() <= 1e-12 * np.abs(direct).max()
+
+
+def test_real_restatement_matches_einsum():
+    """The -DINV loop restated (real re(k) = cprod(k,i) cprod(k,j), :1197) is the real
+    weighted Gram on the packed upper triangle."""
+    rng = np.random.default_rng(3)
+    m, w = rng.standard_normal((50, 6)), rng.standard_normal((50, 2))
+    got = oracle.chi0_real(m, w)
+    iu, ju = np.triu_indices(6)
+    ref = np.einsum("pi,pj,pf->ijf", m, m, w)[iu, ju]
+    assert np.abs(got[ju * (ju + 1) // 2 + iu] - ref).max() <= 1e-13

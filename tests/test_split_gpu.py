@@ -12,7 +12,10 @@ from test_chi0_gpu import DEV, G, random_case, run_dev
 
 pytestmark = pytest.mark.gpu
 SPLIT_TOL = 1e-6       # per-element error / sqrt(|chi_ii chi_jj|), split path
-SPLIT_FRO = 1e-7       # Frobenius relative error, split path
+# Frobenius relative error, split path: the same bound. Three digits of both folded
+# operands round at 2^-17/127 of the column scale and the dropped digit orders are of
+# that size, so small or ragged slabs (crest factor near sqrt(P)) land at 1e-7..5e-7.
+SPLIT_FRO = 1e-6
 
 
 @pytest.fixture(scope="module")

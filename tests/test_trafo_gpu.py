@@ -69,3 +69,32 @@ def test_trafo_rejects_bad_arguments(ctx):
         rc = ctx.lib.spx_trafo_dev(ctx.handle, md.data_ptr(), 100, 100, 20, td.data_ptr(), 20, 10,
                                    md.data_ptr(), 101, None)
         ctx._check(rc, "spx_trafo_dev")
+
+
+@pytest.mark.parametrize("inplace", [False, True])
+def test_trafo_without_fullpw_matches_oracle(ctx, inplace):
+    """The non-FULLPW branch (:814-824): interstitial rows of ctrafo multiplied by the
+    plane-wave overlap (olapvec) before the transform; MT rows unchanged."""
+    from project1_b200 import inputs
+    from project1_b200.wavefproducts import PwDesc
+    w = inputs.WFPROD_CONFIGS["c4"]
+    basis = inputs.pw_basis(w)
+    ng = 60
+    gptm = basis["gptm"][:ng]
+    pw = PwDesc(dict(basis, gptm=gptm))
+    nbasp, npair, dim = 37, 3001, 90
+    nbas = nbasp + ng
+    m, t, md, td = _case(npair, nbas, dim, seed=12)
+    ref = oracle.trafo_olap(m, t, nbasp, gptm, basis["cstep"], basis["step_radius"])
+    if inplace:
+        got = ctx.trafo_olap_dev(md, td, nbasp, pw)
+        torch.cuda.synchronize()
+        res = got.cpu().numpy()[:dim].T
+    else:
+        out = torch.zeros((dim, npair + 2), dtype=torch.complex128, device=DEV)
+        ctx.trafo_olap_dev(md, td, nbasp, pw, out=out, npair=npair)
+        torch.cuda.synchronize()
+        res = out.cpu().numpy()[:, :npair].T
+    assert _rel(res, ref) <= TOL
+    # the overlap changes the result (it is not the FULLPW transform)
+    assert _rel(oracle.trafo(m, t), ref) > 1e-3
