@@ -273,6 +273,39 @@ int spx_headwings_dev(spx_ctx* ctx, const double* cprod, int64_t ldc, int64_t np
                       int32_t dim, const double* dcprod, int64_t ldd, const double* w,
                       int64_t ldw, int32_t nw, double* head, double* wing, void* stream);
 
+/* ---- q -> 0 momentum matrix -------------------------------------------------
+ * Replaces momentum_matrix (src/dwavefproducts.f:89-330, non-SOC, without storeibz)
+ * and the scaling of src/susceptibility.f:848-870: the head/wings input
+ *   dcprod(p, x) = momentum(n', n, k, x) / sqrt(vol) / ediff(p)   (0 if |ediff| <= 1e-8;
+ *                  no energy division when ediff is NULL, the multdiff mode),
+ * p = n' + nunocc*(n + nocc*k), x = 1..3 Cartesian, with
+ *   momentum = -i <phi_n | d/dx | phi_n'> from the MT coefficients (F/G coefficients
+ *   times the radial integrals qmat1, qmat2) and the plane waves (olapvec of the
+ *   occupied coefficients against (k+G)_x times the unoccupied ones).
+ * One atom type; cmt layouts as spx_wfprod_mt_dev, cpw as spx_wfprod_pw_dev (one G
+ * list for all k). Descriptor arrays are host memory; coefficients, ediff, dcprod
+ * (ldd, 3) complex are device memory. */
+typedef struct spx_mom_desc {
+  int32_t natom, lcut, nrad;  /* maxlm = (lcut+1)^2 nrad                               */
+  int32_t ngpt;               /* plane waves per k (0: no interstitial part)           */
+  const double* qmat1;        /* (nrad, nrad, lcut+1): l-1 radial function n1 against l n2,
+                                 int(u' u) + (l+1) int(u u / r) (:153-159)             */
+  const double* qmat2;        /* (nrad, nrad, lcut+1): l+1 n1 against l n2,
+                                 int(u' u) - l int(u u / r) (:160-166)                 */
+  const int32_t* gpt;         /* (3, ngpt) integer G vectors                           */
+  const double* kpt;          /* (3, nk) k points in reciprocal-lattice coordinates     */
+  const double* rlat;         /* (3, 3) column-major reciprocal lattice                 */
+  const double* cstep;        /* complex (2sr+1)^3, x fastest                          */
+  int32_t step_radius;
+  int32_t reserved;
+  double vol;                 /* unit-cell volume                                      */
+} spx_mom_desc;
+
+int spx_dcprod_dev(spx_ctx* ctx, const spx_mom_desc* d, int32_t nk, int32_t nocc,
+                   int32_t nunocc, const double* cmt_occ, const double* cmt_unocc,
+                   const double* cpw_occ, const double* cpw_unocc, const double* ediff,
+                   double* dcprod, int64_t ldd, void* stream);
+
 /* ---- transform to the Coulomb eigenbasis ------------------------------------
  * Replaces src/susceptibility.f:806-832 (the FULLPW branch of the complex build):
  * cprod(:, :dim) = conj(conj(cprod) * ctrafo), i.e.

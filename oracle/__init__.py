@@ -423,3 +423,77 @@ def chi0_real(cprod, w, susceph=None) -> np.ndarray:
         re = cprod[:, : j + 1].astype(np.longdouble) * cprod[:, j].astype(np.longdouble)[:, None]
         susceph[j * (j + 1) // 2: j * (j + 1) // 2 + j + 1] += (re.T @ w).astype(np.float64)
     return susceph
+
+
+def momentum_matrix(cmt_occ, cmt_unocc, cpw_occ, cpw_unocc, lcut, nrad, qmat1, qmat2, gpt, kpt,
+                    rlat, cstep, sr):
+    """momentum(n', n, k, x) as src/dwavefproducts.f:89-330 computes it (non-SOC, one
+    atom type, nindx(l) = nrad for every l), restated loop by loop:
+      F / G coefficients :135-146; MT vectors cvec1/2/3 from l+1 (qmat2, :203-219) and
+      from l-1 (qmat1, :220-240); cvec(x) = dotprod(cvec_x, cmt2) / i and the Cartesian
+      combination :241-253; plane waves :259-283 (vec1 = olapvec(cpw_n), qg = rlat (k+G)).
+    Coefficients: cmt (nk, nb, natom, maxlm), cpw (nk, nb, ngpt). Returns
+    (nunocc, nocc, nk, 3) complex."""
+    nk, nocc, natom, maxlm = cmt_occ.shape
+    nunocc = cmt_unocc.shape[1]
+    mom = np.zeros((nunocc, nocc, nk, 3), dtype=complex)
+    nlm = (lcut + 1) ** 2
+    fco = np.zeros((nlm + 1, 3))
+    gco = np.zeros((nlm + 1, 3))
+    lm = 0
+    for l in range(lcut + 1):
+        for m in range(-l, l + 1):
+            lm += 1
+            fco[lm] = [-np.sqrt((l + m + 1) * (l + m + 2) / (2 * (2 * l + 1) * (2 * l + 3))),
+                       np.sqrt((l - m + 1) * (l + m + 1) / ((2 * l + 1) * (2 * l + 3))),
+                       -np.sqrt((l - m + 1) * (l - m + 2) / (2 * (2 * l + 1) * (2 * l + 3)))]
+            gco[lm] = [np.sqrt(max((l - m) * (l - m - 1), 0) / (2 * (2 * l - 1) * (2 * l + 1))) if l else 0,
+                       np.sqrt(max((l - m) * (l + m), 0) / ((2 * l - 1) * (2 * l + 1))) if l else 0,
+                       np.sqrt(max((l + m) * (l + m - 1), 0) / (2 * (2 * l - 1) * (2 * l + 1))) if l else 0]
+    q1 = np.asarray(qmat1).reshape((nrad, nrad, lcut + 1), order="F")
+    q2 = np.asarray(qmat2).reshape((nrad, nrad, lcut + 1), order="F")
+    for k in range(nk):
+        for a in range(natom):
+            for n in range(nocc):
+                cmt1 = cmt_occ[k, n, a]
+                cv = [np.zeros(maxlm, complex) for _ in range(3)]
+                lm_0, lm_1, lm = 0, nrad, 0
+                for l in range(lcut):
+                    n0 = n1 = nrad
+                    for m in range(-l, l + 1):
+                        lm += 1
+                        lm0 = lm_0 + (m + l) * n0
+                        src = [lm_1 + (m + 1 + l + 1) * n1, lm_1 + (m + l + 1) * n1, lm_1 + (m - 1 + l + 1) * n1]
+                        for x in range(3):
+                            cv[x][lm0:lm0 + n0] = fco[lm, x] * (cmt1[src[x]:src[x] + n1] @ q2[:n1, :n0, l])
+                    lm_0 += (2 * l + 1) * n0
+                    lm_1 += (2 * l + 3) * n1
+                lm_0, lm_1, lm = nrad, 0, 1
+                for l in range(1, lcut + 1):
+                    n0 = n1 = nrad
+                    for m in range(-l, l + 1):
+                        lm += 1
+                        lm0 = lm_0 + (m + l) * n0
+                        mps = [m + 1, m, m - 1]
+                        for x in range(3):
+                            if abs(mps[x]) <= l - 1:
+                                s0 = lm_1 + (mps[x] + l - 1) * n1
+                                cv[x][lm0:lm0 + n0] += gco[lm, x] * (cmt1[s0:s0 + n1] @ q1[:n1, :n0, l])
+                    lm_0 += (2 * l + 1) * n0
+                    lm_1 += (2 * l - 1) * n1
+                for n2 in range(nunocc):
+                    cmt2 = cmt_unocc[k, n2, a]
+                    c = [np.vdot(cv[x], cmt2) / 1j for x in range(3)]
+                    mom[n2, n, k, 0] += (c[0] - c[2]) / np.sqrt(2.0)
+                    mom[n2, n, k, 1] -= (c[0] + c[2]) / np.sqrt(2.0) * 1j
+                    mom[n2, n, k, 2] += c[1]
+    g = np.asarray(gpt)
+    for k in range(nk):
+        qg = (np.asarray(rlat) @ (np.asarray(kpt[k])[:, None] + g.T)).T       # (ngpt, 3)
+        for n in range(nocc):
+            vec1 = olapvec(cpw_occ[k, n], g, cstep, sr)
+            for n2 in range(nunocc):
+                vec2 = cpw_unocc[k, n2]
+                for x in range(3):
+                    mom[n2, n, k, x] += np.vdot(vec1, vec2 * qg[:, x])
+    return mom

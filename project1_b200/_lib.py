@@ -48,6 +48,15 @@ class spx_chi0_stats(C.Structure):
     ]
 
 
+class spx_mom_desc(C.Structure):
+    _fields_ = [
+        ("natom", C.c_int32), ("lcut", C.c_int32), ("nrad", C.c_int32), ("ngpt", C.c_int32),
+        ("qmat1", C.c_void_p), ("qmat2", C.c_void_p), ("gpt", C.c_void_p), ("kpt", C.c_void_p),
+        ("rlat", C.c_void_p), ("cstep", C.c_void_p), ("step_radius", C.c_int32),
+        ("reserved", C.c_int32), ("vol", C.c_double),
+    ]
+
+
 class spx_mt_desc(C.Structure):
     _fields_ = [
         ("natom", C.c_int32), ("lcut", C.c_int32), ("nrad", C.c_int32),
@@ -138,6 +147,8 @@ SIGNATURES = {
     "spx_selftest_wait_dev": (C.c_int, [_P, _I32]),
     "spx_measure_dmma_peak": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "spx_trafo_dev": (C.c_int, [_P, _P, _I64, _I64, _I32, _P, _I64, _I32, _P, _I64, _P]),
+    "spx_dcprod_dev": (C.c_int, [_P, C.POINTER(spx_mom_desc), _I32, _I32, _I32, _P, _P, _P, _P, _P,
+                                 _P, _I64, _P]),
     "spx_trafo_olap_dev": (C.c_int, [_P, _P, _I64, _I64, _I32, _I32, _P, _I64, _I32,
                                      C.POINTER(spx_pw_desc), _P, _I64, _P]),
     "spx_chi0_batched": (

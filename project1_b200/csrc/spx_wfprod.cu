@@ -1018,3 +1018,311 @@ extern "C" int spx_headwings_dev(spx_ctx* ctx, const double* cprod, int64_t ldc,
   }
   return SPX_OK;
 }
+
+// ---------------------------------------------------------------------------
+// q -> 0 momentum matrix: momentum_matrix (src/dwavefproducts.f:89-330, the non-SOC
+// branch without storeibz) and the dcprod scaling of src/susceptibility.f:848-870.
+//
+// MT part: per atom and occupied band, the reference builds cvec1/2/3 from cmt1 with
+// the F / G coefficients (:135-146) times the radial integrals qmat2 (l -> l+1,
+// :215-219) and qmat1 (l -> l-1, :233-238); cvec(x) = zdotc(cvec_x, cmt2) / i and
+//   momentum(1) += (cvec(1) - cvec(3)) / sqrt 2,  momentum(2) -= (cvec(1) + cvec(3)) i / sqrt 2,
+//   momentum(3) += cvec(2).
+// Here the linear map cmt1 -> v_x with v_1 = (cvec1 - cvec3)/sqrt 2, v_2 = i (cvec1 +
+// cvec3)/sqrt 2, v_3 = cvec2 is a complex sparse matrix (CSR, built on the host from
+// the same index nest), applied per (k, atom, band), and
+//   momentum(n', n, k, x) += -i sum_idx cmt2(n', idx) conj(v_x(n, idx))
+// is a batched complex DMMA GEMM (K4c), one launch per atom.
+// PW part (:269-283): vec1 = olapvec(cpw(:, n)) = O cpw_n with O(i, j) =
+// conj(cstep(G_j - G_i)), and momentum(n', n, k, x) += sum_G conj(vec1(G)) cpw(G, n')
+// qg(G, x), qg = rlat (k + G): two K4c GEMMs (conj(O) conj(cpw) gives conj(vec1), then
+// cpw_unocc against vec1 qg).
+
+struct MomMap {
+  int maxlm;
+  std::vector<int> rp, ci;
+  std::vector<double2> cv;
+};
+
+static int build_mom_map(spx_ctx* ctx, const spx_mom_desc* d, MomMap* mp) {
+  const int L = d->lcut, nr = d->nrad;
+  if (L < 0 || L > 16 || nr <= 0 || nr > 16 || !d->qmat1 || !d->qmat2)
+    return set_error(ctx, SPX_EINVAL, "bad momentum descriptor (lcut 0..16, nrad 1..16, qmat1/2)");
+  const int maxlm = (L + 1) * (L + 1) * nr;
+  mp->maxlm = maxlm;
+  auto off = [&](int l) { return l * l * nr; };           // first index of block l
+  auto q1 = [&](int n1, int n2, int l) { return d->qmat1[n1 + nr * (n2 + nr * l)]; };
+  auto q2 = [&](int n1, int n2, int l) { return d->qmat2[n1 + nr * (n2 + nr * l)]; };
+  // c[x][out] : list of (in, real coefficient) for cvec_{x+1}
+  std::vector<std::vector<std::pair<int, double>>> c(3 * maxlm);
+  for (int l = 0; l <= L; ++l)
+    for (int m = -l; m <= l; ++m) {
+      const double fl = (double)l, fm = (double)m;
+      const double f[3] = {-std::sqrt((fl + fm + 1) * (fl + fm + 2) / (2 * (2 * fl + 1) * (2 * fl + 3))),
+                           std::sqrt((fl - fm + 1) * (fl + fm + 1) / ((2 * fl + 1) * (2 * fl + 3))),
+                           -std::sqrt((fl - fm + 1) * (fl - fm + 2) / (2 * (2 * fl + 1) * (2 * fl + 3)))};
+      const double g[3] = {std::sqrt((fl - fm) * (fl - fm - 1) / (2 * (2 * fl - 1) * (2 * fl + 1))),
+                           std::sqrt((fl - fm) * (fl + fm) / ((2 * fl - 1) * (2 * fl + 1))),
+                           std::sqrt((fl + fm) * (fl + fm - 1) / (2 * (2 * fl - 1) * (2 * fl + 1)))};
+      const int out = off(l) + (m + l) * nr;
+      for (int x = 0; x < 3; ++x) {
+        const int mp_ = m + 1 - x;                         // m+1, m, m-1 for cvec1, 2, 3
+        if (l < L) {                                       // from l+1 (:211-219)
+          const int src = off(l + 1) + (mp_ + l + 1) * nr;
+          for (int n2 = 0; n2 < nr; ++n2)
+            for (int n1 = 0; n1 < nr; ++n1)
+              c[x * maxlm + out + n2].push_back({src + n1, f[x] * q2(n1, n2, l)});
+        }
+        if (l >= 1 && std::abs(mp_) <= l - 1) {            // from l-1 (:222-238)
+          const int src = off(l - 1) + (mp_ + l - 1) * nr;
+          for (int n2 = 0; n2 < nr; ++n2)
+            for (int n1 = 0; n1 < nr; ++n1)
+              c[x * maxlm + out + n2].push_back({src + n1, g[x] * q1(n1, n2, l)});
+        }
+      }
+    }
+  // v_1 = (c1 - c3)/sqrt2, v_2 = i (c1 + c3)/sqrt2, v_3 = c2
+  const double r2 = 1.0 / std::sqrt(2.0);
+  mp->rp.assign(1, 0);
+  for (int x = 0; x < 3; ++x)
+    for (int o = 0; o < maxlm; ++o) {
+      std::vector<double2> row(maxlm, make_double2(0.0, 0.0));
+      std::vector<char> used(maxlm, 0);
+      auto add = [&](const std::vector<std::pair<int, double>>& v, double2 s) {
+        for (auto& e : v) {
+          row[e.first].x += s.x * e.second;
+          row[e.first].y += s.y * e.second;
+          used[e.first] = 1;
+        }
+      };
+      if (x == 0) {
+        add(c[0 * maxlm + o], make_double2(r2, 0.0));
+        add(c[2 * maxlm + o], make_double2(-r2, 0.0));
+      } else if (x == 1) {
+        add(c[0 * maxlm + o], make_double2(0.0, r2));
+        add(c[2 * maxlm + o], make_double2(0.0, r2));
+      } else {
+        add(c[1 * maxlm + o], make_double2(1.0, 0.0));
+      }
+      for (int i = 0; i < maxlm; ++i)
+        if (used[i]) {
+          mp->ci.push_back(i);
+          mp->cv.push_back(row[i]);
+        }
+      mp->rp.push_back((int)mp->ci.size());
+    }
+  return SPX_OK;
+}
+
+// v[k][n][atom][x][idx] = sum_in T(x*maxlm + idx, in) cmt1[k][n][atom][in], one CTA per
+// (band, atom, k); the band's coefficients are staged in shared memory.
+__global__ void __launch_bounds__(256) mom_expand_kernel(const double2* __restrict__ c1, int natom,
+                                                         int maxlm, int nocc, const int* __restrict__ rp,
+                                                         const int* __restrict__ ci,
+                                                         const double2* __restrict__ cv,
+                                                         double2* __restrict__ v) {
+  extern __shared__ double2 cm[];
+  const int n = blockIdx.x, a = blockIdx.y, k = blockIdx.z;
+  const double2* src = c1 + (((int64_t)k * nocc + n) * natom + a) * maxlm;
+  for (int i = threadIdx.x; i < maxlm; i += blockDim.x) cm[i] = src[i];
+  __syncthreads();
+  double2* dst = v + (((int64_t)k * nocc + n) * natom + a) * 3 * maxlm;
+  for (int r = threadIdx.x; r < 3 * maxlm; r += blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int e = rp[r]; e < rp[r + 1]; ++e) {
+      const double2 t = cv[e], x = cm[ci[e]];
+      re += t.x * x.x - t.y * x.y;
+      im += t.x * x.y + t.y * x.x;
+    }
+    dst[r] = make_double2(re, im);
+  }
+}
+
+struct Mat3 {
+  double r[9];  // column-major 3 x 3
+};
+
+// Bq[((k n) 3 + x) ngpt + G] = conj(R(G, k n)) qg_k(G, x), qg = rlat (k + G) with
+// kc[3k + x] = (rlat k)_x.
+__global__ void mom_pw_rhs_kernel(const double2* __restrict__ R, int ngpt, int nkn, int nocc,
+                                  const int* __restrict__ gpt, const double* __restrict__ kc, Mat3 rl,
+                                  double2* __restrict__ Bq) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (int64_t)ngpt * nkn;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int G = (int)(t % ngpt), kn = (int)(t / ngpt), k = kn / nocc;
+    const double2 r = R[(int64_t)kn * ngpt + G];
+    const double g0 = gpt[3 * G], g1 = gpt[3 * G + 1], g2 = gpt[3 * G + 2];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      const double q = kc[3 * k + x] + rl.r[x] * g0 + rl.r[x + 3] * g1 + rl.r[x + 6] * g2;
+      Bq[((int64_t)kn * 3 + x) * ngpt + G] = make_double2(r.x * q, -r.y * q);
+    }
+  }
+}
+
+// dcprod(p, x) /= sqrt(vol) e(p), and 0 where |e(p)| <= 1e-8 (src/susceptibility.f:858-869);
+// only the volume factor when e is NULL.
+__global__ void mom_scale_kernel(double2* __restrict__ dc, int64_t ldd, int64_t npair,
+                                 const double* __restrict__ e, double rsv) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 3 * npair;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = t % npair;
+    const int x = (int)(t / npair);
+    double f = rsv;
+    if (e) {
+      const double r = e[p];
+      f = fabs(r) > 1e-8 ? rsv / r : 0.0;
+    }
+    double2* z = dc + x * ldd + p;
+    z->x *= f;
+    z->y *= f;
+  }
+}
+
+extern "C" int spx_dcprod_dev(spx_ctx* ctx, const spx_mom_desc* d, int32_t nk, int32_t nocc,
+                              int32_t nunocc, const double* cmt_occ, const double* cmt_unocc,
+                              const double* cpw_occ, const double* cpw_unocc, const double* ediff,
+                              double* dcprod, int64_t ldd, void* stream) {
+  if (!ctx) return SPX_EINVAL;
+  if (!d || nk < 0 || nocc < 0 || nunocc < 0) return set_error(ctx, SPX_EINVAL, "bad arguments");
+  const int64_t npair = (int64_t)nk * nocc * nunocc;
+  if (npair == 0) return SPX_OK;
+  if (!dcprod || ldd < npair) return set_error(ctx, SPX_EINVAL, "dcprod NULL or ldd < nk*nocc*nunocc");
+  if (d->natom > 0 && (!cmt_occ || !cmt_unocc)) return set_error(ctx, SPX_EINVAL, "MT coefficients missing");
+  if (d->ngpt > 0 && (!cpw_occ || !cpw_unocc || !d->gpt || !d->kpt || !d->rlat || !d->cstep ||
+                      d->step_radius < 0 || d->step_radius > 4))
+    return set_error(ctx, SPX_EINVAL, "plane-wave part of the momentum descriptor incomplete");
+  if (!(d->vol > 0)) return set_error(ctx, SPX_EINVAL, "vol must be positive");
+  if (nocc > 65535 || d->natom > 65535 || nk > 65535) return set_error(ctx, SPX_EINVAL, "too many bands");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = pick_stream(ctx, stream);
+  int rc;
+  MomMap mp{};
+  if (d->natom > 0 && (rc = build_mom_map(ctx, d, &mp))) return rc;
+  const int ng = d->ngpt, sr = d->step_radius, ns = 2 * sr + 1;
+  const int64_t nkn = (int64_t)nk * nocc;
+  size_t need = 0;
+  auto add = [&](size_t b) { need += align_up(b, 256); };
+  if (d->natom > 0) {
+    add(sizeof(int) * mp.rp.size());
+    add(sizeof(int) * std::max<size_t>(mp.ci.size(), 1));
+    add(sizeof(double2) * std::max<size_t>(mp.cv.size(), 1));
+    add(sizeof(double2) * (size_t)nkn * d->natom * 3 * mp.maxlm);
+  }
+  if (ng > 0) {
+    add(sizeof(double2) * (size_t)ng * ng);
+    add(sizeof(double2) * (size_t)ng * nkn);
+    add(sizeof(double2) * (size_t)ng * nkn * 3);
+    add(sizeof(int) * 3 * (size_t)ng);
+    add(sizeof(double2) * (size_t)ns * ns * ns);
+    add(sizeof(double) * 3 * (size_t)nk);
+  }
+  if ((rc = ensure_workspace(ctx, need + 4096))) return rc;
+  Carve cv{(char*)ctx->ws, ctx->ws_bytes};
+  if ((rc = check_cuda(ctx, cudaMemset2DAsync(dcprod, 16 * ldd, 0, 16 * npair, 3, s), "zero dcprod"))) return rc;
+  double2* out = reinterpret_cast<double2*>(dcprod);
+  if (ng > 0) {
+    double2* O = cv.take<double2>((size_t)ng * ng);
+    double2* R = cv.take<double2>((size_t)ng * nkn);
+    double2* Bq = cv.take<double2>((size_t)ng * nkn * 3);
+    int* G = cv.take<int>(3 * (size_t)ng);
+    double2* CS = cv.take<double2>((size_t)ns * ns * ns);
+    double* kc = cv.take<double>(3 * (size_t)nk);
+    if (!cv.ok) return set_error(ctx, SPX_ENOMEM, "momentum scratch");
+    std::vector<double> kch(3 * (size_t)nk);
+    for (int k = 0; k < nk; ++k)
+      for (int x = 0; x < 3; ++x)
+        kch[3 * k + x] = d->rlat[x] * d->kpt[3 * k] + d->rlat[x + 3] * d->kpt[3 * k + 1] +
+                         d->rlat[x + 6] * d->kpt[3 * k + 2];
+    if ((rc = check_cuda(ctx, cudaMemcpyAsync(G, d->gpt, sizeof(int) * 3 * ng, cudaMemcpyHostToDevice, s), "copy G")) ||
+        (rc = check_cuda(ctx, cudaMemcpyAsync(CS, d->cstep, 16 * (size_t)ns * ns * ns, cudaMemcpyHostToDevice, s), "copy cstep")) ||
+        (rc = check_cuda(ctx, cudaMemcpyAsync(kc, kch.data(), sizeof(double) * 3 * nk, cudaMemcpyHostToDevice, s), "copy k")) ||
+        (rc = check_cuda(ctx, cudaStreamSynchronize(s), "copy k")) ||
+        (rc = check_cuda(ctx, cudaMemsetAsync(R, 0, sizeof(double2) * (size_t)ng * nkn, s), "zero R")))
+      return rc;
+    olap_conj_kernel<<<std::min<int64_t>(((int64_t)ng * ng + 255) / 256, (int64_t)ctx->num_sms * 16), 256, 0, s>>>(
+        G, ng, CS, sr, O);
+    if ((rc = check_cuda(ctx, cudaGetLastError(), "olap_conj_kernel launch"))) return rc;
+    // R(i, kn) = conj(vec1_kn(i)) = sum_j conj(O)(i, j) conj(cpw_occ(kn, j))
+    ZgParams p1{};
+    p1.A = O;
+    p1.a_mcontig = 1;
+    p1.lda = ng;
+    p1.B = reinterpret_cast<const double2*>(cpw_occ);
+    p1.sBc = ng;
+    p1.ncin = (int)nkn;
+    p1.O = R;
+    p1.sOc = ng;
+    p1.alpha_v = make_double2(1.0, 0.0);
+    p1.M = ng;
+    p1.ncol = (int)nkn;
+    p1.K = ng;
+    p1.nb1 = 1;
+    if ((rc = launch_zgemm(ctx, p1, 1, s))) return rc;
+    Mat3 rl;
+    for (int i = 0; i < 9; ++i) rl.r[i] = d->rlat[i];
+    mom_pw_rhs_kernel<<<std::min<int64_t>(((int64_t)ng * nkn + 255) / 256, (int64_t)ctx->num_sms * 16), 256, 0, s>>>(
+        R, ng, (int)nkn, nocc, G, kc, rl, Bq);
+    if ((rc = check_cuda(ctx, cudaGetLastError(), "mom_pw_rhs_kernel launch"))) return rc;
+    // momentum(n', n, k, x) += sum_G cpw_unocc(k, n', G) conj(Bq(k, n, x, G))
+    ZgParams p2{};
+    p2.A = reinterpret_cast<const double2*>(cpw_unocc);
+    p2.lda = ng;
+    p2.sA1 = (int64_t)nunocc * ng;
+    p2.B = Bq;
+    p2.sB1 = (int64_t)nocc * 3 * ng;
+    p2.sBn = 3 * (int64_t)ng;
+    p2.sBc = ng;
+    p2.ncin = 3;
+    p2.O = out;
+    p2.sO1 = (int64_t)nocc * nunocc;
+    p2.sOn = nunocc;
+    p2.sOc = ldd;
+    p2.alpha_v = make_double2(1.0, 0.0);
+    p2.M = nunocc;
+    p2.ncol = 3 * nocc;
+    p2.K = ng;
+    p2.nb1 = nk;
+    if ((rc = launch_zgemm(ctx, p2, nk, s))) return rc;
+  }
+  if (d->natom > 0) {
+    int* d_rp = cv.take<int>(mp.rp.size());
+    int* d_ci = cv.take<int>(std::max<size_t>(mp.ci.size(), 1));
+    double2* d_cv = cv.take<double2>(std::max<size_t>(mp.cv.size(), 1));
+    double2* V = cv.take<double2>((size_t)nkn * d->natom * 3 * mp.maxlm);
+    if (!cv.ok) return set_error(ctx, SPX_ENOMEM, "momentum scratch");
+    if ((rc = check_cuda(ctx, cudaMemcpyAsync(d_rp, mp.rp.data(), sizeof(int) * mp.rp.size(), cudaMemcpyHostToDevice, s), "copy map")) ||
+        (!mp.ci.empty() && (rc = check_cuda(ctx, cudaMemcpyAsync(d_ci, mp.ci.data(), sizeof(int) * mp.ci.size(), cudaMemcpyHostToDevice, s), "copy map"))) ||
+        (!mp.cv.empty() && (rc = check_cuda(ctx, cudaMemcpyAsync(d_cv, mp.cv.data(), sizeof(double2) * mp.cv.size(), cudaMemcpyHostToDevice, s), "copy map"))) ||
+        (rc = check_cuda(ctx, cudaStreamSynchronize(s), "copy map")))
+      return rc;
+    mom_expand_kernel<<<dim3(nocc, d->natom, nk), 256, sizeof(double2) * mp.maxlm, s>>>(
+        reinterpret_cast<const double2*>(cmt_occ), d->natom, mp.maxlm, nocc, d_rp, d_ci, d_cv, V);
+    if ((rc = check_cuda(ctx, cudaGetLastError(), "mom_expand_kernel launch"))) return rc;
+    // one launch per atom (the atoms add into the same outputs)
+    for (int a = 0; a < d->natom; ++a) {
+      ZgParams p3{};
+      p3.A = reinterpret_cast<const double2*>(cmt_unocc) + (int64_t)a * mp.maxlm;
+      p3.lda = (int64_t)d->natom * mp.maxlm;
+      p3.sA1 = (int64_t)nunocc * d->natom * mp.maxlm;
+      p3.B = V + (int64_t)a * 3 * mp.maxlm;
+      p3.sB1 = (int64_t)nocc * d->natom * 3 * mp.maxlm;
+      p3.sBn = (int64_t)d->natom * 3 * mp.maxlm;
+      p3.sBc = mp.maxlm;
+      p3.ncin = 3;
+      p3.O = out;
+      p3.sO1 = (int64_t)nocc * nunocc;
+      p3.sOn = nunocc;
+      p3.sOc = ldd;
+      p3.alpha_v = make_double2(0.0, -1.0);   // 1 / i
+      p3.M = nunocc;
+      p3.ncol = 3 * nocc;
+      p3.K = mp.maxlm;
+      p3.nb1 = nk;
+      if ((rc = launch_zgemm(ctx, p3, nk, s))) return rc;
+    }
+  }
+  mom_scale_kernel<<<std::min<int64_t>((3 * npair + 255) / 256, (int64_t)ctx->num_sms * 16), 256, 0, s>>>(
+      out, ldd, npair, ediff, 1.0 / std::sqrt(d->vol));
+  return check_cuda(ctx, cudaGetLastError(), "mom_scale_kernel launch");
+}

@@ -103,3 +103,31 @@ def chi0_from_coeffs(ctx: Context, mt, pw, cmt_occ, cmt_unocc, cpw_occ, cpw_unoc
         C.byref(st) if st is not None else None)
     ctx._check(rc, "spx_chi0_from_coeffs_dev")
     return _stats(st) if st is not None else None
+
+
+class MomDesc:
+    """spx_mom_desc over host arrays kept alive by this object (momentum matrix of the
+    q -> 0 head and wings)."""
+
+    def __init__(self, m: dict):
+        self.qmat1 = np.asfortranarray(m["qmat1"], dtype=np.float64)
+        self.qmat2 = np.asfortranarray(m["qmat2"], dtype=np.float64)
+        self.gpt = np.ascontiguousarray(m["gpt"], dtype=np.int32)
+        self.kpt = np.ascontiguousarray(m["kpt"], dtype=np.float64)
+        self.rlat = np.asfortranarray(m["rlat"], dtype=np.float64)
+        self.cstep = np.ascontiguousarray(m["cstep"], dtype=np.complex128)
+        self.c = _lib.spx_mom_desc(int(m["natom"]), int(m["lcut"]), int(m["nrad"]), self.gpt.shape[0],
+                                   self.qmat1.ctypes.data, self.qmat2.ctypes.data, self.gpt.ctypes.data,
+                                   self.kpt.ctypes.data, self.rlat.ctypes.data, self.cstep.ctypes.data,
+                                   int(m["step_radius"]), 0, float(m["vol"]))
+
+
+def dcprod_dev(ctx: Context, mom: MomDesc, nk: int, nocc: int, nunocc: int, cmt_occ, cmt_unocc,
+               cpw_occ, cpw_unocc, dcprod, ediff=None, stream=None) -> None:
+    """dcprod (3, ldd) complex128 == Fortran (ldd, 3): momentum / sqrt(vol) / ediff
+    (src/dwavefproducts.f:89-330, src/susceptibility.f:848-870)."""
+    ldd = dcprod.shape[1]
+    rc = ctx.lib.spx_dcprod_dev(ctx.handle, C.byref(mom.c), nk, nocc, nunocc, _ptr(cmt_occ), _ptr(cmt_unocc),
+                                _ptr(cpw_occ), _ptr(cpw_unocc), _ptr(ediff), _ptr(dcprod), ldd,
+                                torch_stream(stream, dcprod))
+    ctx._check(rc, "spx_dcprod_dev")
