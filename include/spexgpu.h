@@ -68,7 +68,8 @@ typedef struct spx_options {
   int32_t chunk_pairs;      /* band pairs per streamed chunk, 0 = auto           */
   int32_t timeout_ms;       /* bound on every device-side wait, 0 = 4000 ms      */
   int32_t split_variant;    /* split-path kernel: 0 auto, 1 one CTA per tile,
-                               2 CTA pair (tcgen05 cta_group::2)                 */
+                               2 CTA pair (tcgen05 cta_group::2), 3 the persistent
+                               schedule with its own preparation warps           */
   int32_t products;         /* interstitial product GEMM: SPX_PRODUCTS_*         */
 } spx_options;
 
@@ -389,16 +390,17 @@ int spx_chi0_batched(spx_ctx* ctx, int32_t nq, const spx_q_desc* q, int32_t nw,
 
 /* Split-path tuning table of a context: per (N_MB bucket, pair bucket, nw) the
  * kernel variant and slab size that measured fastest on a probe of that shape,
- * for single calls (variant 1 or 2) and for the persistent batched schedule
- * (variant 3, with its tile shape). */
+ * for single calls (variant 1, 2 or 3) and for the batched schedule (variant 4,
+ * with its tile shape). */
 typedef struct spx_tune_entry {
   int32_t nbas_bucket;      /* ceil(nbas / 128)                                        */
   int32_t npair_bucket;     /* 0: npair <= 16384, 1: <= 32768, 2: more                 */
   int32_t nw;
-  int32_t variant;          /* 1 one CTA per tile, 2 CTA pair, 3 persistent batched    */
+  int32_t variant;          /* single calls: 1 one CTA per tile, 2 CTA pair, 3 the
+                               persistent schedule; 4 an entry of the batched table   */
   int32_t slab_pairs;
-  int32_t tile;             /* variant 3: tile columns (64 or 32) + 256 * pipeline
-                               stages (3 or 4); 0 otherwise                           */
+  int32_t tile;             /* variants 3 and 4: tile columns (64 or 32) + 256 *
+                               pipeline stages (3 or 4); 0 otherwise                  */
   double  tflops;           /* measured throughput of the chosen configuration        */
 } spx_tune_entry;
 

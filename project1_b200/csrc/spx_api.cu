@@ -38,6 +38,39 @@ int split_chi0_slab(spx_ctx*, const double2*, int64_t, int64_t, int, const doubl
                     int, double2*, void*, size_t, cudaStream_t, int*, int variant, int slab);
 size_t split_workspace_bytes(int64_t P, int N, int nw);
 size_t split_workspace_bytes_real(int64_t P, int N, int nw);
+size_t pb_single_bytes(int64_t P, int N, int nw, int slab);
+int pb_single(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N, const double* ediff,
+              const double* wscale, double scale_all, int nw, const double* omega, double2* out,
+              int tile, int slab, char* scratch, size_t scratch_bytes, cudaStream_t s, int* launches);
+
+// The split variant and slab a call of this shape runs with: the context's forced
+// variant, else the tuning table's, else the CTA-pair kernel with 32768-pair slabs.
+static void split_choice(spx_ctx* ctx, int N, int64_t P, int nw, int* variant, int* slab, int* tile) {
+  *variant = ctx->opt.split_variant;
+  *slab = 0;
+  *tile = 64 + 3 * 256;
+  spx_tune_entry te;
+  if (*variant == 0 && spx_tune_lookup(ctx, N, P, nw, &te) == SPX_OK) {
+    *variant = te.variant;
+    *slab = te.slab_pairs;
+    if (te.tile) *tile = te.tile;
+  }
+}
+
+// Scratch of the split path for a call of this shape (the persistent schedule's
+// buffers when that is the variant in force).
+static size_t split_scratch_bytes(spx_ctx* ctx, int64_t P, int N, int nw) {
+  int variant, slab, tile;
+  split_choice(ctx, N, P, nw, &variant, &slab, &tile);
+  size_t b = split_workspace_bytes(P, N, nw);
+  // the host path cuts P into chunks whose buckets may choose differently: any
+  // persistent entry for this width sizes the scratch for it
+  bool persistent = variant == 3;
+  for (const auto& e : ctx->tune)
+    if (e.variant == 3 && e.nw == nw) persistent = true;
+  if (persistent) b = std::max(b, pb_single_bytes(P, N, nw, 32768));
+  return b;
+}
 int split_chi0_real_slab(spx_ctx*, const double*, int64_t, int64_t, int, const double*, int64_t,
                          int, double*, void*, size_t, cudaStream_t, int*);
 int launch_chi0_fp64_real(spx_ctx*, const double*, int64_t, int64_t, int, const double*, int64_t,
@@ -189,15 +222,18 @@ static int chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int
   } else {
     // kernel variant and slab from the context's tuning table when the caller left
     // the variant open and the table has this shape (smaller slabs need less scratch)
-    int variant = 0, slab = 0;
-    spx_tune_entry te;
-    if (ctx->opt.split_variant == 0 && spx_tune_lookup(ctx, N, P, nw, &te) == SPX_OK) {
-      variant = te.variant;
-      slab = te.slab_pairs;
+    int variant, slab, tile;
+    split_choice(ctx, N, P, nw, &variant, &slab, &tile);
+    if (variant == 3) {
+      // the persistent schedule forms its weights from ediff itself
+      timing_mark(ctx, s, 1);
+      rc = pb_single(ctx, M, ldc, P, N, ediff, wscale, scale_all, nw, omega, out, tile,
+                     slab > 0 ? slab : 32768, (char*)split_ws, split_ws_bytes, s, launches);
+    } else {
+      // the split path marks its own preparation / accumulation phases
+      rc = split_chi0_slab(ctx, M, ldc, P, N, W, ldw, nw, out, split_ws, split_ws_bytes, s,
+                           launches, variant == 3 ? 0 : variant, slab);
     }
-    // the split path marks its own preparation / accumulation phases
-    rc = split_chi0_slab(ctx, M, ldc, P, N, W, ldw, nw, out, split_ws, split_ws_bytes, s,
-                         launches, variant, slab);
   }
   timing_mark(ctx, s, 2);
   return rc;
@@ -376,7 +412,7 @@ extern "C" int spx_chi0_accumulate_dev(spx_ctx* ctx, const double* cprod, int64_
   cudaStream_t s = pick_stream(ctx, stream);
   const int64_t ldw = (int64_t)align_up((size_t)npair, 16);
   size_t wbytes = align_up(sizeof(double) * (size_t)ldw * nw, 256);
-  size_t sbytes = precision == SPX_SPLIT ? split_workspace_bytes(npair, nbas, nw) : 0;
+  size_t sbytes = precision == SPX_SPLIT ? split_scratch_bytes(ctx, npair, nbas, nw) : 0;
   if ((rc = ensure_workspace(ctx, wbytes + sbytes))) return rc;
   double* W = (double*)ctx->ws;
   void* sws = (char*)ctx->ws + wbytes;
@@ -520,7 +556,7 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
   const size_t e_bytes = align_up(sizeof(double) * (size_t)slab, 256);
   const size_t om_bytes = align_up(sizeof(double) * (size_t)nw, 256);
   const size_t w_bytes = align_up(sizeof(double) * (size_t)slab * nw, 256);
-  const size_t s_bytes = precision == SPX_SPLIT ? split_workspace_bytes(slab, nbas, nw) : 0;
+  const size_t s_bytes = precision == SPX_SPLIT ? split_scratch_bytes(ctx, slab, nbas, nw) : 0;
   size_t total = out_bytes + nslab_buf * (slab_bytes + 2 * e_bytes) + om_bytes + w_bytes + s_bytes;
   if ((rc = ensure_workspace(ctx, total))) return rc;
   char* base = (char*)ctx->ws;
@@ -675,7 +711,7 @@ extern "C" int spx_chi0_from_coeffs_dev(spx_ctx* ctx, const spx_mt_desc* mt,
                                      wfprod_pw_workspace(pw, nk, nocc, nunocc, split_products));
   const int64_t ldw = ldc;
   const size_t w_bytes = align_up(sizeof(double) * (size_t)ldw * nw, 256);
-  const size_t s_bytes = precision == SPX_SPLIT ? split_workspace_bytes(npair, nbas, nw) : 0;
+  const size_t s_bytes = precision == SPX_SPLIT ? split_scratch_bytes(ctx, npair, nbas, nw) : 0;
   const size_t scratch = std::max(prod_bytes, w_bytes + s_bytes);
   if ((rc = ensure_workspace(ctx, m_bytes + scratch))) return rc;
   double2* M = (double2*)ctx->ws;

@@ -44,7 +44,12 @@ struct PbConfig {
   int bn, stages;
 };
 int pb_run(spx_ctx* ctx, int nq, const spx_q_desc* q, int nw, const double* omega, int flags,
-           cudaStream_t s, int* launches, const PbConfig* force, int force_slab);
+           cudaStream_t s, int* launches, const PbConfig* force, int force_slab, char* scratch,
+           size_t scratch_bytes);
+size_t pb_single_bytes(int64_t P, int N, int nw, int slab);
+int pb_single(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N, const double* ediff,
+              const double* wscale, double scale_all, int nw, const double* omega, double2* out,
+              int tile, int slab, char* scratch, size_t scratch_bytes, cudaStream_t s, int* launches);
 
 constexpr int kDefaultVariant = 2;
 constexpr int kDefaultSlab = 32768;
@@ -57,13 +62,13 @@ static int npair_bucket(int64_t P) { return P <= 16384 ? 0 : (P <= 32768 ? 1 : 2
 static const spx_tune_entry* find_tune(const spx_ctx* ctx, int N, int64_t P, int nw) {
   const int nb = nbas_bucket(N), pb = npair_bucket(P);
   for (const auto& e : ctx->tune)
-    if (e.variant != 3 && e.nbas_bucket == nb && e.npair_bucket == pb && e.nw == nw) return &e;
+    if (e.variant != 4 && e.nbas_bucket == nb && e.npair_bucket == pb && e.nw == nw) return &e;
   return nullptr;
 }
 
 static void store_tune(spx_ctx* ctx, const spx_tune_entry& t) {
   for (auto& e : ctx->tune)
-    if ((e.variant == 3) == (t.variant == 3) && e.nbas_bucket == t.nbas_bucket &&
+    if ((e.variant == 4) == (t.variant == 4) && e.nbas_bucket == t.nbas_bucket &&
         e.npair_bucket == t.npair_bucket && e.nw == t.nw) {
       e = t;
       return;
@@ -84,8 +89,10 @@ static QPlan plan_q(const spx_ctx* ctx, const spx_q_desc& q, int nw, int precisi
   if (precision == SPX_SPLIT && (p.variant == 0 || p.slab == 0)) {
     const spx_tune_entry* t = find_tune(ctx, q.nbas, q.npair, nw);
     if (p.variant == 0)
-      p.variant = t ? t->variant
-                    : (ctx->opt.split_variant ? ctx->opt.split_variant : kDefaultVariant);
+      p.variant = t && t->variant <= 2 ? t->variant
+                                       : (ctx->opt.split_variant == 1 || ctx->opt.split_variant == 2
+                                              ? ctx->opt.split_variant
+                                              : kDefaultVariant);
     if (p.slab == 0) p.slab = t ? t->slab_pairs : kDefaultSlab;
   }
   if (p.slab <= 0) p.slab = kDefaultSlab;
@@ -205,7 +212,7 @@ extern "C" int spx_chi0_batched(spx_ctx* ctx, int32_t nq, const spx_q_desc* q, i
     cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
     if (stats) cudaEventRecord(e0, s);
     int launches = 0;
-    if ((rc = pb_run(ctx, nq, q, nw, omega, flags, s, &launches, nullptr, 0))) return rc;
+    if ((rc = pb_run(ctx, nq, q, nw, omega, flags, s, &launches, nullptr, 0, nullptr, 0))) return rc;
     if (stats) {
       cudaEventRecord(e1, s);
       if ((rc = collect_status(ctx, s, "chi0_batched"))) return rc;
@@ -333,7 +340,8 @@ extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int
   const int64_t npack = (int64_t)nbas * (nbas + 1) / 2;
   const int slabs[2] = {16384, 32768};
   size_t sws = 0;
-  for (int sl : slabs) sws = std::max(sws, split_workspace_bytes(P, nbas, nw, sl));
+  for (int sl : slabs)
+    sws = std::max({sws, split_workspace_bytes(P, nbas, nw, sl), pb_single_bytes(P, nbas, nw, sl)});
   const size_t m_bytes = align_up(sizeof(double2) * (size_t)ld * nbas, 256);
   const size_t o_bytes = align_up(sizeof(double2) * (size_t)npack * nw, 256);
   const size_t e_bytes = align_up(sizeof(double) * (size_t)ld, 256);
@@ -368,14 +376,20 @@ extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int
   best.tflops = -1;
   const double flops = 8.0 * (double)nbas * nbas * (double)P * nw;
   cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
-  for (int variant = 1; variant <= 2; ++variant)
+  // variants 1 and 2: the slab kernels with the quantizer beside them; 3: the
+  // persistent schedule (its own preparation warps, 64 x 64 tiles, 3 stages)
+  for (int variant = 1; variant <= 3; ++variant)
     for (int sl : slabs) {
       if (sl == 32768 && npair <= 16384) continue;  // one slab either way
       int launches = 0;
       float best_ms = 1e30f;
       for (int rep = 0; rep < 2; ++rep) {  // the first run warms up
         cudaEventRecord(e0, s);
-        rc = split_chi0_slab(ctx, M, ld, P, nbas, W, ld, nw, O, S, sws, s, &launches, variant, sl);
+        if (variant == 3)
+          rc = pb_single(ctx, M, ld, P, nbas, E, nullptr, 1.0, nw, OM, O, 64 + 3 * 256, sl, (char*)S,
+                         sws, s, &launches);
+        else
+          rc = split_chi0_slab(ctx, M, ld, P, nbas, W, ld, nw, O, S, sws, s, &launches, variant, sl);
         if (rc) return rc;
         cudaEventRecord(e1, s);
         if ((rc = collect_status(ctx, s, "autotune"))) return rc;
@@ -388,6 +402,7 @@ extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int
         best.tflops = tf;
         best.variant = variant;
         best.slab_pairs = sl;
+        best.tile = variant == 3 ? 64 + 3 * 256 : 0;
       }
     }
   store_tune(ctx, best);
@@ -460,7 +475,7 @@ extern "C" int spx_tune_load(spx_ctx* ctx, const char* path) {
       return set_error(ctx, SPX_EINVAL, "malformed tuning entry");
     json_field(obj, "tflops", &tf);
     json_field(obj, "tile", &tile);
-    if (var < 1 || var > 3 || sl < 64 || sl > 32768 || nb < 1 || nw < 1 || pb < 0 || pb > 2 ||
+    if (var < 1 || var > 4 || sl < 64 || sl > 32768 || nb < 1 || nw < 1 || pb < 0 || pb > 2 ||
         tile < 0 || tile > 4 * 256 + 64)
       return set_error(ctx, SPX_EINVAL, "tuning entry out of range");
     spx_tune_entry t{};

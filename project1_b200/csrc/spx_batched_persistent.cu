@@ -741,7 +741,7 @@ static int pb_npair_bucket(int64_t P) { return P <= 16384 ? 0 : (P <= 32768 ? 1 
 
 static const spx_tune_entry* pb_find_tune(const spx_ctx* ctx, int N, int64_t P, int nw) {
   for (const auto& e : ctx->tune)
-    if (e.variant == 3 && e.nbas_bucket == pb_nbas_bucket(N) && e.npair_bucket == pb_npair_bucket(P) &&
+    if (e.variant == 4 && e.nbas_bucket == pb_nbas_bucket(N) && e.npair_bucket == pb_npair_bucket(P) &&
         e.nw == nw)
       return &e;
   return nullptr;
@@ -766,7 +766,8 @@ static uint64_t pb_fnv(uint64_t h, const void* p, size_t n) {
 // descriptor's, else the tuned, else 16384; tile shape: the tuned shape of the q
 // with most work, else 64 x 64 with 3 stages (`force` overrides both when set).
 int pb_run(spx_ctx* ctx, int nq, const spx_q_desc* q, int nw, const double* omega, int flags,
-           cudaStream_t s, int* launches, const PbConfig* force, int force_slab) {
+           cudaStream_t s, int* launches, const PbConfig* force, int force_slab, char* scratch,
+           size_t scratch_bytes) {
   std::vector<int> S(nq, PB_DEFAULT_SLAB);
   PbConfig cfg = PB_DEFAULT_CFG;
   double most = -1;
@@ -789,8 +790,15 @@ int pb_run(spx_ctx* ctx, int nq, const spx_q_desc* q, int nw, const double* omeg
   size_t ctr_bytes = 0;
   int rc;
   if (flags & SPX_BATCH_NOGRAPH) {
-    if ((rc = ensure_workspace(ctx, bytes))) return rc;
-    if ((rc = pb_build(ctx, nq, q, S.data(), nw, PB_NSLOT, cfg, omega, (char*)ctx->ws, ctx->ws_bytes,
+    // the caller's scratch, or the workspace from its start
+    if (scratch) {
+      if (scratch_bytes < bytes) return set_error(ctx, SPX_EINVAL, "persistent schedule: scratch too small");
+    } else {
+      if ((rc = ensure_workspace(ctx, bytes))) return rc;
+      scratch = (char*)ctx->ws;
+      scratch_bytes = ctx->ws_bytes;
+    }
+    if ((rc = pb_build(ctx, nq, q, S.data(), nw, PB_NSLOT, cfg, omega, scratch, scratch_bytes,
                        &prm, &ctr, &ctr_bytes)))
       return rc;
     if ((rc = pb_launch(ctx, prm, cfg, ctr, ctr_bytes, s))) return rc;
@@ -848,6 +856,42 @@ int pb_run(spx_ctx* ctx, int nq, const spx_q_desc* q, int nw, const double* omeg
   return check_cuda(ctx, cudaGraphLaunch(hit->exec, s), "graph launch");
 }
 
+// Scratch of one call through the persistent schedule: nbas x npair explicit M,
+// slabs of `slab` pairs.
+size_t pb_single_bytes(int64_t P, int N, int nw, int slab) {
+  spx_q_desc d;
+  std::memset(&d, 0, sizeof(d));
+  d.nbas = N;
+  d.npair = P;
+  d.cprod = reinterpret_cast<const double*>(16);   // explicit M: no generation buffer
+  const int S = std::max(SP_KB, std::min(SP_SLAB, slab / SP_KB * SP_KB));
+  return pb_plan_bytes(1, &d, &S, nw, PB_NSLOT);
+}
+
+// One spx_chi0_accumulate_dev-style call (HILBERT NONE weights from ediff, explicit
+// M on the device) through the persistent schedule with tile code `tile` and slab
+// `slab`, in the caller's scratch.
+int pb_single(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N, const double* ediff,
+              const double* wscale, double scale_all, int nw, const double* omega, double2* out,
+              int tile, int slab, char* scratch, size_t scratch_bytes, cudaStream_t s, int* launches) {
+  spx_q_desc d;
+  std::memset(&d, 0, sizeof(d));
+  d.nbas = N;
+  d.npair = P;
+  d.cprod = reinterpret_cast<const double*>(M);
+  d.ldc = ldc;
+  d.ediff = ediff;
+  d.wscale = wscale;
+  d.scale_all = scale_all;
+  d.susceph = reinterpret_cast<double*>(out);
+  const PbConfig cfg = pb_cfg_of(tile);
+  int n = 0;
+  const int rc = pb_run(ctx, 1, &d, nw, omega, SPX_BATCH_NOGRAPH, s, &n, &cfg, slab > 0 ? slab : PB_DEFAULT_SLAB,
+                        scratch, scratch_bytes);
+  *launches += n + 1;   // the counters' memset and the kernel
+  return rc;
+}
+
 }  // namespace spx
 
 using namespace spx;
@@ -857,7 +901,7 @@ int launch_gen_normal(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, double, do
 }
 
 // Times the persistent schedule's tile shapes and slab sizes on a seeded probe of one
-// q (M generated on the device), keeps the fastest as a variant-3 entry.
+// q (M generated on the device), keeps the fastest as a variant-4 entry.
 extern "C" int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
                                     spx_tune_entry* out) {
   if (!ctx) return SPX_EINVAL;
@@ -890,7 +934,7 @@ extern "C" int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, i
   best.nbas_bucket = pb_nbas_bucket(nbas);
   best.npair_bucket = pb_npair_bucket(npair);
   best.nw = nw;
-  best.variant = 3;
+  best.variant = 4;
   best.tflops = -1;
   spx_q_desc d;
   std::memset(&d, 0, sizeof(d));
@@ -911,7 +955,7 @@ extern "C" int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, i
       for (int rep = 0; rep < 2 && !rc; ++rep) {
         int launches = 0;
         cudaEventRecord(e0, s);
-        rc = pb_run(ctx, 1, &d, nw, OM, SPX_BATCH_NOGRAPH, s, &launches, &cfgs[ci], sl);
+        rc = pb_run(ctx, 1, &d, nw, OM, SPX_BATCH_NOGRAPH, s, &launches, &cfgs[ci], sl, nullptr, 0);
         if (rc) break;
         cudaEventRecord(e1, s);
         if ((rc = collect_status(ctx, s, "batched autotune"))) break;
@@ -931,7 +975,7 @@ extern "C" int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, i
   if (rc) return rc;
   bool stored = false;
   for (auto& e : ctx->tune)
-    if (e.variant == 3 && e.nbas_bucket == best.nbas_bucket && e.npair_bucket == best.npair_bucket &&
+    if (e.variant == 4 && e.nbas_bucket == best.nbas_bucket && e.npair_bucket == best.npair_bucket &&
         e.nw == nw) {
       e = best;
       stored = true;

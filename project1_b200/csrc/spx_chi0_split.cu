@@ -560,9 +560,10 @@ __global__ void split_wstat_kernel(const double* __restrict__ W, int64_t ldw, in
 // rows 128 (i / 64) + 2 (i % 64) (Re) and the next one (Im). For frequency f the
 // planes f*6 + t hold the digits t of round(x |G| / s) (the folded operand), and,
 // when the frequency's weights have both signs, planes f*6 + 3 + t those of
-// round(x G / s). At most 128 registers a thread: a block fits on an SM beside the
-// accumulation kernel's CTA, so slab s+1 is prepared while slab s accumulates.
-__global__ void __launch_bounds__(128, 4)
+// round(x G / s). At most 96 registers a thread: a block fits on an SM beside the
+// accumulation kernel's CTA (192 threads x 256 registers), so slab s+1 is prepared
+// while slab s accumulates.
+__global__ void __launch_bounds__(128, 5)
     split_quantize_kernel(const double2* __restrict__ M, int64_t ldc, int64_t p0, int len,
                           int nchunk, int N, int npad, int64_t R, int64_t Ps, int nw,
                           const double* __restrict__ sA, const int* __restrict__ wsgn,

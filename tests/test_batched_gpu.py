@@ -127,7 +127,7 @@ def test_variants_and_slabs_agree(ctx):
 
 def test_autotune_table_roundtrip(ctx, tmp_path):
     e = ctx.autotune_split(200, 40000, 3)
-    assert e["variant"] in (1, 2) and e["slab_pairs"] in (16384, 32768) and e["tflops"] > 0
+    assert e["variant"] in (1, 2, 3) and e["slab_pairs"] in (16384, 32768) and e["tflops"] > 0
     assert ctx.tune_lookup(200, 40000, 3) == e
     assert ctx.tune_lookup(200, 40000, 4) is None
     path = tmp_path / "tune.json"
@@ -154,7 +154,7 @@ def test_autotuned_batch(ctx):
     ctx.chi0_batched(qs, omega, flags=_lib.SPX_BATCH_AUTOTUNE, stats=True)
     for q in qs:
         t = ctx.tune_lookup_batched(q["nbas"], q["npair"], 2)
-        assert t is not None and t["variant"] == 3 and t["tile"] in (64 + 3 * 256, 32 + 3 * 256, 32 + 4 * 256)
+        assert t is not None and t["variant"] == 4 and t["tile"] in (64 + 3 * 256, 32 + 3 * 256, 32 + 4 * 256)
         assert torch.isfinite(torch.view_as_real(q["susceph"])).all()
         assert q["susceph"].abs().max() > 0
 
@@ -176,7 +176,7 @@ def _force_tile(c, tmp_path, qs, nw, tile, slab):
     for q in qs:
         n, p = q["nbas"], q["npair"]
         ents.append({"nbas_bucket": (n + 127) // 128, "npair_bucket": 0 if p <= 16384 else (1 if p <= 32768 else 2),
-                     "nw": nw, "variant": 3, "slab_pairs": slab, "tile": tile, "tflops": 1.0})
+                     "nw": nw, "variant": 4, "slab_pairs": slab, "tile": tile, "tflops": 1.0})
     path = tmp_path / f"tile{tile}.json"
     path.write_text(json.dumps({"format": "spexgpu-tune-1", "entries": ents}))
     c.tune_load(path)

@@ -113,6 +113,22 @@ def test_split_cta_pair_equals_single_cta(nbas, npair, nw):
     assert emax <= SPLIT_TOL and fro <= SPLIT_FRO, (emax, fro)
 
 
+@pytest.mark.parametrize("nbas,npair,nw", [(65, 3000, 2), (200, 40000, 3)])
+def test_split_persistent_single_call_equals_slab_kernels(nbas, npair, nw):
+    """Variant 3 (one persistent kernel with its own preparation warps) adds the same
+    slab sums in the same order as the slab kernels (32768-pair slabs for both): the
+    results are identical."""
+    m, d, om = random_case(nbas, npair, nw, seed=nbas * 5 + npair, degfrac=0.01)
+    outs = []
+    for variant in (1, 3):
+        with spx.Context(0, split_variant=variant) as c:
+            outs.append(run_dev(c, m, d, om, None, 0.5, precision="split"))
+    ref = oracle.chi0(m, oracle.weights(d, om, None, 0.5), accurate=True)
+    emax, fro = normalized_error(outs[1], ref, nbas)
+    assert emax <= SPLIT_TOL and fro <= SPLIT_FRO, (emax, fro)
+    assert np.array_equal(outs[0], outs[1])
+
+
 def test_split_host_ramp_equals_device_path(ctx):
     """With default chunking, the host-pointer call streams chunks of 32768, 65536,
     98304, ... pairs. They fall on the 32768-pair exact slabs of the split path, so
