@@ -238,12 +238,27 @@ def bench_config(w, world: int) -> dict:
 
 def int8_ops(N: int, P: int, nw: int, variant: int, slab: int) -> float:
     """int8 ops the accumulation kernel issues for P pairs: 6 digit products per real MAC
-    of each 128 x 128 real-stacked MMA tile (one CTA: the upper 64-blocks; CTA pair: two
-    tiles per pair item), over the slabs padded to 64 pairs, 2 ops per MAC."""
+    of each 128 x 128 real-stacked MMA tile (one CTA or the persistent kernel: the upper
+    64-blocks; CTA pair: two tiles per pair item), over the slabs padded to 64 pairs, 2 ops
+    per MAC."""
     nblk = (N + 63) // 64
-    tiles = nblk * (nblk + 1) // 2 if variant == 1 else 2 * sum(bj // 2 + 1 for bj in range(nblk))
+    tiles = nblk * (nblk + 1) // 2 if variant in (1, 3) else 2 * sum(bj // 2 + 1 for bj in range(nblk))
     pad = sum(((min(slab, P - s0) + 63) // 64) * 64 for s0 in range(0, P, slab))
     return 2.0 * 6 * 128 * 128 * tiles * pad * nw
+
+
+def fp64_roofline(ctx, N: int, achieved: float) -> dict:
+    """Roofline of the FP64 accumulation (DMMA) against this GPU's DMMA rate, measured
+    here by the library's own in-register DMMA loop. The kernel computes only the upper
+    64 x 64 tiles, so the rate the pipe executes is the algorithmic rate times the
+    executed share of the full Gram."""
+    peak = ctx.measure_dmma_peak()
+    nblk = (N + 63) // 64
+    share = nblk * (nblk + 1) / 2 * 64 * 64 / (N * N)
+    return {"bound": "tensor (FP64 DMMA)", "achieved": achieved, "peak": peak, "unit": UNIT,
+            "frac": achieved / peak, "executed_tflops": achieved * share, "executed_frac": achieved * share / peak,
+            "executed_share_of_full_gram": share, "traffic": None,
+            "peak_source": "measured: spx_measure_dmma_peak (mma.sync m16n8k8 f64 loop, CUDA events)"}
 
 
 def measured_traffic(kernel: str, nbas: int, nw: int, slab: int, npair_step: int):
@@ -289,7 +304,8 @@ def run_ours(args):
     Pr = p_hi - p_lo
     N, nw = w.nbas, w.nw
     npk = spx.npack(N)
-    ctx = spx.Context(local, split_variant=args.variant)
+    # a pinned slab travels in the tuning table, which names the variant too
+    ctx = spx.Context(local, split_variant=0 if args.slab else args.variant)
     stream = torch.cuda.current_stream(dev)
 
     # inputs resident in HBM: M (N, P) column blocks generated on device, bit-identical
@@ -358,8 +374,21 @@ def run_ours(args):
     if args.precision:
         head = args.precision
 
-    # the autotuner picks the accumulation kernel and slab for this shape (untimed)
-    tuned = ctx.autotune_split(N, Pr, nw) if head == "split" and args.autotune else None
+    # the autotuner picks the accumulation kernel and slab for this shape (untimed);
+    # --slab pins one (profiling) through a one-entry tuning table
+    tuned = None
+    if head == "split" and args.slab:
+        import tempfile
+        tuned = {"variant": args.variant or 1, "slab_pairs": args.slab, "tflops": 0.0}
+        entry = {"nbas_bucket": (N + 127) // 128, "npair_bucket": 0 if Pr <= 16384 else (1 if Pr <= 32768 else 2),
+                 "nw": nw, "variant": tuned["variant"], "slab_pairs": args.slab,
+                 "tile": 64 + 3 * 256 if tuned["variant"] == 3 else 0, "tflops": 0.0}
+        with tempfile.TemporaryDirectory() as td:
+            with open(os.path.join(td, "tune.json"), "w") as fh:
+                json.dump({"format": "spexgpu-tune-1", "entries": [entry]}, fh)
+            ctx.tune_load(os.path.join(td, "tune.json"))
+    elif head == "split" and args.autotune:
+        tuned = ctx.autotune_split(N, Pr, nw)
     sampler = ClockSampler(local) if rank == 0 else None
     ms, gram_ms, launches, clocks = timed(head, args.warmup, args.steps, sampler)
     value = w.flops / (ms * 1e-3) / 1e12   # whole job: all ranks' pairs / max-over-ranks time
@@ -421,7 +450,7 @@ def run_ours(args):
         roof = {"bound": "tensor", "achieved": ach, "peak": bf16s, "unit": UNIT, "frac": ach / bf16s,
                 "traffic": None, "peak_source": f"{src} bf16_tflops_sustained (kernel timed inside a long step)"}
         # the same kernel seen from the int8 pipe it runs on, for the variant and slab that ran
-        variant = tuned["variant"] if tuned else (1 if ctx.split_variant == 1 else 2)
+        variant = tuned["variant"] if tuned else (ctx.split_variant if ctx.split_variant in (1, 3) else 2)
         slab = tuned["slab_pairs"] if tuned else 32768
         ops = int8_ops(N, Pr, nw, variant, slab)
         i8 = ops / (kernel_ms * 1e-3) / 1e12
@@ -429,7 +458,7 @@ def run_ours(args):
                              "achieved_tops": i8, "peak_tops": 2 * bf16s, "frac": i8 / (2 * bf16s),
                              "peak_source": "2 x measured bf16 sustained (int8 peak is 16384 ops/cycle/SM "
                                             "in ncu, twice the bf16 pipe)"}
-        kname = "split_gram_kernel" if variant == 1 else "split_gram2_kernel"
+        kname = {1: "split_gram_kernel", 2: "split_gram2_kernel", 3: "pb_kernel"}.get(variant, "split_gram_kernel")
         tr = measured_traffic(kname, N, nw, slab, Pr)
         if tr:
             nblk = (N + 63) // 64
@@ -438,8 +467,9 @@ def run_ours(args):
             roof["traffic_detail"] = dict(tr, kernel=kname, unit="bytes per launch (one slab, all frequencies)",
                                           operand_plane_bytes_per_launch=3.0 * nw * R * min(slab, Pr))
     else:
-        roof = {"bound": "tensor", "achieved": ach, "peak": None, "unit": UNIT, "frac": None, "traffic": None,
-                "peak_source": "FP64 DMMA has no measured peak on this pool"}
+        roof = fp64_roofline(ctx, N, ach)
+    if fp64 is not None:
+        fp64["roofline"] = fp64_roofline(ctx, N, w.flops * (Pr / P) / (fp64["kernel_ms"] * 1e-3) / 1e12)
 
     if rank == 0:
         res = {
@@ -734,8 +764,11 @@ def main():
     ap.add_argument("--c4-kpts", type=int, default=0, help="override the products workload's k-point count (profiling)")
     ap.add_argument("--precision", choices=["split", "fp64"], default=None,
                     help="force the measured path (profiling captures)")
-    ap.add_argument("--variant", type=int, default=0, choices=[0, 1, 2],
-                    help="accumulation kernel: 1 one CTA per tile, 2 CTA pair, 0 the library's choice")
+    ap.add_argument("--variant", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="accumulation kernel: 1 one CTA per tile, 2 CTA pair, 3 persistent schedule, "
+                         "0 the library's choice")
+    ap.add_argument("--slab", type=int, default=0,
+                    help="pin the split path's slab (pairs per exact accumulation; profiling)")
     ap.add_argument("--kpts", type=int, default=0, help="override the k-point count (profiling)")
     ap.add_argument("--freqs", type=int, default=0, help="override the frequency count (profiling)")
     args = ap.parse_args()

@@ -666,7 +666,7 @@ namespace spx {
 int wfprod_mt_run(spx_ctx*, const spx_mt_desc*, int, int, int, const double2*, const double2*,
                   double2*, int64_t, void*, size_t, cudaStream_t, int*);
 int wfprod_pw_run(spx_ctx*, const spx_pw_desc*, int, int, int, const double2*, const double2*,
-                  double2*, int64_t, int, void*, size_t, cudaStream_t, int*, bool);
+                  double2*, int64_t, int, void*, size_t, cudaStream_t, int*, bool, bool);
 size_t wfprod_mt_workspace(const spx_mt_desc*, int, int);
 size_t wfprod_pw_workspace(const spx_pw_desc*, int, int, int, bool);
 }  // namespace spx
@@ -726,7 +726,7 @@ extern "C" int spx_chi0_from_coeffs_dev(spx_ctx* ctx, const spx_mt_desc* mt,
   if (!rc)
     rc = wfprod_pw_run(ctx, pw, nk, nocc, nunocc, reinterpret_cast<const double2*>(cpw_occ),
                        reinterpret_cast<const double2*>(cpw_unocc), M, ldc, mt->natom * maxllm,
-                       sc, scratch, s, &launches, split_products);
+                       sc, scratch, s, &launches, split_products, /*overwrite: M was zeroed*/ true);
   if (rc) {
     ctx->timing = false;
     return rc;

@@ -338,7 +338,8 @@ extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int
   const int64_t P = std::min<int64_t>(npair, 2 * (int64_t)kDefaultSlab);
   const int64_t ld = (int64_t)align_up((size_t)P, 16);
   const int64_t npack = (int64_t)nbas * (nbas + 1) / 2;
-  const int slabs[2] = {16384, 32768};
+  // smaller slabs cost more epilogues but keep a round's operand blocks in L2
+  const int slabs[3] = {8192, 16384, 32768};
   size_t sws = 0;
   for (int sl : slabs)
     sws = std::max({sws, split_workspace_bytes(P, nbas, nw, sl), pb_single_bytes(P, nbas, nw, sl)});

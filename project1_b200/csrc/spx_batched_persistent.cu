@@ -365,7 +365,9 @@ __global__ void __launch_bounds__(PB_THREADS, 1) pb_kernel(PbParams prm) {
         const PbSlab& sl = prm.slab[k];
         const PbQ& q = prm.q[sl.q];
         const int local = (int)(g - sl.g0);
-        const int f = local / q.ntile, tile = local % q.ntile;
+        const int f = local / q.ntile;
+        const int tile = split_round_tile(local % q.ntile, q.ntile, g - local % q.ntile, gridDim.x);
+        const int jr = (int)((g / gridDim.x) & 1);  // this round's K direction
         int bi, bj;
         pb_decode_tile<BN>(tile, &bi, &bj);
         // the slab's planes must be ready before the first copy
@@ -386,8 +388,9 @@ __global__ void __launch_bounds__(PB_THREADS, 1) pb_kernel(PbParams prm) {
             break;
           }
           mbar_arrive_expect_tx(&sm.full[st], (uint32_t)(SP_SF * (SP_PLANE + (same ? 0 : BROWS * SP_KB))));
-          tma_load_4d(&sm.a[st][0][0], mA, 0, bi * SP_ROWS, ks, za, &sm.full[st]);
-          if (!same) tma_load_4d(&sm.b[st][0][0], mB, 0, bj * BROWS, ks, zb, &sm.full[st]);
+          const int kc = split_k_order(jr, ks, sl.nk);
+          tma_load_4d(&sm.a[st][0][0], mA, 0, bi * SP_ROWS, kc, za, &sm.full[st]);
+          if (!same) tma_load_4d(&sm.b[st][0][0], mB, 0, bj * BROWS, kc, zb, &sm.full[st]);
           issued[st] = true;
           last_ph[st] = ph;
           if (++st == ST) st = 0, ph ^= 1u;
@@ -908,7 +911,7 @@ extern "C" int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, i
   if (nbas <= 0 || npair <= 0 || nw <= 0) return set_error(ctx, SPX_EINVAL, "empty probe");
   if (nbas > 46340) return set_error(ctx, SPX_EINVAL, "nbas too large");
   cudaSetDevice(ctx->device);
-  const int slabs[2] = {16384, 32768};
+  const int slabs[3] = {8192, 16384, 32768};
   const PbConfig cfgs[3] = {{64, 3}, {32, 3}, {32, 4}};
   const int64_t P = std::min<int64_t>(npair, 4 * (int64_t)SP_SLAB);
   const int64_t npack = (int64_t)nbas * (nbas + 1) / 2;

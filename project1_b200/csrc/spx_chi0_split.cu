@@ -47,6 +47,13 @@ namespace spx {
 
 constexpr int SP_ST = 4;               // pipeline stages (one CTA per tile)
 constexpr int SP_THREADS = 192;        // warp 0 TMA, warp 1 MMA + TMEM, warps 2-5 epilogue
+// The one-CTA kernel drains a tile with 8 epilogue warps (warps 2-9; two per TMEM lane
+// quarter, each half of the columns): fewer registers per thread, so the operand
+// quantizer of the next slab keeps more warps resident beside it on every SM.
+constexpr int SP1_EPI = 8;
+constexpr int SP1_THREADS = 64 + 32 * SP1_EPI;
+constexpr int SP1_NC = SP_TILE * 4 / SP1_EPI;  // complex columns per epilogue warp
+constexpr int SP1_REGS = 128;  // 40960 registers: two 96-register quantizer blocks fit beside
 
 struct __align__(1024) SplitSmem {
   uint8_t a[SP_ST][SP_SF][SP_PLANE];
@@ -72,19 +79,20 @@ struct SplitParams {
   uint64_t timeout_ns;
 };
 
-// The epilogue of one tile, run by the four epilogue warps (warp q reads TMEM lanes
-// 32q..32q+31, i.e. rows i = 16q + lane/2, part c = lane & 1). The whole accumulator
-// is read into registers first and released to the MMA warp, so the next item's
-// MMAs overlap this tile's reductions into the output.
-template <class Release>
+// The epilogue of one tile (or of NC of its 64 complex columns, from column j0), run
+// by the epilogue warps (warp q reads TMEM lanes 32q..32q+31, i.e. rows
+// i = 16q + lane/2, part c = lane & 1). The warp's part of the accumulator is read
+// into registers first and released to the MMA warp, so the next item's MMAs overlap
+// this tile's reductions into the output.
+template <int NC = SP_TILE, class Release>
 __device__ __forceinline__ void fold_epilogue(uint32_t tl, int q, int lane, int bi, int bj, int f,
-                                              const SplitParams& prm, Release release) {
+                                              const SplitParams& prm, Release release, int j0 = 0) {
   const int c = lane & 1;
-  double o[SP_TILE];
+  double o[NC];
 #pragma unroll
-  for (int cc = 0; cc < SP_TILE / 8; ++cc) {
+  for (int cc = 0; cc < NC / 8; ++cc) {
     double T[16];
-    load_fold16(tl + (uint32_t)(16 * cc), 128u, T);
+    load_fold16(tl + (uint32_t)(2 * j0 + 16 * cc), 128u, T);
 #pragma unroll
     for (int jj = 0; jj < 8; ++jj) {
       // both lanes of a row pair send their (., Im_j) product to the other one
@@ -98,30 +106,31 @@ __device__ __forceinline__ void fold_epilogue(uint32_t tl, int q, int lane, int 
   const double fac = fold_row_factor(prm.wsgn[f], prm.sA[gil], prm.wmax[f]);
   double* ob = prm.out + 2 * (int64_t)f * prm.npack + 2 * gil + c;
 #pragma unroll
-  for (int jj = 0; jj < SP_TILE; ++jj) {
-    const int gj = bj * SP_TILE + jj;
+  for (int jj = 0; jj < NC; ++jj) {
+    const int gj = bj * SP_TILE + j0 + jj;
     // one add per element per launch: launches are stream-ordered, so the sum is
     // deterministic, and the reduction needs no read round trip
     if (gil <= gj && gj < prm.N) atomicAdd(ob + (int64_t)gj * (gj + 1), fac * prm.sA[gj] * o[jj]);
   }
 }
 
-// The -DINV (real) epilogue: a 128 x 128 tile of real chi, TMEM lane = row i of the
-// block, column = j; read and added 16 columns at a time, then the accumulator is
-// released.
+// The -DINV (real) epilogue: columns [j0, j0 + ncol) of a 128 x 128 tile of real chi,
+// TMEM lane = row i of the block, column = j; read and added 16 columns at a time,
+// then the accumulator is released.
 template <class Release>
 __device__ __forceinline__ void real_epilogue(uint32_t tl, int q, int lane, int bi, int bj, int f,
-                                              const SplitParams& prm, Release release) {
+                                              const SplitParams& prm, Release release, int j0,
+                                              int ncol) {
   const int gi = bi * SP_ROWS + 32 * q + lane;
   const double fac = gi < prm.N ? fold_row_factor(prm.wsgn[f], prm.sA[gi], prm.wmax[f]) : 0.0;
   double* of = prm.out + (int64_t)f * prm.npack + gi;
 #pragma unroll 1
-  for (int cc = 0; cc < SP_ROWS / 16; ++cc) {
+  for (int cc = 0; cc < ncol / 16; ++cc) {
     double T[16];
-    load_fold16(tl + (uint32_t)(16 * cc), 128u, T);
+    load_fold16(tl + (uint32_t)(j0 + 16 * cc), 128u, T);
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-      const int gj = bj * SP_ROWS + 16 * cc + k;
+      const int gj = bj * SP_ROWS + j0 + 16 * cc + k;
       if (gi < prm.N && gi <= gj && gj < prm.N)
         atomicAdd(of + (int64_t)gj * (gj + 1) / 2, fac * prm.sA[gj] * T[k]);
     }
@@ -130,7 +139,7 @@ __device__ __forceinline__ void real_epilogue(uint32_t tl, int q, int lane, int 
 }
 
 template <bool REAL>
-__global__ void __launch_bounds__(SP_THREADS, 1)
+__global__ void __maxnreg__(SP1_REGS)
     split_gram_kernel(const __grid_constant__ CUtensorMap mapF, SplitParams prm) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   SplitSmem& sm = *reinterpret_cast<SplitSmem*>(
@@ -143,7 +152,7 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       mbar_init(&sm.empty[s], 1);
     }
     mbar_init(&sm.tfull, 1);
-    mbar_init(&sm.tempty, 4);
+    mbar_init(&sm.tempty, SP1_EPI);
     mbar_init(&sm.mdone, 1);
     fence_barrier_init();
   }
@@ -162,10 +171,11 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       uint32_t last_ph[SP_ST];
       for (int s = 0; s < SP_ST; ++s) issued[s] = false, last_ph[s] = 0;
       bool ok = true;
-      for (int item = blockIdx.x; item < prm.nitems && ok; item += gridDim.x) {
+      int j = 0;
+      for (int item = blockIdx.x; item < prm.nitems && ok; item += gridDim.x, ++j) {
         const int f = item / prm.ntile;
         int bi, bj;
-        split_decode_tile(item % prm.ntile, &bi, &bj);
+        split_decode_tile(split_item_tile(item, prm.ntile, gridDim.x), &bi, &bj);
         const int sg = prm.wsgn[f];
         // a diagonal tile of a one-signed frequency multiplies A by itself
         const bool same = sg != 0 && bi == bj;
@@ -175,9 +185,10 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
             ok = false;
             break;
           }
+          const int kc = split_k_order(j, ks, prm.nk);
           mbar_arrive_expect_tx(&sm.full[st], (uint32_t)((same ? 1 : 2) * SP_SF * SP_PLANE));
-          tma_load_4d(&sm.a[st][0][0], &mapF, 0, bi * SP_ROWS, ks, za, &sm.full[st]);
-          if (!same) tma_load_4d(&sm.b[st][0][0], &mapF, 0, bj * SP_ROWS, ks, zb, &sm.full[st]);
+          tma_load_4d(&sm.a[st][0][0], &mapF, 0, bi * SP_ROWS, kc, za, &sm.full[st]);
+          if (!same) tma_load_4d(&sm.b[st][0][0], &mapF, 0, bj * SP_ROWS, kc, zb, &sm.full[st]);
           issued[st] = true;
           last_ph[st] = ph;
           if (++st == SP_ST) st = 0, ph ^= 1u;
@@ -197,7 +208,7 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j) {
         const int f = item / prm.ntile;
         int bi, bj;
-        split_decode_tile(item % prm.ntile, &bi, &bj);
+        split_decode_tile(split_item_tile(item, prm.ntile, gridDim.x), &bi, &bj);
         const bool same = prm.wsgn[f] != 0 && bi == bj;
         // accumulators free (first item: immediately)
         if (!mbar_wait(&sm.tempty, (uint32_t)(j & 1) ^ 1u, prm.timeout_ns, prm.status)) break;
@@ -242,8 +253,8 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       }
     }
   } else {
-    // ---------------- epilogue: 4 warps, one TMEM lane quarter each ----------------
-    const int q = warp & 3;
+    // ---- epilogue: SP1_EPI warps, SP1_EPI / 4 per TMEM lane quarter (column ranges) ----
+    const int q = warp & 3, h = (warp - 2) >> 2;
     const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16);
     int j = 0;
     for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j) {
@@ -251,14 +262,14 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       tc_fence_after();
       const int f = item / prm.ntile;
       int bi, bj;
-      split_decode_tile(item % prm.ntile, &bi, &bj);
+      split_decode_tile(split_item_tile(item, prm.ntile, gridDim.x), &bi, &bj);
       auto release = [&] {
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.tempty);
       };
-      if constexpr (REAL) real_epilogue(tl, q, lane, bi, bj, f, prm, release);
-      else fold_epilogue(tl, q, lane, bi, bj, f, prm, release);
+      if constexpr (REAL) real_epilogue(tl, q, lane, bi, bj, f, prm, release, 2 * SP1_NC * h, 2 * SP1_NC);
+      else fold_epilogue<SP1_NC>(tl, q, lane, bi, bj, f, prm, release, SP1_NC * h);
     }
   }
 
@@ -339,11 +350,10 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       bool issued[SP2_ST];
       uint32_t last_ph[SP2_ST];
       for (int q = 0; q < SP2_ST; ++q) issued[q] = false, last_ph[q] = 0;
-      bool ok = true;
       // Cursor over this cluster's (item, stage) sequence; it advances by increments
       // and decodes a tile only when it enters a new item.
       struct Cursor {
-        int item, ks, ya, yb, za, zb;
+        int item, ks, ya, yb, za, zb, j;
       };
       auto enter = [&](Cursor& u) {
         int bI, bJ;
@@ -358,27 +368,25 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
         if (++u.ks == prm.nk) {
           u.ks = 0;
           u.item += ncl;
+          ++u.j;
           if (u.item < prm.nitems) enter(u);
         }
       };
-      Cursor ld{cid, 0, 0, 0, 0, 0};
+      Cursor ld{cid, 0, 0, 0, 0, 0, 0};
       if (cid < prm.nitems) enter(ld);
       while (ld.item < prm.nitems) {
-        if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) {
-          ok = false;
-          break;
-        }
+        if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) break;
         const uint32_t lead_full = mapa_shared(smem_u32(&sm.full[st]), 0);
         if (rank == 0)
           mbar_arrive_expect_tx(&sm.full[st], (uint32_t)(2 * SP_SF * (SP_PLANE + SP2_BPLANE)));
-        tma_load_4d_pair(&sm.a[st][0][0], &mapF, 0, ld.ya, ld.ks, ld.za, lead_full);
-        tma_load_4d_pair(&sm.b[st][0][0], &mapFh, 0, ld.yb, ld.ks, ld.zb, lead_full);
+        const int kc = split_k_order(ld.j, ld.ks, prm.nk);
+        tma_load_4d_pair(&sm.a[st][0][0], &mapF, 0, ld.ya, kc, ld.za, lead_full);
+        tma_load_4d_pair(&sm.b[st][0][0], &mapFh, 0, ld.yb, kc, ld.zb, lead_full);
         advance(ld);
         issued[st] = true;
         last_ph[st] = ph;
         if (++st == SP2_ST) st = 0, ph ^= 1u;
       }
-      (void)ok;
       if (rank == 0) {
         // the leader's stage barriers count both CTAs' bytes
         for (int q = 0; q < SP2_ST; ++q)
@@ -560,10 +568,10 @@ __global__ void split_wstat_kernel(const double* __restrict__ W, int64_t ldw, in
 // rows 128 (i / 64) + 2 (i % 64) (Re) and the next one (Im). For frequency f the
 // planes f*6 + t hold the digits t of round(x |G| / s) (the folded operand), and,
 // when the frequency's weights have both signs, planes f*6 + 3 + t those of
-// round(x G / s). At most 96 registers a thread: a block fits on an SM beside the
-// accumulation kernel's CTA (192 threads x 256 registers), so slab s+1 is prepared
+// round(x G / s). At most 96 registers a thread: two blocks fit on an SM beside the
+// accumulation kernel's CTA (320 threads x 128 registers), so slab s+1 is prepared
 // while slab s accumulates.
-__global__ void __launch_bounds__(128, 5)
+__global__ void __maxnreg__(96)
     split_quantize_kernel(const double2* __restrict__ M, int64_t ldc, int64_t p0, int len,
                           int nchunk, int N, int npad, int64_t R, int64_t Ps, int nw,
                           const double* __restrict__ sA, const int* __restrict__ wsgn,
@@ -882,11 +890,12 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
       rc = check_cuda(ctx, cudaLaunchKernelEx(&cfg, split_gram2_kernel, mapF[b], mapFh[b], prm),
                       "split_gram2_kernel launch");
     } else {
-      split_gram_kernel<false><<<grid, SP_THREADS, smem, stream>>>(mapF[b], prm);
+      split_gram_kernel<false><<<grid, SP1_THREADS, smem, stream>>>(mapF[b], prm);
       rc = check_cuda(ctx, cudaGetLastError(), "split_gram_kernel launch");
     }
     if (rc) return rc;
     *launches += 1;
+    timing_mark(ctx, stream, 2);  // the accumulation interval ends with the kernel
     if ((rc = check_cuda(ctx, cudaEventRecord(gram_done[b], stream), "event"))) return rc;
     if (s + 1 < nslab) {
       // with one buffer, the next preparation waits for this accumulation
@@ -1002,9 +1011,10 @@ int split_chi0_real_slab(spx_ctx* ctx, const double* M, int64_t ldc, int64_t P, 
     prm.npack = (int64_t)N * (N + 1) / 2;
     prm.status = ctx->d_status;
     prm.timeout_ns = (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
-    split_gram_kernel<true><<<grid, SP_THREADS, smem, stream>>>(mapF[b], prm);
+    split_gram_kernel<true><<<grid, SP1_THREADS, smem, stream>>>(mapF[b], prm);
     if ((rc = check_cuda(ctx, cudaGetLastError(), "split_gram_kernel (real) launch"))) return rc;
     *launches += 1;
+    timing_mark(ctx, stream, 2);
     if ((rc = check_cuda(ctx, cudaEventRecord(gram_done[b], stream), "event"))) return rc;
     if (s + 1 < nslab) {
       if (nbuf == 1 && (rc = check_cuda(ctx, cudaStreamWaitEvent(ps, gram_done[0], 0), "event")))
@@ -1028,8 +1038,9 @@ int split_chi0_real_slab(spx_ctx* ctx, const double* M, int64_t ldc, int64_t P, 
 // so the only rounding is the slicing: 2^-17/127 of A's row scale per value, so
 // |error of C(m, col)| <= 2^-17/127 * crest(A_m) * ||A_m|| ||B_col||.
 // Items are rectangular (batch, column tile, row tile), row tiles fastest so that
-// concurrent CTAs share the large B tile through L2. The epilogue adds alpha
-// times the tile into cprod's columns: each double is written by one thread.
+// concurrent CTAs share the large B tile through L2. The epilogue stages alpha times
+// the tile in shared memory and writes (or adds) it into cprod's columns as runs of
+// 32 consecutive complex values.
 
 namespace spx {
 
@@ -1042,6 +1053,7 @@ struct SgParams {
   double* out;             // cprod as doubles, at (row 0, column 0) of batch 0
   int64_t sO2, sOn, sOc;   // complex strides: batch, n, c
   double alpha;
+  int overwrite;           // 1: store (the output range holds nothing yet), 0: add
   int* status;
   uint64_t timeout_ns;
 };
@@ -1059,11 +1071,12 @@ constexpr uint32_t SG_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(2
 struct __align__(1024) SgSmem {
   uint8_t a[SG_ST][SP_SA][SP_PLANE];
   uint8_t b[SG_ST][SP_SB][SG_BPLANE];
-  long long xchg[2][SP_TILE][33];
+  long long xchg[2][SP_TILE][SG_TB];   // the Re-row and Im-row products, column k ^ (row & 15)
+  double2 stage[SP_TILE][SG_TB];       // the output tile, column k ^ (row & 31)
   uint64_t full[SG_ST];
   uint64_t empty[SG_ST];
   uint64_t tfull[2], tempty[2];
-  uint64_t xfull, xfree, mdone;
+  uint64_t xfull, xstage, xfree, mdone;
   uint32_t tmem_base;
 };
 
@@ -1100,6 +1113,7 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       mbar_init(&sm.tempty[b], 4);
     }
     mbar_init(&sm.xfull, 4);
+    mbar_init(&sm.xstage, 4);
     mbar_init(&sm.xfree, 4);
     mbar_init(&sm.mdone, 1);
     fence_barrier_init();
@@ -1210,22 +1224,47 @@ __global__ void __launch_bounds__(SP_THREADS, 1)
       const double fac = prm.alpha * prm.sA[(int64_t)b * mtiles * SP_TILE + gm] *
                          (1.0 / (127.0 * 127.0 * 16777216.0));
       const double* sbb = prm.sB + (int64_t)b * ntiles * SG_TB;
-      double* ob = prm.out + 2 * (b * prm.sO2 + gm) + (is_re ? 0 : 1);
+      // the previous tile's staged values have been written out
       if (!mbar_wait(&sm.xfree, (xseq & 1u) ^ 1u, prm.timeout_ns, prm.status)) break;
 #pragma unroll
-      for (int k = 0; k < 32; ++k) sm.xchg[is_re ? 0 : 1][ii][k] = tim[k];
+      for (int k = 0; k < 32; ++k) sm.xchg[is_re ? 0 : 1][ii][k ^ (ii & 15)] = tim[k];
       __syncwarp();
       if (lane == 0) mbar_arrive(&sm.xfull);
       if (!mbar_wait(&sm.xfull, xseq & 1u, prm.timeout_ns, prm.status)) break;
+      // this thread's part (Re or Im) of row ii, 32 columns, into the staged tile
+      double* st = reinterpret_cast<double*>(&sm.stage[ii][0]) + (is_re ? 0 : 1);
 #pragma unroll
       for (int k = 0; k < 32; ++k) {
-        const int gc = ct * SG_TB + k;
-        const long long partner = sm.xchg[is_re ? 1 : 0][ii][k];
+        const long long partner = sm.xchg[is_re ? 1 : 0][ii][k ^ (ii & 15)];
         const long long v = is_re ? tre[k] + partner : tre[k] - partner;
-        if (gm < prm.M && gc < prm.ncol) {
-          const int n = gc / prm.ncin, c = gc - n * prm.ncin;
-          // one add per element per launch: a reduction that nothing waits on
-          atomicAdd(ob + 2 * (n * prm.sOn + c * prm.sOc), fac * sbb[gc] * (double)v);
+        st[2 * (k ^ lane)] = fac * sbb[ct * SG_TB + k] * (double)v;
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.xstage);
+      if (!mbar_wait(&sm.xstage, xseq & 1u, prm.timeout_ns, prm.status)) break;
+      // write out: warp q takes columns q, q + 4, ...; a lane one row of the two 32-row
+      // halves, so each store is 32 consecutive complex values of one cprod column
+      // (whole 32-byte sectors). Each element belongs to one thread of one launch.
+      double2* ob = reinterpret_cast<double2*>(prm.out) + b * prm.sO2 + mt * SP_TILE;
+#pragma unroll 2
+      for (int k = q; k < SG_TB; k += 4) {
+        const int gc = ct * SG_TB + k;
+        if (gc >= prm.ncol) break;
+        const int n = gc / prm.ncin, c = gc - n * prm.ncin;
+        double2* oc = ob + n * prm.sOn + c * prm.sOc;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int row = 32 * h + lane;
+          if (mt * SP_TILE + row >= prm.M) continue;
+          const double2 v = sm.stage[row][k ^ lane];
+          if (prm.overwrite) {
+            oc[row] = v;
+          } else {
+            double2 o = oc[row];
+            o.x += v.x;
+            o.y += v.y;
+            oc[row] = o;
+          }
         }
       }
       __syncwarp();
@@ -1343,7 +1382,7 @@ int sgemm_products(spx_ctx* ctx, int nbatch, int M, int ncol, int K, const doubl
                    int64_t lda, int64_t a_bstride, const double2* grid, int64_t g_bstride,
                    int64_t g_nstride, const int64_t* coff, const int* koff, int ncin,
                    double2* out, int64_t sO2, int64_t sOn, int64_t sOc, double alpha, void* ws,
-                   size_t ws_bytes, cudaStream_t s, int* launches) {
+                   size_t ws_bytes, cudaStream_t s, int* launches, bool overwrite) {
   if (nbatch <= 0 || M <= 0 || ncol <= 0 || K <= 0) return SPX_OK;
   const int mt = (M + SP_TILE - 1) / SP_TILE, nt = (ncol + SG_TB - 1) / SG_TB;
   const int64_t RA = (int64_t)mt * SP_ROWS, RB = (int64_t)nt * 2 * SG_TB;
@@ -1407,6 +1446,7 @@ int sgemm_products(spx_ctx* ctx, int nbatch, int M, int ncol, int K, const doubl
     prm.sOn = sOn;
     prm.sOc = sOc;
     prm.alpha = alpha;
+    prm.overwrite = overwrite && kbeg == 0;  // later K slabs add to the first
     prm.status = ctx->d_status;
     prm.timeout_ns = (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
     const int grid_n = std::min(prm.nitems, ctx->num_sms);

@@ -85,6 +85,11 @@ __device__ __forceinline__ int64_t split_row_re(int i) {
   return (int64_t)(i / SP_TILE) * SP_ROWS + 2 * (i % SP_TILE);
 }
 
+// The quantizers read M and write the planes with streaming (evict-first) accesses:
+// the planes of a slab are read again only after the accumulation of the slab before
+// it, so keeping them in L2 would only push out the row blocks that accumulation
+// reuses.
+//
 // One quantizer task: column i and the 16 pairs [p, p+16) of a slab of `len` pairs
 // (`lenp` padded to 64). `col` points at M(p0 .. , i) (pairs contiguous). Planes are
 // [plane][k-block of 64 pairs][row][64 bytes], `pstride` bytes apart; for frequency
@@ -101,7 +106,7 @@ __device__ __forceinline__ void quantize_task(const double2* __restrict__ col, b
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
     double2 v = make_double2(0.0, 0.0);
-    if (col_ok && p + k < len) v = col[p + k];
+    if (col_ok && p + k < len) v = __ldcs(col + p + k);
     xr[k] = v.x;
     xi[k] = v.y;
   }
@@ -146,19 +151,15 @@ __device__ __forceinline__ void quantize_task(const double2* __restrict__ col, b
 #pragma unroll
     for (int t = 0; t < SP_SF; ++t) {
       const int64_t plane = (int64_t)f * SP_SLOT + t;
-      *reinterpret_cast<uint4*>(F + o_re + plane * pstride) =
-          make_uint4(ar[t][0], ar[t][1], ar[t][2], ar[t][3]);
-      *reinterpret_cast<uint4*>(F + o_im + plane * pstride) =
-          make_uint4(ai[t][0], ai[t][1], ai[t][2], ai[t][3]);
+      __stcs(reinterpret_cast<uint4*>(F + o_re + plane * pstride), make_uint4(ar[t][0], ar[t][1], ar[t][2], ar[t][3]));
+      __stcs(reinterpret_cast<uint4*>(F + o_im + plane * pstride), make_uint4(ai[t][0], ai[t][1], ai[t][2], ai[t][3]));
     }
     if (mixed) {
 #pragma unroll
       for (int t = 0; t < SP_SF; ++t) {
         const int64_t plane = (int64_t)f * SP_SLOT + SP_SF + t;
-        *reinterpret_cast<uint4*>(F + o_re + plane * pstride) =
-            make_uint4(br[t][0], br[t][1], br[t][2], br[t][3]);
-        *reinterpret_cast<uint4*>(F + o_im + plane * pstride) =
-            make_uint4(bim[t][0], bim[t][1], bim[t][2], bim[t][3]);
+        __stcs(reinterpret_cast<uint4*>(F + o_re + plane * pstride), make_uint4(br[t][0], br[t][1], br[t][2], br[t][3]));
+        __stcs(reinterpret_cast<uint4*>(F + o_im + plane * pstride), make_uint4(bim[t][0], bim[t][1], bim[t][2], bim[t][3]));
       }
     }
   }
@@ -177,15 +178,29 @@ __device__ __forceinline__ void quantize_task8(const double2* __restrict__ col, 
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     double2 v = make_double2(0.0, 0.0);
-    if (col_ok && p + k < len) v = col[p + k];
+    if (col_ok && p + k < len) v = __ldcs(col + p + k);
     xr[k] = v.x;
     xi[k] = v.y;
   }
   const double inv = s > 0.0 ? 1.0 / s : 0.0;
+  // the factors of frequency f + 1 are loaded while frequency f is quantized, so the
+  // loop does not wait on one L2 round trip per frequency
+  double2 gn[4];
+  int sn = 0;
+  auto fetch = [&](int f) {
+    const double2* gf = reinterpret_cast<const double2*>(G + (int64_t)f * lenp + p);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) gn[e] = __ldg(gf + e);
+    sn = __ldg(wsgn + f);
+  };
+  fetch(0);
 #pragma unroll 1
   for (int f = 0; f < nw; ++f) {
-    const double* gf = G + (int64_t)f * lenp + p;
-    const bool mixed = wsgn[f] == 0;
+    double gv[8];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) gv[2 * e] = gn[e].x, gv[2 * e + 1] = gn[e].y;
+    const bool mixed = sn == 0;
+    if (f + 1 < nw) fetch(f + 1);
     uint32_t ar[SP_SF][2], ai[SP_SF][2], br[SP_SF][2], bim[SP_SF][2];
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
@@ -193,7 +208,7 @@ __device__ __forceinline__ void quantize_task8(const double2* __restrict__ col, 
       double gq[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        gq[e] = gf[4 * q + e] * inv;
+        gq[e] = gv[4 * q + e] * inv;
         const double ga = fabs(gq[e]);
         yr[e] = round_mul(xr[4 * q + e], ga);
         yi[e] = round_mul(xi[4 * q + e], ga);
@@ -215,15 +230,15 @@ __device__ __forceinline__ void quantize_task8(const double2* __restrict__ col, 
 #pragma unroll
     for (int t = 0; t < SP_SF; ++t) {
       const int64_t plane = (int64_t)f * SP_SLOT + t;
-      *reinterpret_cast<uint2*>(F + o_re + plane * pstride) = make_uint2(ar[t][0], ar[t][1]);
-      *reinterpret_cast<uint2*>(F + o_im + plane * pstride) = make_uint2(ai[t][0], ai[t][1]);
+      __stcs(reinterpret_cast<uint2*>(F + o_re + plane * pstride), make_uint2(ar[t][0], ar[t][1]));
+      __stcs(reinterpret_cast<uint2*>(F + o_im + plane * pstride), make_uint2(ai[t][0], ai[t][1]));
     }
     if (mixed) {
 #pragma unroll
       for (int t = 0; t < SP_SF; ++t) {
         const int64_t plane = (int64_t)f * SP_SLOT + SP_SF + t;
-        *reinterpret_cast<uint2*>(F + o_re + plane * pstride) = make_uint2(br[t][0], br[t][1]);
-        *reinterpret_cast<uint2*>(F + o_im + plane * pstride) = make_uint2(bim[t][0], bim[t][1]);
+        __stcs(reinterpret_cast<uint2*>(F + o_re + plane * pstride), make_uint2(br[t][0], br[t][1]));
+        __stcs(reinterpret_cast<uint2*>(F + o_im + plane * pstride), make_uint2(bim[t][0], bim[t][1]));
       }
     }
   }
@@ -239,7 +254,7 @@ __device__ __forceinline__ void quantize_task_real(const double* __restrict__ co
                                                    int8_t* __restrict__ F) {
   double x[16];
 #pragma unroll
-  for (int k = 0; k < 16; ++k) x[k] = (col_ok && p + k < len) ? col[p + k] : 0.0;
+  for (int k = 0; k < 16; ++k) x[k] = (col_ok && p + k < len) ? __ldcs(col + p + k) : 0.0;
   const double inv = s > 0.0 ? 1.0 / s : 0.0;
   for (int f = 0; f < nw; ++f) {
     const double* gf = G + (int64_t)f * lenp + p;
@@ -269,13 +284,11 @@ __device__ __forceinline__ void quantize_task_real(const double* __restrict__ co
     }
 #pragma unroll
     for (int t = 0; t < SP_SF; ++t)
-      *reinterpret_cast<uint4*>(F + o + ((int64_t)f * SP_SLOT + t) * pstride) =
-          make_uint4(a[t][0], a[t][1], a[t][2], a[t][3]);
+      __stcs(reinterpret_cast<uint4*>(F + o + ((int64_t)f * SP_SLOT + t) * pstride), make_uint4(a[t][0], a[t][1], a[t][2], a[t][3]));
     if (mixed) {
 #pragma unroll
       for (int t = 0; t < SP_SF; ++t)
-        *reinterpret_cast<uint4*>(F + o + ((int64_t)f * SP_SLOT + SP_SF + t) * pstride) =
-            make_uint4(b[t][0], b[t][1], b[t][2], b[t][3]);
+        __stcs(reinterpret_cast<uint4*>(F + o + ((int64_t)f * SP_SLOT + SP_SF + t) * pstride), make_uint4(b[t][0], b[t][1], b[t][2], b[t][3]));
     }
   }
 }
@@ -287,6 +300,29 @@ __device__ __forceinline__ void split_decode_tile(int t, int* bi, int* bj) {
   while ((j + 1) * (j + 2) / 2 <= t) ++j;
   *bj = j;
   *bi = t - j * (j + 1) / 2;
+}
+
+// Tile of a frequency-major item when `grid` CTAs take items round-robin. A frequency's
+// ntile tiles fall into two rounds of the grid: the first `a` of them beside the
+// previous frequency's last tiles, the rest in the next round. The smaller part is made
+// the one whose tiles cover the fewest panels (a prefix of the column-major order is
+// the upper triangle of panels 0..p), so fewer panels are read again, from DRAM, in the
+// round after. Every role of a CTA decodes an item the same way.
+// `first` is the item number of the frequency's first tile.
+__device__ __forceinline__ int split_round_tile(int t, int ntile, int64_t first, int grid) {
+  const int a = grid - (int)(first % grid);
+  return (a < ntile && a > ntile - a) ? ntile - 1 - t : t;
+}
+__device__ __forceinline__ int split_item_tile(int item, int ntile, int grid) {
+  const int t = item % ntile;
+  return split_round_tile(t, ntile, item - t, grid);
+}
+
+// K step `ks` of a CTA's j-th item: every second item runs the slab backwards, so it
+// starts on the K blocks that the CTAs' previous items read last, which are the ones
+// still in L2. The integer sums are exact, so the order does not change any bit.
+__device__ __forceinline__ int split_k_order(int j, int ks, int nk) {
+  return (j & 1) ? nk - 1 - ks : ks;
 }
 
 // 16 consecutive columns of this lane's row: the slab's exact integer sum

@@ -541,7 +541,7 @@ int sgemm_products(spx_ctx* ctx, int nbatch, int M, int ncol, int K, const doubl
                    int64_t lda, int64_t a_bstride, const double2* grid, int64_t g_bstride,
                    int64_t g_nstride, const int64_t* coff, const int* koff, int ncin,
                    double2* out, int64_t sO2, int64_t sOn, int64_t sOc, double alpha, void* ws,
-                   size_t ws_bytes, cudaStream_t s, int* launches);
+                   size_t ws_bytes, cudaStream_t s, int* launches, bool overwrite);
 int wfprod_pw_fft_run(spx_ctx* ctx, const spx_pw_desc* d, int nk, int nocc, int nunocc,
                       const double2* c1, const double2* c2, double2* cprod, int64_t ldc, int col0,
                       void* ws, size_t ws_bytes, cudaStream_t s, int* launches);
@@ -562,10 +562,12 @@ size_t wfprod_pw_workspace(const spx_pw_desc* d, int nk, int nocc, int nunocc, b
 }
 
 // Runs the explicit-convolution PW products into cprod columns [col0, col0+ngptm).
-// split: the product GEMM on int8 digit slices (K4s) instead of FP64 (K4c).
+// split: the product GEMM on int8 digit slices (K4s) instead of FP64 (K4c);
+// overwrite: those columns hold nothing yet, so K4s stores instead of adding.
 int wfprod_pw_run(spx_ctx* ctx, const spx_pw_desc* d, int nk, int nocc, int nunocc,
                   const double2* c1, const double2* c2, double2* cprod, int64_t ldc, int col0,
-                  void* ws, size_t ws_bytes, cudaStream_t s, int* launches, bool split) {
+                  void* ws, size_t ws_bytes, cudaStream_t s, int* launches, bool split,
+                  bool overwrite) {
   if (d->nfft > 0)
     return wfprod_pw_fft_run(ctx, d, nk, nocc, nunocc, c1, c2, cprod, ldc, col0, ws, ws_bytes, s,
                              launches);
@@ -626,7 +628,7 @@ int wfprod_pw_run(spx_ctx* ctx, const spx_pw_desc* d, int nk, int nocc, int nuno
                           pl.b0.size(), d_coff, d_koff, d->ngptm,
                           cprod + (int64_t)k0 * nocc * nunocc + ldc * col0,
                           (int64_t)nocc * nunocc, nunocc, ldc, 1.0 / std::sqrt(d->vol), sg_ws,
-                          sg_bytes, s, launches);
+                          sg_bytes, s, launches, overwrite);
       if (rc) return rc;
       continue;
     }
@@ -717,7 +719,7 @@ extern "C" int spx_wfprod_pw_dev(spx_ctx* ctx, const spx_pw_desc* pw, int32_t nk
   cudaStream_t s = pick_stream(ctx, stream);
   return wfprod_pw_run(ctx, pw, nk, nocc, nunocc, reinterpret_cast<const double2*>(cpw_occ),
                        reinterpret_cast<const double2*>(cpw_unocc), reinterpret_cast<double2*>(cprod),
-                       ldc, col0, ctx->ws, ctx->ws_bytes, s, &launches, split);
+                       ldc, col0, ctx->ws, ctx->ws_bytes, s, &launches, split, false);
 }
 
 // ---------------------------------------------------------------------------

@@ -11,10 +11,14 @@
 //     G box, so each of the three separable passes sums only over the box
 //     extent of its axis (19 of 48 for a 3000-wave sphere on a 48^3 grid); the last pass applies
 //     conj, 1/sqrt(vol), theta or 1/nnfft;
-//   * pair z and y passes (K5b, `fft_pair_zy_kernel`): one CTA per (occupied
-//     band, x plane, group of unoccupied bands) forms the product line by line
-//     and transforms it along z to the kz values that occur in G_M - g only
-//     (13 of 48), then along y to the needed ky values, in shared memory;
+//   * pair z and y passes (K5b): one CTA per (occupied band, x plane, group of
+//     unoccupied bands) forms the product line by line and transforms it along z,
+//     keeping the kz values that occur in G_M - g only (13 of 48), then along y to
+//     the needed ky values, in shared memory. Grid edges n = 16 r (r <= 4, the
+//     48^3 grid among them) use a radix-16 x r line FFT
+//     (`fft_pair_zy_radix_kernel`, the transform the reference gets from FFTW,
+//     src/fft.f:69-93); other edges sum the pruned DFT directly
+//     (`fft_pair_zy_kernel`);
 //   * pair x pass and gather (K5c, `fft_pair_x_kernel`): one CTA per pair sums
 //     over x for exactly the (kx, ky, kz) of each G_M and adds the result into
 //     cprod's column.
@@ -158,6 +162,124 @@ __global__ void __launch_bounds__(FFT_NMAX * FFT_NP) fft_pair_zy_kernel(PairPara
     for (int yy = 0; yy < n; ++yy) cfma(s, ey[yy], t1[yy]);
     const int64_t pairc = (int64_t)kn * p.nunocc + npp;
     p.T2[((pairc * n + x) * p.nkz + kz) * p.nky + ky] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K5b as a line FFT, for grid edges n = 16 r (r = 1..4): the 48-point transform of
+// the 48^3 grid is radix 16 x 3. With z = r n1 + n2 and k = k1 + 16 k2,
+//   X[k] = sum_{n2<r} W_n^{n2 k1} W_r^{n2 k2} F_{n2}[k1],
+//   F_{n2}[k1] = sum_{n1<16} x[r n1 + n2] W_16^{n1 k1},
+// so thread (line, n2) transforms its 16 decimated points in registers (radix 4 x 4),
+// applies W_n^{n2 k1}, and the r partial spectra of a line are combined, through
+// shared memory, only at the k the gather needs. W = exp(-2 pi i / n) (forward).
+
+// 4-point forward DFT in place: (x0, x1, x2, x3) -> (X0, X1, X2, X3), W_4 = -i.
+__device__ __forceinline__ void dft4_fwd(double2& x0, double2& x1, double2& x2, double2& x3) {
+  const double2 t0 = make_double2(x0.x + x2.x, x0.y + x2.y), t1 = make_double2(x0.x - x2.x, x0.y - x2.y);
+  const double2 t2 = make_double2(x1.x + x3.x, x1.y + x3.y), t3 = make_double2(x1.x - x3.x, x1.y - x3.y);
+  x0 = make_double2(t0.x + t2.x, t0.y + t2.y);
+  x2 = make_double2(t0.x - t2.x, t0.y - t2.y);
+  x1 = make_double2(t1.x + t3.y, t1.y - t3.x);  // t1 - i t3
+  x3 = make_double2(t1.x - t3.y, t1.y + t3.x);  // t1 + i t3
+}
+
+// 16-point forward DFT of v (natural order in): n1 = 4a + b, k1 = c + 4d; 4-point
+// transforms over a, twiddles W_16^{bc} (w16[m] = W_16^m), 4-point transforms over b.
+// The output is left digit-reversed: X[k1] is v[fft16_pos(k1)].
+__host__ __device__ constexpr int fft16_pos(int k1) { return 4 * (k1 & 3) + (k1 >> 2); }
+__device__ __forceinline__ void fft16_fwd(double2 (&v)[16], const double2* __restrict__ w16) {
+#pragma unroll
+  for (int b = 0; b < 4; ++b) dft4_fwd(v[b], v[4 + b], v[8 + b], v[12 + b]);  // v[4c + b] = Y_b[c]
+#pragma unroll
+  for (int b = 1; b < 4; ++b)
+#pragma unroll
+    for (int c = 1; c < 4; ++c) v[4 * c + b] = cmul(v[4 * c + b], w16[b * c]);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) dft4_fwd(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);  // v[4c + d] = X[c + 4d]
+}
+
+struct PairFftParams {
+  const double2* A;    // [kl*nocc + n][x][y][z]
+  const double2* B;    // [kl*nunocc + n'][x][y][z]
+  double2* T2;         // [pairc][x][kz][ky]
+  const double2* twf;  // W_n^m = exp(-2 pi i m / n), m < n
+  const int* kz;       // distinct kz values (nkz)
+  const int* ky;
+  int n, r, bpc, nocc, nunocc, nkz, nky;
+};
+
+// grid (kl*nocc + n, group of bpc unoccupied bands, x); block bpc * n * r threads:
+// thread t of band j is line t / r, decimation phase t % r.
+__global__ void __launch_bounds__(512) fft_pair_zy_radix_kernel(PairFftParams p) {
+  extern __shared__ double2 smr[];
+  const int n = p.n, r = p.r, per = n * r;
+  double2* tw = smr;                                 // [n]
+  double2* w16 = tw + n;                             // [16]
+  double2* Fb = w16 + 16;                            // [bpc][n lines][r][16]
+  double2* T1 = Fb + (size_t)p.bpc * n * r * 16;     // [bpc][FFT_KMAX][n]
+  const int kn = blockIdx.x, grp = blockIdx.y, x = blockIdx.z;
+  const int kl = kn / p.nocc;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = p.twf[i];
+  for (int i = threadIdx.x; i < 16; i += blockDim.x) w16[i] = p.twf[i * r];
+  __syncthreads();
+  const int j = threadIdx.x / per, t = threadIdx.x - j * per;
+  const int np = grp * p.bpc + j;
+  const bool live = j < p.bpc && np < p.nunocc;
+  double2* F = Fb + (size_t)j * n * r * 16;
+  double2* T = T1 + (size_t)j * FFT_KMAX * n;
+  // z pass: line y = t / r of the product plane A(x, y, .) B(x, y, .)
+  if (live) {
+    const int y = t / r, n2 = t - (t / r) * r;
+    const double2* a = p.A + (((int64_t)kn * n + x) * n + y) * n;
+    const double2* bl = p.B + ((((int64_t)kl * p.nunocc + np) * n + x) * n + y) * n;
+    double2 v[16];
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) {
+      const int z = r * n1 + n2;
+      v[n1] = cmul(__ldg(a + z), __ldg(bl + z));
+    }
+    fft16_fwd(v, w16);
+    double2* f = F + ((size_t)y * r + n2) * 16;
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) f[k1] = n2 ? cmul(v[fft16_pos(k1)], tw[n2 * k1]) : v[fft16_pos(k1)];
+  }
+  __syncthreads();
+  // combine at the needed kz: T[kk][y]
+  if (live) {
+    for (int o = t; o < p.nkz * n; o += per) {
+      const int kk = o / n, y = o - kk * n;
+      const int k = p.kz[kk], k1 = k & 15, k2 = k >> 4;
+      const double2* f = F + (size_t)y * r * 16 + k1;
+      double2 acc = f[0];
+      for (int n2 = 1; n2 < r; ++n2) cfma(acc, f[n2 * 16], tw[(16 * n2 * k2) % n]);
+      T[kk * n + y] = acc;
+    }
+  }
+  __syncthreads();
+  // y pass: line kk of T along y
+  if (live && t < p.nkz * r) {
+    const int kk = t / r, n2 = t - (t / r) * r;
+    double2 v[16];
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) v[n1] = T[kk * n + r * n1 + n2];
+    fft16_fwd(v, w16);
+    double2* f = F + ((size_t)kk * r + n2) * 16;
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) f[k1] = n2 ? cmul(v[fft16_pos(k1)], tw[n2 * k1]) : v[fft16_pos(k1)];
+  }
+  __syncthreads();
+  if (live) {
+    const int64_t pairc = (int64_t)kn * p.nunocc + np;
+    double2* out = p.T2 + (pairc * n + x) * p.nkz * p.nky;
+    for (int o = t; o < p.nkz * p.nky; o += per) {
+      const int kk = o / p.nky, kyi = o - kk * p.nky;
+      const int k = p.ky[kyi], k1 = k & 15, k2 = k >> 4;
+      const double2* f = F + (size_t)kk * r * 16 + k1;
+      double2 acc = f[0];
+      for (int n2 = 1; n2 < r; ++n2) cfma(acc, f[n2 * 16], tw[(16 * n2 * k2) % n]);
+      out[o] = acc;
+    }
   }
 }
 
@@ -411,6 +533,14 @@ int wfprod_pw_fft_run(spx_ctx* ctx, const spx_pw_desc* d, int nk, int nocc, int 
   const size_t zy_smem = sizeof(double2) * ((size_t)n * n + 2 * FFT_KMAX * n + (size_t)FFT_NP * FFT_KMAX * n);
   const size_t x_smem = sizeof(double2) * ((size_t)FFT_KMAX * n + d->ngptm + (size_t)FFT_XC * nky * nkz);
   cudaFuncSetAttribute(fft_pair_zy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zy_smem);
+  // grid edges 16 r (r <= 4) take the line FFT; bpc bands per CTA within 100 KB of
+  // shared memory and 512 threads
+  const bool radix = n % 16 == 0 && n / 16 >= 1 && n / 16 <= 4;
+  const size_t band_smem = sizeof(double2) * ((size_t)n * (n / 16) * 16 + (size_t)FFT_KMAX * n);
+  const int bpc = radix ? std::max(1, std::min({4, 512 / (n * (n / 16)), (int)((100 << 10) / band_smem)})) : 1;
+  const size_t radix_smem = sizeof(double2) * ((size_t)n + 16) + bpc * band_smem;
+  if (radix)
+    cudaFuncSetAttribute(fft_pair_zy_radix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)radix_smem);
   cudaFuncSetAttribute(fft_pair_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)x_smem);
   for (int k0 = 0; k0 < nk; k0 += kchunk) {
     const int kn = std::min(kchunk, nk - k0);
@@ -432,10 +562,17 @@ int wfprod_pw_fft_run(spx_ctx* ctx, const spx_pw_desc* d, int nk, int nocc, int 
     }
     if ((rc = band_grids(ctx, pl.b2, nb2, box, ta, tb, Bg, d_twb, n, 0, 1.0 / (double)n3, nullptr, s, launches)))
       return rc;
-    PairParams pp{A, Bg, T2, d_twf, d_ks[2], d_ks[1], n, nocc, nunocc, nkz, nky};
-    dim3 gz(nb1, (nunocc + FFT_NP - 1) / FFT_NP, n), bz(n, FFT_NP);
-    fft_pair_zy_kernel<<<gz, bz, zy_smem, s>>>(pp);
-    if ((rc = check_cuda(ctx, cudaGetLastError(), "fft_pair_zy_kernel launch"))) return rc;
+    if (radix) {
+      PairFftParams pr{A, Bg, T2, d_twf, d_ks[2], d_ks[1], n, n / 16, bpc, nocc, nunocc, nkz, nky};
+      dim3 gz(nb1, (nunocc + bpc - 1) / bpc, n);
+      fft_pair_zy_radix_kernel<<<gz, bpc * n * (n / 16), radix_smem, s>>>(pr);
+      if ((rc = check_cuda(ctx, cudaGetLastError(), "fft_pair_zy_radix_kernel launch"))) return rc;
+    } else {
+      PairParams pp{A, Bg, T2, d_twf, d_ks[2], d_ks[1], n, nocc, nunocc, nkz, nky};
+      dim3 gz(nb1, (nunocc + FFT_NP - 1) / FFT_NP, n), bz(n, FFT_NP);
+      fft_pair_zy_kernel<<<gz, bz, zy_smem, s>>>(pp);
+      if ((rc = check_cuda(ctx, cudaGetLastError(), "fft_pair_zy_kernel launch"))) return rc;
+    }
     ++*launches;
     GatherParams gp{T2, d_twf, d_ks[0], d_gmap, cprod + (int64_t)k0 * nocc * nunocc + ldc * col0, ldc,
                     n, nkx, nky, nkz, d->ngptm};

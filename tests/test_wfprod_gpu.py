@@ -184,7 +184,10 @@ def test_chi0_from_coeffs_equals_products_then_accumulate(products):
 @pytest.mark.parametrize("kw,shifted,nfft", [
     (dict(), False, 24), (dict(), True, 24), (dict(nk=1, nocc=1, nunocc=1, ngptm=1), True, 20),
     (dict(ngpt=150, ngptm=70, nunocc=9, step_radius=0), False, 27),
-    (dict(ngpt=120, ngptm=33, nunocc=5, step_radius=4), True, 30)])
+    (dict(ngpt=120, ngptm=33, nunocc=5, step_radius=4), True, 30),
+    # grid edges 16 r take the radix-16 x r line FFT
+    (dict(), True, 16), (dict(ngpt=150, ngptm=70, nunocc=9), False, 64),
+    (dict(nunocc=7), True, 48)])
 def test_pw_fft_branch_matches_oracle(ctx, kw, shifted, nfft):
     w = small_workload(**kw)
     pw = shifted_pw(w) if shifted else inputs.pw_basis(w)
