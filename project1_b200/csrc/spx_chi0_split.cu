@@ -568,30 +568,108 @@ __global__ void split_wstat_kernel(const double* __restrict__ W, int64_t ldw, in
 // rows 128 (i / 64) + 2 (i % 64) (Re) and the next one (Im). For frequency f the
 // planes f*6 + t hold the digits t of round(x |G| / s) (the folded operand), and,
 // when the frequency's weights have both signs, planes f*6 + 3 + t those of
-// round(x G / s). At most 96 registers a thread: two blocks fit on an SM beside the
-// accumulation kernel's CTA (320 threads x 128 registers), so slab s+1 is prepared
-// while slab s accumulates.
+// round(x G / s). A block is 16 columns x one 64-pair k-block; the block stages the
+// folded factors of its 64 pairs (SPQ_FCH frequencies at a time) in shared memory,
+// so the frequency loop waits on no L2 round trip. The kernel is bound by the HBM
+// writes of the planes; 96 registers keep five blocks per SM.
+constexpr int SPQ_FCH = 24;
 __global__ void __maxnreg__(96)
     split_quantize_kernel(const double2* __restrict__ M, int64_t ldc, int64_t p0, int len,
                           int nchunk, int N, int npad, int64_t R, int64_t Ps, int nw,
                           const double* __restrict__ sA, const int* __restrict__ wsgn,
                           const double* __restrict__ G, int8_t* __restrict__ F) {
+  __shared__ __align__(16) double gs[SPQ_FCH][SP_KB];
+  __shared__ int ss[SPQ_FCH];
+  // thread -> (k-block, column group of 4, eighth of the k-block, column in group); the
+  // 4 warps of a block share the k-block (npad / 4 is a multiple of 4)
   const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (tid >= (int64_t)npad * nchunk * 2) return;
-  // tid -> (k-block, column group of 4, eighth of the k-block, column in group)
+  const bool active = tid < (int64_t)npad * nchunk * 2;
   const int ngroup = npad / 4;
   const int lane4 = (int)(tid & 3), eighth = (int)((tid >> 2) & 7);
   const int64_t rest = tid >> 5;
   const int i = (int)(rest % ngroup) * 4 + lane4;
-  const int64_t kb = rest / ngroup;
+  const int64_t kb = ((blockIdx.x * (int64_t)blockDim.x) >> 5) / ngroup;  // the block's k-block
   const int p = (int)(kb * SP_KB) + eighth * 8;
+  const int lenp = nchunk * 16;
   const int64_t nkb = Ps / SP_KB;
   // planes are nkb * R * 64 bytes apart
   const int64_t pstride = nkb * R * SP_KB;
   const int64_t o_re = (kb * R + split_row_re(i)) * SP_KB + eighth * 8;
-  const bool col_ok = i < N;
-  quantize_task8(M + (int64_t)(col_ok ? i : 0) * ldc + p0, col_ok, len, p, col_ok ? sA[i] : 0.0,
-                 o_re, pstride, nw, wsgn, G, nchunk * 16, F);
+  const bool col_ok = active && i < N;
+  const double2* col = M + (int64_t)(col_ok ? i : 0) * ldc + p0;
+  double xr[8], xi[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    double2 v = make_double2(0.0, 0.0);
+    if (col_ok && p + k < len) v = __ldg(col + p + k);
+    xr[k] = v.x;
+    xi[k] = v.y;
+  }
+  const double s = col_ok ? sA[i] : 0.0;
+  const double inv = s > 0.0 ? 1.0 / s : 0.0;
+  for (int f0 = 0; f0 < nw; f0 += SPQ_FCH) {
+    const int nf = min(SPQ_FCH, nw - f0);
+    __syncthreads();  // the previous chunk's factors are consumed
+    // 16-byte chunk c = 4 e + j (eighth e, chunk j of its 8 pairs) is kept at
+    // 4 e + (j ^ ((e >> 1) & 3)): the eight eighths a warp reads at once fall in
+    // distinct banks
+    for (int e = threadIdx.x; e < nf * (SP_KB / 2); e += blockDim.x) {
+      const int f = e / (SP_KB / 2), c = e - f * (SP_KB / 2);
+      const int ce = c >> 2, cj = c & 3;
+      reinterpret_cast<double2*>(&gs[f][0])[4 * ce + (cj ^ ((ce >> 1) & 3))] =
+          __ldg(reinterpret_cast<const double2*>(G + (int64_t)(f0 + f) * lenp + kb * SP_KB) + c);
+    }
+    for (int f = threadIdx.x; f < nf; f += blockDim.x) ss[f] = wsgn[f0 + f];
+    __syncthreads();
+    if (!active) continue;
+#pragma unroll 1
+    for (int f = 0; f < nf; ++f) {
+      const bool mixed = ss[f] == 0;
+      const double2* gq2 = reinterpret_cast<const double2*>(&gs[f][eighth * 8]);
+      const int sw = (eighth >> 1) & 3;
+      uint32_t ar[SP_SF][2], ai[SP_SF][2], br[SP_SF][2], bim[SP_SF][2];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        uint32_t yr[4], yi[4], pr[SP_SF], pi[SP_SF];
+        double gq[4];
+        const double2 g01 = gq2[(2 * q) ^ sw], g23 = gq2[(2 * q + 1) ^ sw];
+        gq[0] = g01.x * inv, gq[1] = g01.y * inv, gq[2] = g23.x * inv, gq[3] = g23.y * inv;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const double ga = fabs(gq[e]);
+          yr[e] = round_mul(xr[4 * q + e], ga);
+          yi[e] = round_mul(xi[4 * q + e], ga);
+        }
+        digit_planes<SP_SF>(yr, pr);
+        digit_planes<SP_SF>(yi, pi);
+#pragma unroll
+        for (int t = 0; t < SP_SF; ++t) ar[t][q] = pr[t], ai[t][q] = pi[t];
+        if (mixed) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (gq[e] < 0.0) yr[e] = 0u - yr[e], yi[e] = 0u - yi[e];
+          digit_planes<SP_SF>(yr, pr);
+          digit_planes<SP_SF>(yi, pi);
+#pragma unroll
+          for (int t = 0; t < SP_SF; ++t) br[t][q] = pr[t], bim[t][q] = pi[t];
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < SP_SF; ++t) {
+        const int64_t plane = (int64_t)(f0 + f) * SP_SLOT + t;
+        *reinterpret_cast<uint2*>(F + o_re + plane * pstride) = make_uint2(ar[t][0], ar[t][1]);
+        *reinterpret_cast<uint2*>(F + o_re + SP_KB + plane * pstride) = make_uint2(ai[t][0], ai[t][1]);
+      }
+      if (mixed) {
+#pragma unroll
+        for (int t = 0; t < SP_SF; ++t) {
+          const int64_t plane = (int64_t)(f0 + f) * SP_SLOT + SP_SF + t;
+          *reinterpret_cast<uint2*>(F + o_re + plane * pstride) = make_uint2(br[t][0], br[t][1]);
+          *reinterpret_cast<uint2*>(F + o_re + SP_KB + plane * pstride) = make_uint2(bim[t][0], bim[t][1]);
+        }
+      }
+    }
+  }
 }
 
 // -DINV (real M): column scales and digit planes with one plane row per column

@@ -85,11 +85,6 @@ __device__ __forceinline__ int64_t split_row_re(int i) {
   return (int64_t)(i / SP_TILE) * SP_ROWS + 2 * (i % SP_TILE);
 }
 
-// The quantizers read M and write the planes with streaming (evict-first) accesses:
-// the planes of a slab are read again only after the accumulation of the slab before
-// it, so keeping them in L2 would only push out the row blocks that accumulation
-// reuses.
-//
 // One quantizer task: column i and the 16 pairs [p, p+16) of a slab of `len` pairs
 // (`lenp` padded to 64). `col` points at M(p0 .. , i) (pairs contiguous). Planes are
 // [plane][k-block of 64 pairs][row][64 bytes], `pstride` bytes apart; for frequency
@@ -106,7 +101,7 @@ __device__ __forceinline__ void quantize_task(const double2* __restrict__ col, b
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
     double2 v = make_double2(0.0, 0.0);
-    if (col_ok && p + k < len) v = __ldcs(col + p + k);
+    if (col_ok && p + k < len) v = __ldg(col + p + k);
     xr[k] = v.x;
     xi[k] = v.y;
   }
@@ -151,94 +146,15 @@ __device__ __forceinline__ void quantize_task(const double2* __restrict__ col, b
 #pragma unroll
     for (int t = 0; t < SP_SF; ++t) {
       const int64_t plane = (int64_t)f * SP_SLOT + t;
-      __stcs(reinterpret_cast<uint4*>(F + o_re + plane * pstride), make_uint4(ar[t][0], ar[t][1], ar[t][2], ar[t][3]));
-      __stcs(reinterpret_cast<uint4*>(F + o_im + plane * pstride), make_uint4(ai[t][0], ai[t][1], ai[t][2], ai[t][3]));
+      *reinterpret_cast<uint4*>(F + o_re + plane * pstride) = make_uint4(ar[t][0], ar[t][1], ar[t][2], ar[t][3]);
+      *reinterpret_cast<uint4*>(F + o_im + plane * pstride) = make_uint4(ai[t][0], ai[t][1], ai[t][2], ai[t][3]);
     }
     if (mixed) {
 #pragma unroll
       for (int t = 0; t < SP_SF; ++t) {
         const int64_t plane = (int64_t)f * SP_SLOT + SP_SF + t;
-        __stcs(reinterpret_cast<uint4*>(F + o_re + plane * pstride), make_uint4(br[t][0], br[t][1], br[t][2], br[t][3]));
-        __stcs(reinterpret_cast<uint4*>(F + o_im + plane * pstride), make_uint4(bim[t][0], bim[t][1], bim[t][2], bim[t][3]));
-      }
-    }
-  }
-}
-
-// quantize_task for 8 pairs [p, p+8): the same digits (the same arithmetic per
-// value), written as 8-byte pieces of the plane rows. Fewer live registers let the
-// preparation kernel run beside the accumulation kernel on every SM.
-__device__ __forceinline__ void quantize_task8(const double2* __restrict__ col, bool col_ok, int len,
-                                               int p, double s, int64_t o_re, int64_t pstride,
-                                               int nw, const int* __restrict__ wsgn,
-                                               const double* __restrict__ G, int lenp,
-                                               int8_t* __restrict__ F) {
-  const int64_t o_im = o_re + SP_KB;
-  double xr[8], xi[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    double2 v = make_double2(0.0, 0.0);
-    if (col_ok && p + k < len) v = __ldcs(col + p + k);
-    xr[k] = v.x;
-    xi[k] = v.y;
-  }
-  const double inv = s > 0.0 ? 1.0 / s : 0.0;
-  // the factors of frequency f + 1 are loaded while frequency f is quantized, so the
-  // loop does not wait on one L2 round trip per frequency
-  double2 gn[4];
-  int sn = 0;
-  auto fetch = [&](int f) {
-    const double2* gf = reinterpret_cast<const double2*>(G + (int64_t)f * lenp + p);
-#pragma unroll
-    for (int e = 0; e < 4; ++e) gn[e] = __ldg(gf + e);
-    sn = __ldg(wsgn + f);
-  };
-  fetch(0);
-#pragma unroll 1
-  for (int f = 0; f < nw; ++f) {
-    double gv[8];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) gv[2 * e] = gn[e].x, gv[2 * e + 1] = gn[e].y;
-    const bool mixed = sn == 0;
-    if (f + 1 < nw) fetch(f + 1);
-    uint32_t ar[SP_SF][2], ai[SP_SF][2], br[SP_SF][2], bim[SP_SF][2];
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      uint32_t yr[4], yi[4], pr[SP_SF], pi[SP_SF];
-      double gq[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        gq[e] = gv[4 * q + e] * inv;
-        const double ga = fabs(gq[e]);
-        yr[e] = round_mul(xr[4 * q + e], ga);
-        yi[e] = round_mul(xi[4 * q + e], ga);
-      }
-      digit_planes<SP_SF>(yr, pr);
-      digit_planes<SP_SF>(yi, pi);
-#pragma unroll
-      for (int t = 0; t < SP_SF; ++t) ar[t][q] = pr[t], ai[t][q] = pi[t];
-      if (mixed) {
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-          if (gq[e] < 0.0) yr[e] = 0u - yr[e], yi[e] = 0u - yi[e];
-        digit_planes<SP_SF>(yr, pr);
-        digit_planes<SP_SF>(yi, pi);
-#pragma unroll
-        for (int t = 0; t < SP_SF; ++t) br[t][q] = pr[t], bim[t][q] = pi[t];
-      }
-    }
-#pragma unroll
-    for (int t = 0; t < SP_SF; ++t) {
-      const int64_t plane = (int64_t)f * SP_SLOT + t;
-      __stcs(reinterpret_cast<uint2*>(F + o_re + plane * pstride), make_uint2(ar[t][0], ar[t][1]));
-      __stcs(reinterpret_cast<uint2*>(F + o_im + plane * pstride), make_uint2(ai[t][0], ai[t][1]));
-    }
-    if (mixed) {
-#pragma unroll
-      for (int t = 0; t < SP_SF; ++t) {
-        const int64_t plane = (int64_t)f * SP_SLOT + SP_SF + t;
-        __stcs(reinterpret_cast<uint2*>(F + o_re + plane * pstride), make_uint2(br[t][0], br[t][1]));
-        __stcs(reinterpret_cast<uint2*>(F + o_im + plane * pstride), make_uint2(bim[t][0], bim[t][1]));
+        *reinterpret_cast<uint4*>(F + o_re + plane * pstride) = make_uint4(br[t][0], br[t][1], br[t][2], br[t][3]);
+        *reinterpret_cast<uint4*>(F + o_im + plane * pstride) = make_uint4(bim[t][0], bim[t][1], bim[t][2], bim[t][3]);
       }
     }
   }
@@ -254,7 +170,7 @@ __device__ __forceinline__ void quantize_task_real(const double* __restrict__ co
                                                    int8_t* __restrict__ F) {
   double x[16];
 #pragma unroll
-  for (int k = 0; k < 16; ++k) x[k] = (col_ok && p + k < len) ? __ldcs(col + p + k) : 0.0;
+  for (int k = 0; k < 16; ++k) x[k] = (col_ok && p + k < len) ? __ldg(col + p + k) : 0.0;
   const double inv = s > 0.0 ? 1.0 / s : 0.0;
   for (int f = 0; f < nw; ++f) {
     const double* gf = G + (int64_t)f * lenp + p;
@@ -284,11 +200,11 @@ __device__ __forceinline__ void quantize_task_real(const double* __restrict__ co
     }
 #pragma unroll
     for (int t = 0; t < SP_SF; ++t)
-      __stcs(reinterpret_cast<uint4*>(F + o + ((int64_t)f * SP_SLOT + t) * pstride), make_uint4(a[t][0], a[t][1], a[t][2], a[t][3]));
+      *reinterpret_cast<uint4*>(F + o + ((int64_t)f * SP_SLOT + t) * pstride) = make_uint4(a[t][0], a[t][1], a[t][2], a[t][3]);
     if (mixed) {
 #pragma unroll
       for (int t = 0; t < SP_SF; ++t)
-        __stcs(reinterpret_cast<uint4*>(F + o + ((int64_t)f * SP_SLOT + SP_SF + t) * pstride), make_uint4(b[t][0], b[t][1], b[t][2], b[t][3]));
+        *reinterpret_cast<uint4*>(F + o + ((int64_t)f * SP_SLOT + SP_SF + t) * pstride) = make_uint4(b[t][0], b[t][1], b[t][2], b[t][3]);
     }
   }
 }

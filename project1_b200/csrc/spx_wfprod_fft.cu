@@ -199,6 +199,10 @@ __device__ __forceinline__ void fft16_fwd(double2 (&v)[16], const double2* __res
   for (int c = 0; c < 4; ++c) dft4_fwd(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);  // v[4c + d] = X[c + 4d]
 }
 
+// Shared-memory row strides of the line FFT: 17 complex per (line, phase) spectrum and
+// n + 1 per kz row, so that lanes walking lines hit distinct banks.
+constexpr int FFTR_LD = 17;
+
 struct PairFftParams {
   const double2* A;    // [kl*nocc + n][x][y][z]
   const double2* B;    // [kl*nunocc + n'][x][y][z]
@@ -216,8 +220,8 @@ __global__ void __launch_bounds__(512) fft_pair_zy_radix_kernel(PairFftParams p)
   const int n = p.n, r = p.r, per = n * r;
   double2* tw = smr;                                 // [n]
   double2* w16 = tw + n;                             // [16]
-  double2* Fb = w16 + 16;                            // [bpc][n lines][r][16]
-  double2* T1 = Fb + (size_t)p.bpc * n * r * 16;     // [bpc][FFT_KMAX][n]
+  double2* Fb = w16 + 16;                            // [bpc][n lines][r][FFTR_LD]
+  double2* T1 = Fb + (size_t)p.bpc * n * r * FFTR_LD;  // [bpc][FFT_KMAX][n + 1]
   const int kn = blockIdx.x, grp = blockIdx.y, x = blockIdx.z;
   const int kl = kn / p.nocc;
   for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = p.twf[i];
@@ -226,8 +230,9 @@ __global__ void __launch_bounds__(512) fft_pair_zy_radix_kernel(PairFftParams p)
   const int j = threadIdx.x / per, t = threadIdx.x - j * per;
   const int np = grp * p.bpc + j;
   const bool live = j < p.bpc && np < p.nunocc;
-  double2* F = Fb + (size_t)j * n * r * 16;
-  double2* T = T1 + (size_t)j * FFT_KMAX * n;
+  double2* F = Fb + (size_t)j * n * r * FFTR_LD;
+  double2* T = T1 + (size_t)j * FFT_KMAX * (n + 1);
+  const int tl = n + 1;
   // z pass: line y = t / r of the product plane A(x, y, .) B(x, y, .)
   if (live) {
     const int y = t / r, n2 = t - (t / r) * r;
@@ -240,7 +245,7 @@ __global__ void __launch_bounds__(512) fft_pair_zy_radix_kernel(PairFftParams p)
       v[n1] = cmul(__ldg(a + z), __ldg(bl + z));
     }
     fft16_fwd(v, w16);
-    double2* f = F + ((size_t)y * r + n2) * 16;
+    double2* f = F + ((size_t)y * r + n2) * FFTR_LD;
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) f[k1] = n2 ? cmul(v[fft16_pos(k1)], tw[n2 * k1]) : v[fft16_pos(k1)];
   }
@@ -250,10 +255,10 @@ __global__ void __launch_bounds__(512) fft_pair_zy_radix_kernel(PairFftParams p)
     for (int o = t; o < p.nkz * n; o += per) {
       const int kk = o / n, y = o - kk * n;
       const int k = p.kz[kk], k1 = k & 15, k2 = k >> 4;
-      const double2* f = F + (size_t)y * r * 16 + k1;
+      const double2* f = F + (size_t)y * r * FFTR_LD + k1;
       double2 acc = f[0];
-      for (int n2 = 1; n2 < r; ++n2) cfma(acc, f[n2 * 16], tw[(16 * n2 * k2) % n]);
-      T[kk * n + y] = acc;
+      for (int n2 = 1; n2 < r; ++n2) cfma(acc, f[n2 * FFTR_LD], tw[(16 * n2 * k2) % n]);
+      T[kk * tl + y] = acc;
     }
   }
   __syncthreads();
@@ -262,9 +267,9 @@ __global__ void __launch_bounds__(512) fft_pair_zy_radix_kernel(PairFftParams p)
     const int kk = t / r, n2 = t - (t / r) * r;
     double2 v[16];
 #pragma unroll
-    for (int n1 = 0; n1 < 16; ++n1) v[n1] = T[kk * n + r * n1 + n2];
+    for (int n1 = 0; n1 < 16; ++n1) v[n1] = T[kk * tl + r * n1 + n2];
     fft16_fwd(v, w16);
-    double2* f = F + ((size_t)kk * r + n2) * 16;
+    double2* f = F + ((size_t)kk * r + n2) * FFTR_LD;
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) f[k1] = n2 ? cmul(v[fft16_pos(k1)], tw[n2 * k1]) : v[fft16_pos(k1)];
   }
@@ -275,9 +280,9 @@ __global__ void __launch_bounds__(512) fft_pair_zy_radix_kernel(PairFftParams p)
     for (int o = t; o < p.nkz * p.nky; o += per) {
       const int kk = o / p.nky, kyi = o - kk * p.nky;
       const int k = p.ky[kyi], k1 = k & 15, k2 = k >> 4;
-      const double2* f = F + (size_t)kk * r * 16 + k1;
+      const double2* f = F + (size_t)kk * r * FFTR_LD + k1;
       double2 acc = f[0];
-      for (int n2 = 1; n2 < r; ++n2) cfma(acc, f[n2 * 16], tw[(16 * n2 * k2) % n]);
+      for (int n2 = 1; n2 < r; ++n2) cfma(acc, f[n2 * FFTR_LD], tw[(16 * n2 * k2) % n]);
       out[o] = acc;
     }
   }
@@ -533,11 +538,11 @@ int wfprod_pw_fft_run(spx_ctx* ctx, const spx_pw_desc* d, int nk, int nocc, int 
   const size_t zy_smem = sizeof(double2) * ((size_t)n * n + 2 * FFT_KMAX * n + (size_t)FFT_NP * FFT_KMAX * n);
   const size_t x_smem = sizeof(double2) * ((size_t)FFT_KMAX * n + d->ngptm + (size_t)FFT_XC * nky * nkz);
   cudaFuncSetAttribute(fft_pair_zy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zy_smem);
-  // grid edges 16 r (r <= 4) take the line FFT; bpc bands per CTA within 100 KB of
+  // grid edges 16 r (r <= 4) take the line FFT; bpc bands per CTA within 108 KB of
   // shared memory and 512 threads
   const bool radix = n % 16 == 0 && n / 16 >= 1 && n / 16 <= 4;
-  const size_t band_smem = sizeof(double2) * ((size_t)n * (n / 16) * 16 + (size_t)FFT_KMAX * n);
-  const int bpc = radix ? std::max(1, std::min({4, 512 / (n * (n / 16)), (int)((100 << 10) / band_smem)})) : 1;
+  const size_t band_smem = sizeof(double2) * ((size_t)n * (n / 16) * FFTR_LD + (size_t)FFT_KMAX * (n + 1));
+  const int bpc = radix ? std::max(1, std::min({4, 512 / (n * (n / 16)), (int)((108 << 10) / band_smem)})) : 1;
   const size_t radix_smem = sizeof(double2) * ((size_t)n + 16) + bpc * band_smem;
   if (radix)
     cudaFuncSetAttribute(fft_pair_zy_radix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)radix_smem);
