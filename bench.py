@@ -242,9 +242,15 @@ def int8_ops(N: int, P: int, nw: int, variant: int, slab: int) -> float:
     64-blocks; CTA pair: two tiles per pair item), over the slabs padded to 64 pairs, 2 ops
     per MAC."""
     nblk = (N + 63) // 64
-    tiles = nblk * (nblk + 1) // 2 if variant in (1, 3) else 2 * sum(bj // 2 + 1 for bj in range(nblk))
+    if variant == 5:
+        # 64 x 80 complex tiles: 128 x 160 real MMA tiles, column blocks of 80
+        tiles = upper_tiles(N, 5)
+        ncols = 160
+    else:
+        tiles = nblk * (nblk + 1) // 2 if variant in (1, 3) else 2 * sum(bj // 2 + 1 for bj in range(nblk))
+        ncols = 128
     pad = sum(((min(slab, P - s0) + 63) // 64) * 64 for s0 in range(0, P, slab))
-    return 2.0 * 6 * 128 * 128 * tiles * pad * nw
+    return 2.0 * 6 * 128 * ncols * tiles * pad * nw
 
 
 def fp64_roofline(ctx, N: int, achieved: float) -> dict:
@@ -261,7 +267,16 @@ def fp64_roofline(ctx, N: int, achieved: float) -> dict:
             "peak_source": "measured: spx_measure_dmma_peak (mma.sync m16n8k8 f64 loop, CUDA events)"}
 
 
-def measured_traffic(kernel: str, nbas: int, nw: int, slab: int, npair_step: int):
+def upper_tiles(N: int, variant: int) -> int:
+    """Upper-region tiles the accumulation kernel visits per frequency: 64 x 64 complex
+    tiles, or 64 x 80 for variant 5 (column blocks of 80, row blocks of 64)."""
+    nblk = (N + 63) // 64
+    if variant == 5:
+        return sum(min((bj * 80 + 79) // 64, nblk - 1) + 1 for bj in range(-(-N // 80)))
+    return nblk * (nblk + 1) // 2
+
+
+def measured_traffic(kernel: str, nbas: int, nw: int, slab: int, npair_step: int, tiles: int = 0):
     """DRAM bytes of the dominant kernel from the committed ncu capture, scaled to one
     launch (one slab of all frequencies) of this shape: the capture's bytes per pair,
     frequency and 64-block tile. None when no capture of `kernel` is recorded."""
@@ -279,7 +294,8 @@ def measured_traffic(kernel: str, nbas: int, nw: int, slab: int, npair_step: int
         key = min(rec["by_slab"], key=lambda k: abs(int(k) - slab))
         rec = dict(rec["by_slab"][key], captured_slab=int(key))
     nblk = (nbas + 63) // 64
-    per_launch = rec["bytes_per_pair_freq_tile"] * min(slab, npair_step) * nw * nblk * (nblk + 1) / 2
+    tiles = tiles or nblk * (nblk + 1) // 2
+    per_launch = rec["bytes_per_pair_freq_tile"] * min(slab, npair_step) * nw * tiles
     out = {"bytes_per_launch": per_launch, "launches_per_step": -(-npair_step // slab),
            "source": rec["source"]}
     if "captured_slab" in rec:
@@ -440,6 +456,26 @@ def run_ours(args):
         e2e = {"value": w.flops / dt / 1e12, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3, "steps": args.e2e_steps,
                "warmup": 1, "source": "pinned host memory"}
+        # the host link's own rate (one pinned 2 GiB copy to the device, CUDA events): the
+        # end-to-end step cannot beat its bytes over this rate
+        nbw = min(host.numel(), (2 << 30) // 16)
+        src = host.view(-1)[:nbw]
+        dst = torch.empty(nbw, dtype=torch.complex128, device=dev)
+        dst.copy_(src, non_blocking=True)
+        torch.cuda.synchronize()
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record()
+        dst.copy_(src, non_blocking=True)
+        c1.record()
+        torch.cuda.synchronize()
+        h2d_gbs = 16.0 * nbw / (c0.elapsed_time(c1) * 1e-3) / 1e9
+        del dst
+        e2e["h2d_link_gbs"] = h2d_gbs
+        e2e["copy_bound_ms"] = (h2d + d2h) / (h2d_gbs * 1e9) * 1e3
+        e2e["roofline"] = {"bound": "host link (PCIe)", "achieved_gbs": (h2d + d2h) / dt / 1e9,
+                           "peak_gbs": h2d_gbs, "frac": (h2d + d2h) / dt / 1e9 / h2d_gbs,
+                           "peak_source": "measured: one 2 GiB pinned host-to-device copy"}
         ctx2.close()
         del host
 
@@ -457,7 +493,7 @@ def run_ours(args):
         roof = {"bound": "tensor", "achieved": ach, "peak": bf16s, "unit": UNIT, "frac": ach / bf16s,
                 "traffic": None, "peak_source": f"{src} bf16_tflops_sustained (kernel timed inside a long step)"}
         # the same kernel seen from the int8 pipe it runs on, for the variant and slab that ran
-        variant = tuned["variant"] if tuned else (ctx.split_variant if ctx.split_variant in (1, 3) else 2)
+        variant = tuned["variant"] if tuned else (ctx.split_variant if ctx.split_variant in (1, 3, 5) else 2)
         slab = tuned["slab_pairs"] if tuned else 32768
         ops = int8_ops(N, Pr, nw, variant, slab)
         i8 = ops / (kernel_ms * 1e-3) / 1e12
@@ -465,8 +501,9 @@ def run_ours(args):
                              "achieved_tops": i8, "peak_tops": 2 * bf16s, "frac": i8 / (2 * bf16s),
                              "peak_source": "2 x measured bf16 sustained (int8 peak is 16384 ops/cycle/SM "
                                             "in ncu, twice the bf16 pipe)"}
-        kname = {1: "split_gram_kernel", 2: "split_gram2_kernel", 3: "pb_kernel"}.get(variant, "split_gram_kernel")
-        tr = measured_traffic(kname, N, nw, slab, Pr)
+        kname = {1: "split_gram_kernel", 2: "split_gram2_kernel", 3: "pb_kernel",
+                 5: "split_gram_kernel_64x80"}.get(variant, "split_gram_kernel")
+        tr = measured_traffic(kname, N, nw, slab, Pr, upper_tiles(N, variant))
         if tr:
             nblk = (N + 63) // 64
             R = (nblk + 1) // 2 * 2 * 128
@@ -792,9 +829,9 @@ def main():
     ap.add_argument("--c4-kpts", type=int, default=0, help="override the products workload's k-point count (profiling)")
     ap.add_argument("--precision", choices=["split", "fp64"], default=None,
                     help="force the measured path (profiling captures)")
-    ap.add_argument("--variant", type=int, default=0, choices=[0, 1, 2, 3],
-                    help="accumulation kernel: 1 one CTA per tile, 2 CTA pair, 3 persistent schedule, "
-                         "0 the library's choice")
+    ap.add_argument("--variant", type=int, default=0, choices=[0, 1, 2, 3, 5],
+                    help="accumulation kernel: 1 one CTA per 64 x 64 tile, 2 CTA pair, 3 persistent "
+                         "schedule, 5 one CTA per 64 x 80 tile, 0 the library's choice")
     ap.add_argument("--slab", type=int, default=0,
                     help="pin the split path's slab (pairs per exact accumulation; profiling)")
     ap.add_argument("--kpts", type=int, default=0, help="override the k-point count (profiling)")

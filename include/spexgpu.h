@@ -67,9 +67,10 @@ typedef struct spx_options {
   int64_t pinned_limit;     /* pinned host staging bytes, 0 = auto               */
   int32_t chunk_pairs;      /* band pairs per streamed chunk, 0 = auto           */
   int32_t timeout_ms;       /* bound on every device-side wait, 0 = 4000 ms      */
-  int32_t split_variant;    /* split-path kernel: 0 auto, 1 one CTA per tile,
-                               2 CTA pair (tcgen05 cta_group::2), 3 the persistent
-                               schedule with its own preparation warps           */
+  int32_t split_variant;    /* split-path kernel: 0 auto, 1 one CTA per 64 x 64
+                               tile, 2 CTA pair (tcgen05 cta_group::2), 3 the
+                               persistent schedule with its own preparation warps,
+                               5 one CTA per 64 x 80 tile (N = 160 MMAs)         */
   int32_t products;         /* interstitial product GEMM: SPX_PRODUCTS_*         */
 } spx_options;
 
@@ -362,7 +363,7 @@ int spx_dielec_dev(spx_ctx* ctx, int32_t nbas, int32_t nw, double* susceph,
 typedef struct spx_q_desc {
   int32_t nbas;             /* N_MB of this q                                         */
   int32_t variant;          /* split kernel: 0 tuned / context default, 1 one CTA per
-                               tile, 2 CTA pair                                       */
+                               64 x 64 tile, 2 CTA pair, 5 one CTA per 64 x 80 tile   */
   int64_t npair;
   int32_t slab_pairs;       /* pairs per exact int32 slab, multiple of 64 and
                                <= 32768; 0 tuned / 32768                              */
@@ -390,14 +391,15 @@ int spx_chi0_batched(spx_ctx* ctx, int32_t nq, const spx_q_desc* q, int32_t nw,
 
 /* Split-path tuning table of a context: per (N_MB bucket, pair bucket, nw) the
  * kernel variant and slab size that measured fastest on a probe of that shape,
- * for single calls (variant 1, 2 or 3) and for the batched schedule (variant 4,
+ * for single calls (variant 1, 2, 3 or 5) and for the batched schedule (variant 4,
  * with its tile shape). */
 typedef struct spx_tune_entry {
   int32_t nbas_bucket;      /* ceil(nbas / 128)                                        */
   int32_t npair_bucket;     /* 0: npair <= 16384, 1: <= 32768, 2: more                 */
   int32_t nw;
-  int32_t variant;          /* single calls: 1 one CTA per tile, 2 CTA pair, 3 the
-                               persistent schedule; 4 an entry of the batched table   */
+  int32_t variant;          /* single calls: 1 one CTA per 64 x 64 tile, 2 CTA pair,
+                               3 the persistent schedule, 5 one CTA per 64 x 80 tile;
+                               4 an entry of the batched table                        */
   int32_t slab_pairs;
   int32_t tile;             /* variants 3 and 4: tile columns (64 or 32) + 256 *
                                pipeline stages (3 or 4); 0 otherwise                  */
@@ -413,7 +415,7 @@ int spx_tune_lookup(const spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
                     spx_tune_entry* out);
 /* The same for the persistent batched schedule: measures its tile shapes (64 or 32
  * complex columns per tile, 3 or 4 pipeline stages) and slab sizes on a seeded
- * probe of one q, stores the fastest (variant 3), and looks entries up. */
+ * probe of one q, stores the fastest (variant 4), and looks entries up. */
 int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
                          spx_tune_entry* out);
 int spx_tune_lookup_batched(const spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,

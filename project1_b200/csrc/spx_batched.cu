@@ -39,6 +39,7 @@ int launch_gen_cmatrix_rows(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, int6
                             int64_t, double, double2*, cudaStream_t);
 int launch_gen_normal(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, double, double*,
                       cudaStream_t);
+int launch_abs(spx_ctx*, int64_t, double*, cudaStream_t);
 
 struct PbConfig {
   int bn, stages;
@@ -88,11 +89,12 @@ static QPlan plan_q(const spx_ctx* ctx, const spx_q_desc& q, int nw, int precisi
   p.slab = q.slab_pairs;
   if (precision == SPX_SPLIT && (p.variant == 0 || p.slab == 0)) {
     const spx_tune_entry* t = find_tune(ctx, q.nbas, q.npair, nw);
+    // the slab kernels: one CTA (64 x 64 or 64 x 80 tiles) or the CTA pair
+    auto slab_kernel = [](int v) { return v == 1 || v == 2 || v == 5; };
     if (p.variant == 0)
-      p.variant = t && t->variant <= 2 ? t->variant
-                                       : (ctx->opt.split_variant == 1 || ctx->opt.split_variant == 2
-                                              ? ctx->opt.split_variant
-                                              : kDefaultVariant);
+      p.variant = t && slab_kernel(t->variant) ? t->variant
+                                               : (slab_kernel(ctx->opt.split_variant) ? ctx->opt.split_variant
+                                                                                      : kDefaultVariant);
     if (p.slab == 0) p.slab = t ? t->slab_pairs : kDefaultSlab;
   }
   if (p.slab <= 0) p.slab = kDefaultSlab;
@@ -181,7 +183,7 @@ extern "C" int spx_chi0_batched(spx_ctx* ctx, int32_t nq, const spx_q_desc* q, i
     const std::string at = " in q " + std::to_string(i);
     if (d.nbas < 0 || d.npair < 0) return set_error(ctx, SPX_EINVAL, "negative size" + at);
     if (d.nbas > 46340) return set_error(ctx, SPX_EINVAL, "nbas too large" + at);
-    if (d.slab_pairs < 0 || d.variant < 0 || d.variant > 2)
+    if (d.slab_pairs < 0 || d.variant < 0 || (d.variant > 2 && d.variant != 5))
       return set_error(ctx, SPX_EINVAL, "bad variant or slab" + at);
     if (d.npair > 0 && d.nbas > 0 && nw > 0) {
       if (!d.ediff || !d.susceph || !omega) return set_error(ctx, SPX_EINVAL, "null array" + at);
@@ -358,10 +360,12 @@ extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int
   double* OM = (double*)(b += w_bytes);
   void* S = (void*)(b += om_bytes);
   cudaStream_t s = ctx->stream;
-  // seeded probe: M ~ N(0,1)/sqrt(N), energy differences 3 N(0,1), frequencies 1..nw
+  // seeded probe: M ~ N(0,1)/sqrt(N), energy differences |3 N(0,1)| (one-signed
+  // weights, as on the imaginary axis), frequencies 1..nw
   if ((rc = launch_gen_cmatrix_rows(ctx, 0x5eed, 77, P, 0, P, nbas, ld,
                                     1.0 / std::sqrt((double)nbas), M, s)) ||
-      (rc = launch_gen_normal(ctx, 0x5eed, 78, 0, P, 3.0, E, s)))
+      (rc = launch_gen_normal(ctx, 0x5eed, 78, 0, P, 3.0, E, s)) ||
+      (rc = launch_abs(ctx, P, E, s)))
     return rc;
   std::vector<double> om(nw);
   for (int f = 0; f < nw; ++f) om[f] = 1.0 + f;
@@ -377,35 +381,46 @@ extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int
   best.tflops = -1;
   const double flops = 8.0 * (double)nbas * nbas * (double)P * nw;
   cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
-  // variants 1 and 2: the slab kernels with the quantizer beside them; 3: the
-  // persistent schedule (its own preparation warps, 64 x 64 tiles, 3 stages)
-  for (int variant = 1; variant <= 3; ++variant)
+  // Candidates: variants 1, 5 and 2 (the slab kernels with the quantizer beside them:
+  // one CTA per 64 x 64 tile, one CTA per 64 x 80 tile, the CTA pair) and 3 (the
+  // persistent schedule with its own preparation warps, 64 x 64 tiles, 3 stages), at
+  // each slab size. The rounds interleave the candidates, so a clock that drifts under
+  // the power cap while the probe runs favours none of them; each keeps its best round.
+  struct Cand {
+    int variant, slab;
+    float ms;
+  };
+  std::vector<Cand> cands;
+  for (int variant : {1, 5, 2, 3})
     for (int sl : slabs) {
       if (sl == 32768 && npair <= 16384) continue;  // one slab either way
-      int launches = 0;
-      float best_ms = 1e30f;
-      for (int rep = 0; rep < 2; ++rep) {  // the first run warms up
-        cudaEventRecord(e0, s);
-        if (variant == 3)
-          rc = pb_single(ctx, M, ld, P, nbas, E, nullptr, 1.0, nw, OM, O, 64 + 3 * 256, sl, (char*)S,
-                         sws, s, &launches);
-        else
-          rc = split_chi0_slab(ctx, M, ld, P, nbas, W, ld, nw, O, S, sws, s, &launches, variant, sl);
-        if (rc) return rc;
-        cudaEventRecord(e1, s);
-        if ((rc = collect_status(ctx, s, "autotune"))) return rc;
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (rep) best_ms = std::min(best_ms, ms);
-      }
-      const double tf = flops / (best_ms * 1e-3) / 1e12;
-      if (tf > best.tflops) {
-        best.tflops = tf;
-        best.variant = variant;
-        best.slab_pairs = sl;
-        best.tile = variant == 3 ? 64 + 3 * 256 : 0;
-      }
+      cands.push_back({variant, sl, 1e30f});
     }
+  for (int round = 0; round < 3; ++round)  // round 0 warms up
+    for (auto& c : cands) {
+      int launches = 0;
+      cudaEventRecord(e0, s);
+      if (c.variant == 3)
+        rc = pb_single(ctx, M, ld, P, nbas, E, nullptr, 1.0, nw, OM, O, 64 + 3 * 256, c.slab, (char*)S,
+                       sws, s, &launches);
+      else
+        rc = split_chi0_slab(ctx, M, ld, P, nbas, W, ld, nw, O, S, sws, s, &launches, c.variant, c.slab);
+      if (rc) return rc;
+      cudaEventRecord(e1, s);
+      if ((rc = collect_status(ctx, s, "autotune"))) return rc;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (round) c.ms = std::min(c.ms, ms);
+    }
+  for (const auto& c : cands) {
+    const double tf = flops / (c.ms * 1e-3) / 1e12;
+    if (tf > best.tflops) {
+      best.tflops = tf;
+      best.variant = c.variant;
+      best.slab_pairs = c.slab;
+      best.tile = c.variant == 3 ? 64 + 3 * 256 : 0;
+    }
+  }
   store_tune(ctx, best);
   if (out) *out = best;
   return SPX_OK;
@@ -476,7 +491,7 @@ extern "C" int spx_tune_load(spx_ctx* ctx, const char* path) {
       return set_error(ctx, SPX_EINVAL, "malformed tuning entry");
     json_field(obj, "tflops", &tf);
     json_field(obj, "tile", &tile);
-    if (var < 1 || var > 4 || sl < 64 || sl > 32768 || nb < 1 || nw < 1 || pb < 0 || pb > 2 ||
+    if (var < 1 || var > 5 || sl < 64 || sl > 32768 || nb < 1 || nw < 1 || pb < 0 || pb > 2 ||
         tile < 0 || tile > 4 * 256 + 64)
       return set_error(ctx, SPX_EINVAL, "tuning entry out of range");
     spx_tune_entry t{};

@@ -901,6 +901,7 @@ using namespace spx;
 
 namespace spx {
 int launch_gen_normal(spx_ctx*, uint64_t, uint32_t, int64_t, int64_t, double, double*, cudaStream_t);
+int launch_abs(spx_ctx*, int64_t, double*, cudaStream_t);
 }
 
 // Times the persistent schedule's tile shapes and slab sizes on a seeded probe of one
@@ -931,6 +932,7 @@ extern "C" int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, i
   std::vector<double> om(nw);
   for (int f = 0; f < nw; ++f) om[f] = 1.0 + f;
   int rc = launch_gen_normal(ctx, 0x5eed, 78, 0, P, 3.0, E, s);
+  if (!rc) rc = launch_abs(ctx, P, E, s);  // positive energies: one-signed weights
   if (!rc) rc = check_cuda(ctx, cudaMemcpyAsync(OM, om.data(), sizeof(double) * nw, cudaMemcpyHostToDevice, s), "probe");
   if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(s), "probe");
   spx_tune_entry best{};
@@ -951,27 +953,37 @@ extern "C" int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, i
   d.susceph = O;
   const double flops = 8.0 * (double)nbas * nbas * (double)P * nw;
   cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
-  for (int ci = 0; ci < 3 && !rc; ++ci)
+  // rounds interleave the candidates (tile shape x slab) so that clock drift under the
+  // power cap favours none of them; round 0 warms up, each keeps its best round
+  struct Cand {
+    int ci, slab;
+    float ms;
+  };
+  std::vector<Cand> cands;
+  for (int ci = 0; ci < 3; ++ci)
     for (int sl : slabs) {
       if (sl == 32768 && P <= 16384) continue;
-      float best_ms = 1e30f;
-      for (int rep = 0; rep < 2 && !rc; ++rep) {
-        int launches = 0;
-        cudaEventRecord(e0, s);
-        rc = pb_run(ctx, 1, &d, nw, OM, SPX_BATCH_NOGRAPH, s, &launches, &cfgs[ci], sl, nullptr, 0);
-        if (rc) break;
-        cudaEventRecord(e1, s);
-        if ((rc = collect_status(ctx, s, "batched autotune"))) break;
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (rep) best_ms = std::min(best_ms, ms);
-      }
+      cands.push_back({ci, sl, 1e30f});
+    }
+  for (int round = 0; round < 3 && !rc; ++round)
+    for (auto& c : cands) {
+      int launches = 0;
+      cudaEventRecord(e0, s);
+      rc = pb_run(ctx, 1, &d, nw, OM, SPX_BATCH_NOGRAPH, s, &launches, &cfgs[c.ci], c.slab, nullptr, 0);
       if (rc) break;
-      const double tf = flops / (best_ms * 1e-3) / 1e12;
+      cudaEventRecord(e1, s);
+      if ((rc = collect_status(ctx, s, "batched autotune"))) break;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (round) c.ms = std::min(c.ms, ms);
+    }
+  if (!rc)
+    for (const auto& c : cands) {
+      const double tf = flops / (c.ms * 1e-3) / 1e12;
       if (tf > best.tflops) {
         best.tflops = tf;
-        best.slab_pairs = sl;
-        best.tile = cfgs[ci].bn + 256 * cfgs[ci].stages;
+        best.slab_pairs = c.slab;
+        best.tile = cfgs[c.ci].bn + 256 * cfgs[c.ci].stages;
       }
     }
   cudaFree(buf);

@@ -51,21 +51,26 @@ constexpr int SP_THREADS = 192;        // warp 0 TMA, warp 1 MMA + TMEM, warps 2
 // quarter, each half of the columns): fewer registers per thread, so the operand
 // quantizer of the next slab keeps more warps resident beside it on every SM.
 constexpr int SP1_EPI = 8;
+constexpr int SP_WIDE_BN = 80;  // complex columns of the wide tile (variant 5): N = 160
 constexpr int SP1_THREADS = 64 + 32 * SP1_EPI;
-constexpr int SP1_NC = SP_TILE * 4 / SP1_EPI;  // complex columns per epilogue warp
 constexpr int SP1_REGS = 128;  // 40960 registers: two 96-register quantizer blocks fit beside
 
-struct __align__(1024) SplitSmem {
+// BROWS: real rows of the B tile (the MMA's N): 128 for 64 x 64 complex tiles, 160
+// for 64 x 80 (three orders x 160 TMEM columns still fit in 512).
+template <int BROWS>
+struct __align__(1024) SplitSmemT {
   uint8_t a[SP_ST][SP_SF][SP_PLANE];
-  uint8_t b[SP_ST][SP_SF][SP_PLANE];
+  uint8_t b[SP_ST][SP_SF][BROWS * SP_KB];
   uint64_t full[SP_ST];
   uint64_t empty[SP_ST];
   uint64_t tfull, tempty, mdone;
   uint32_t tmem_base;
 };
+using SplitSmem = SplitSmemT<SP_ROWS>;
 
 struct SplitParams {
   int N;
+  int nbr;                // 64-row blocks covering N
   int ntile;
   int nw;
   int nitems;
@@ -84,7 +89,7 @@ struct SplitParams {
 // i = 16q + lane/2, part c = lane & 1). The warp's part of the accumulator is read
 // into registers first and released to the MMA warp, so the next item's MMAs overlap
 // this tile's reductions into the output.
-template <int NC = SP_TILE, class Release>
+template <int NC = SP_TILE, int BN = SP_TILE, class Release>
 __device__ __forceinline__ void fold_epilogue(uint32_t tl, int q, int lane, int bi, int bj, int f,
                                               const SplitParams& prm, Release release, int j0 = 0) {
   const int c = lane & 1;
@@ -92,7 +97,7 @@ __device__ __forceinline__ void fold_epilogue(uint32_t tl, int q, int lane, int 
 #pragma unroll
   for (int cc = 0; cc < NC / 8; ++cc) {
     double T[16];
-    load_fold16(tl + (uint32_t)(2 * j0 + 16 * cc), 128u, T);
+    load_fold16(tl + (uint32_t)(2 * j0 + 16 * cc), (uint32_t)(2 * BN), T);
 #pragma unroll
     for (int jj = 0; jj < 8; ++jj) {
       // both lanes of a row pair send their (., Im_j) product to the other one
@@ -107,7 +112,7 @@ __device__ __forceinline__ void fold_epilogue(uint32_t tl, int q, int lane, int 
   double* ob = prm.out + 2 * (int64_t)f * prm.npack + 2 * gil + c;
 #pragma unroll
   for (int jj = 0; jj < NC; ++jj) {
-    const int gj = bj * SP_TILE + j0 + jj;
+    const int gj = bj * BN + j0 + jj;
     // one add per element per launch: launches are stream-ordered, so the sum is
     // deterministic, and the reduction needs no read round trip
     if (gil <= gj && gj < prm.N) atomicAdd(ob + (int64_t)gj * (gj + 1), fac * prm.sA[gj] * o[jj]);
@@ -138,11 +143,18 @@ __device__ __forceinline__ void real_epilogue(uint32_t tl, int q, int lane, int 
   release();
 }
 
-template <bool REAL>
+// BN: complex columns of a tile (64 or 80; the -DINV form uses 64, i.e. 128 x 128
+// real tiles). mapF loads 128-row A boxes, mapB (2 BN)-row B boxes.
+template <bool REAL, int BN>
 __global__ void __maxnreg__(SP1_REGS)
-    split_gram_kernel(const __grid_constant__ CUtensorMap mapF, SplitParams prm) {
+    split_gram_kernel(const __grid_constant__ CUtensorMap mapF, const __grid_constant__ CUtensorMap mapB,
+                      SplitParams prm) {
+  constexpr int BROWS = 2 * BN;
+  constexpr uint32_t IDESC = sp_idesc(BROWS);
+  static_assert(!REAL || BN == SP_TILE, "the -DINV form uses square tiles");
+  using Smem = SplitSmemT<BROWS>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  SplitSmem& sm = *reinterpret_cast<SplitSmem*>(
+  Smem& sm = *reinterpret_cast<Smem*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -175,10 +187,10 @@ __global__ void __maxnreg__(SP1_REGS)
       for (int item = blockIdx.x; item < prm.nitems && ok; item += gridDim.x, ++j) {
         const int f = item / prm.ntile;
         int bi, bj;
-        split_decode_tile(split_item_tile(item, prm.ntile, gridDim.x), &bi, &bj);
+        split_decode_tile_bn<BN>(split_item_tile(item, prm.ntile, gridDim.x), prm.nbr, &bi, &bj);
         const int sg = prm.wsgn[f];
-        // a diagonal tile of a one-signed frequency multiplies A by itself
-        const bool same = sg != 0 && bi == bj;
+        // a diagonal square tile of a one-signed frequency multiplies A by itself
+        const bool same = BN == SP_TILE && sg != 0 && bi == bj;
         const int za = f * SP_SLOT, zb = za + (sg == 0 ? SP_SF : 0);
         for (int ks = 0; ks < prm.nk; ++ks) {
           if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) {
@@ -186,9 +198,9 @@ __global__ void __maxnreg__(SP1_REGS)
             break;
           }
           const int kc = split_k_order(j, ks, prm.nk);
-          mbar_arrive_expect_tx(&sm.full[st], (uint32_t)((same ? 1 : 2) * SP_SF * SP_PLANE));
+          mbar_arrive_expect_tx(&sm.full[st], (uint32_t)(SP_SF * (SP_PLANE + (same ? 0 : BROWS * SP_KB))));
           tma_load_4d(&sm.a[st][0][0], &mapF, 0, bi * SP_ROWS, kc, za, &sm.full[st]);
-          if (!same) tma_load_4d(&sm.b[st][0][0], &mapF, 0, bj * SP_ROWS, kc, zb, &sm.full[st]);
+          if (!same) tma_load_4d(&sm.b[st][0][0], &mapB, 0, bj * BROWS, kc, zb, &sm.full[st]);
           issued[st] = true;
           last_ph[st] = ph;
           if (++st == SP_ST) st = 0, ph ^= 1u;
@@ -208,8 +220,8 @@ __global__ void __maxnreg__(SP1_REGS)
       for (int item = blockIdx.x; item < prm.nitems; item += gridDim.x, ++j) {
         const int f = item / prm.ntile;
         int bi, bj;
-        split_decode_tile(split_item_tile(item, prm.ntile, gridDim.x), &bi, &bj);
-        const bool same = prm.wsgn[f] != 0 && bi == bj;
+        split_decode_tile_bn<BN>(split_item_tile(item, prm.ntile, gridDim.x), prm.nbr, &bi, &bj);
+        const bool same = BN == SP_TILE && prm.wsgn[f] != 0 && bi == bj;
         // accumulators free (first item: immediately)
         if (!mbar_wait(&sm.tempty, (uint32_t)(j & 1) ^ 1u, prm.timeout_ns, prm.status)) break;
         tc_fence_after();
@@ -220,8 +232,8 @@ __global__ void __maxnreg__(SP1_REGS)
             break;
           }
           tc_fence_after();
-          // order g = t + u lives at TMEM columns [128 g, 128 g + 128); the first
-          // product of every order in a slab (first K step) overwrites it
+          // order g = t + u lives at TMEM columns [BROWS g, BROWS g + BROWS); the
+          // first product of every order in a slab (first K step) overwrites it
 #pragma unroll
           for (int kk = 0; kk < SP_NKS; ++kk) {
             uint64_t da[SP_SF], db[SP_SF];
@@ -231,12 +243,12 @@ __global__ void __maxnreg__(SP1_REGS)
               db[t] = same ? da[t] : desc_sw64(&sm.b[st][t][0]) + (uint64_t)(kk * 2);
             }
             const uint32_t k0 = (ks > 0 || kk > 0);
-            mma_i8<1>(tmem + 0 * 128, da[0], db[0], SP_IDESC, k0);
-            mma_i8<2>(tmem + 1 * 128, da[0], db[1], SP_IDESC, k0);
-            mma_i8<3>(tmem + 2 * 128, da[0], db[2], SP_IDESC, k0);
-            mma_i8<1>(tmem + 1 * 128, da[1], db[0], SP_IDESC, 1u);
-            mma_i8<3>(tmem + 2 * 128, da[1], db[1], SP_IDESC, 1u);
-            mma_i8<0>(tmem + 2 * 128, da[2], db[0], SP_IDESC, 1u);
+            mma_i8<1>(tmem + 0 * BROWS, da[0], db[0], IDESC, k0);
+            mma_i8<2>(tmem + 1 * BROWS, da[0], db[1], IDESC, k0);
+            mma_i8<3>(tmem + 2 * BROWS, da[0], db[2], IDESC, k0);
+            mma_i8<1>(tmem + 1 * BROWS, da[1], db[0], IDESC, 1u);
+            mma_i8<3>(tmem + 2 * BROWS, da[1], db[1], IDESC, 1u);
+            mma_i8<0>(tmem + 2 * BROWS, da[2], db[0], IDESC, 1u);
           }
           tc_commit(&sm.empty[st]);  // stage free once these MMAs have read it
           committed = true;
@@ -262,14 +274,15 @@ __global__ void __maxnreg__(SP1_REGS)
       tc_fence_after();
       const int f = item / prm.ntile;
       int bi, bj;
-      split_decode_tile(split_item_tile(item, prm.ntile, gridDim.x), &bi, &bj);
+      split_decode_tile_bn<BN>(split_item_tile(item, prm.ntile, gridDim.x), prm.nbr, &bi, &bj);
       auto release = [&] {
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.tempty);
       };
-      if constexpr (REAL) real_epilogue(tl, q, lane, bi, bj, f, prm, release, 2 * SP1_NC * h, 2 * SP1_NC);
-      else fold_epilogue<SP1_NC>(tl, q, lane, bi, bj, f, prm, release, SP1_NC * h);
+      constexpr int NC = BN * 4 / SP1_EPI;  // complex columns per epilogue warp
+      if constexpr (REAL) real_epilogue(tl, q, lane, bi, bj, f, prm, release, 2 * NC * h, 2 * NC);
+      else fold_epilogue<NC, BN>(tl, q, lane, bi, bj, f, prm, release, NC * h);
     }
   }
 
@@ -825,8 +838,8 @@ size_t split_workspace_bytes(int64_t P, int N, int nw) {
 
 void timing_mark(spx_ctx* ctx, cudaStream_t s, int kind);
 
-// variant: 1 one CTA per tile, 2 CTA pair, 0 the context's choice; slab: pairs per
-// exact int32 slab (0 = 32768).
+// variant: 1 one CTA per 64 x 64 tile, 2 CTA pair, 5 one CTA per 64 x 80 tile, 0 the
+// context's choice; slab: pairs per exact int32 slab (0 = 32768).
 int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N, const double* W,
                     int64_t ldw, int nw, double2* out, void* ws, size_t ws_bytes,
                     cudaStream_t stream, int* launches, int variant, int slab) {
@@ -856,8 +869,9 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
   // with increasing strides; a box (K, rows, 1, 3 planes) lands as [plane][row][K]
   const uint64_t nkb = (uint64_t)(L.Ps / SP_KB);
   if (variant == 0) variant = ctx->opt.split_variant;
-  const bool pair = variant != 1;  // 0 (auto) and 2 select the CTA pair
-  CUtensorMap mapF[2], mapFh[2];
+  const bool pair = variant != 1 && variant != 5;  // 0 (auto) and 2 select the CTA pair
+  const bool wide = variant == 5;                  // one CTA per 64 x 80 tile (N = 160)
+  CUtensorMap mapF[2], mapFh[2], mapW[2];
   for (int b = 0; b < nbuf; ++b) {
     const uint64_t st[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};
     const uint64_t d[4] = {SP_KB, (uint64_t)L.R, nkb, (uint64_t)SP_SLOT * nw};
@@ -867,23 +881,31 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
     const uint32_t bh[4] = {SP_KB, SP2_BROWS, 1, SP_SF};
     rc0 = make_tmap_u8_4d(ctx, &mapFh[b], F[b], d, st, bh, CU_TENSOR_MAP_SWIZZLE_64B);
     if (rc0) return rc0;
+    const uint32_t bw[4] = {SP_KB, 2 * SP_WIDE_BN, 1, SP_SF};
+    rc0 = make_tmap_u8_4d(ctx, &mapW[b], F[b], d, st, bw, CU_TENSOR_MAP_SWIZZLE_64B);
+    if (rc0) return rc0;
   }
   int rc = SPX_OK;
 
   const size_t smem = sizeof(SplitSmem) + 1024;
+  const size_t smemw = sizeof(SplitSmemT<2 * SP_WIDE_BN>) + 1024;
   const size_t smem2 = sizeof(Split2Smem) + 1024;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(split_gram_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(split_gram_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(split_gram_kernel<false, SP_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(split_gram_kernel<false, SP_WIDE_BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemw);
+    cudaFuncSetAttribute(split_gram_kernel<true, SP_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(split_gram2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem2);
     attr_set = true;
   }
+  const int nbr = (N + SP_TILE - 1) / SP_TILE;
   const int ntile = L.nblk * (L.nblk + 1) / 2;
-  int ntile2 = 0;
+  int ntile2 = 0, ntilew = 0;
   for (int bj = 0; bj < L.nblk; ++bj) ntile2 += bj / 2 + 1;
-  const int nitems = (pair ? ntile2 : ntile) * nw;
+  for (int bj = 0; bj * SP_WIDE_BN < N; ++bj) ntilew += split_rows_of(bj, SP_WIDE_BN, nbr);
+  const int ntile_used = pair ? ntile2 : (wide ? ntilew : ntile);
+  const int nitems = ntile_used * nw;
   const int grid = std::min(nitems, ctx->num_sms);
   const int npad = (int)(L.R / 2);  // columns covered by the stacked rows
   // CTA-pair launch: as many clusters as can be resident at once (persistent)
@@ -952,7 +974,8 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
     timing_mark(ctx, stream, 1);
     SplitParams prm;
     prm.N = N;
-    prm.ntile = pair ? ntile2 : ntile;
+    prm.nbr = nbr;
+    prm.ntile = ntile_used;
     prm.nw = nw;
     prm.nitems = nitems;
     prm.nk = lenp / SP_KB;
@@ -967,8 +990,11 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
     if (pair) {
       rc = check_cuda(ctx, cudaLaunchKernelEx(&cfg, split_gram2_kernel, mapF[b], mapFh[b], prm),
                       "split_gram2_kernel launch");
+    } else if (wide) {
+      split_gram_kernel<false, SP_WIDE_BN><<<grid, SP1_THREADS, smemw, stream>>>(mapF[b], mapW[b], prm);
+      rc = check_cuda(ctx, cudaGetLastError(), "split_gram_kernel (64 x 80) launch");
     } else {
-      split_gram_kernel<false><<<grid, SP1_THREADS, smem, stream>>>(mapF[b], prm);
+      split_gram_kernel<false, SP_TILE><<<grid, SP1_THREADS, smem, stream>>>(mapF[b], mapF[b], prm);
       rc = check_cuda(ctx, cudaGetLastError(), "split_gram_kernel launch");
     }
     if (rc) return rc;
@@ -1035,7 +1061,7 @@ int split_chi0_real_slab(spx_ctx* ctx, const double* M, int64_t ldc, int64_t P, 
     if (rc0) return rc0;
   }
   const size_t smem = sizeof(SplitSmem) + 1024;
-  cudaFuncSetAttribute(split_gram_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(split_gram_kernel<true, SP_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int ntile = L.nblk * (L.nblk + 1) / 2;
   const int nitems = ntile * nw;
   const int grid = std::min(nitems, ctx->num_sms);
@@ -1078,6 +1104,7 @@ int split_chi0_real_slab(spx_ctx* ctx, const double* M, int64_t ldc, int64_t P, 
     timing_mark(ctx, stream, 1);
     SplitParams prm;
     prm.N = N;
+    prm.nbr = (N + SP_ROWS - 1) / SP_ROWS;
     prm.ntile = ntile;
     prm.nw = nw;
     prm.nitems = nitems;
@@ -1089,7 +1116,7 @@ int split_chi0_real_slab(spx_ctx* ctx, const double* M, int64_t ldc, int64_t P, 
     prm.npack = (int64_t)N * (N + 1) / 2;
     prm.status = ctx->d_status;
     prm.timeout_ns = (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
-    split_gram_kernel<true><<<grid, SP1_THREADS, smem, stream>>>(mapF[b], prm);
+    split_gram_kernel<true, SP_TILE><<<grid, SP1_THREADS, smem, stream>>>(mapF[b], mapF[b], prm);
     if ((rc = check_cuda(ctx, cudaGetLastError(), "split_gram_kernel (real) launch"))) return rc;
     *launches += 1;
     timing_mark(ctx, stream, 2);

@@ -218,6 +218,25 @@ __device__ __forceinline__ void split_decode_tile(int t, int* bi, int* bj) {
   *bi = t - j * (j + 1) / 2;
 }
 
+// Tile t of the upper region for tiles of 64 rows x BN columns, column-major: column
+// block bj holds row blocks 0 .. min((bj BN + BN - 1) / 64, nbr - 1) (nbr row blocks
+// cover N). BN = 64 is the square case above.
+__host__ __device__ __forceinline__ int split_rows_of(int bj, int bn, int nbr) {
+  const int r = (bj * bn + bn - 1) / 64;
+  return (r < nbr - 1 ? r : nbr - 1) + 1;
+}
+template <int BN>
+__device__ __forceinline__ void split_decode_tile_bn(int t, int nbr, int* bi, int* bj) {
+  if constexpr (BN == SP_TILE) {
+    split_decode_tile(t, bi, bj);
+  } else {
+    int j = 0, c = 0;
+    while (c + split_rows_of(j, BN, nbr) <= t) c += split_rows_of(j++, BN, nbr);
+    *bj = j;
+    *bi = t - c;
+  }
+}
+
 // Tile of a frequency-major item when `grid` CTAs take items round-robin. A frequency's
 // ntile tiles fall into two rounds of the grid: the first `a` of them beside the
 // previous frequency's last tiles, the rest in the next round. The smaller part is made

@@ -127,6 +127,21 @@ int launch_gen_normal(spx_ctx* ctx, uint64_t seed, uint32_t sid, int64_t offset,
   return check_cuda(ctx, cudaGetLastError(), "gen_normal_kernel launch");
 }
 
+__global__ void abs_kernel(int64_t n, double* __restrict__ x) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x)
+    x[t] = fabs(x[t]);
+}
+
+// x = |x| in place (the autotuners' probe energies: positive transition energies
+// give one-signed imaginary-axis weights, as in the calls they tune for).
+int launch_abs(spx_ctx* ctx, int64_t n, double* x, cudaStream_t stream) {
+  if (n <= 0) return SPX_OK;
+  int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 32);
+  abs_kernel<<<grid, 256, 0, stream>>>(n, x);
+  return check_cuda(ctx, cudaGetLastError(), "abs_kernel launch");
+}
+
 int launch_gen_cmatrix(spx_ctx* ctx, uint64_t seed, uint32_t sid, int64_t rows, int64_t cols,
                        int64_t ld, int64_t col0, double scale, double* out,
                        cudaStream_t stream) {

@@ -98,16 +98,20 @@ def test_split_accumulates(ctx):
     assert np.max(np.abs(got - ref)) <= 1e-6 * np.max(np.abs(ref))
 
 
-@pytest.mark.parametrize("nbas,npair,nw", [(65, 3000, 2), (200, 40000, 3), (130, 33, 1)])
+@pytest.mark.parametrize("nbas,npair,nw", [(65, 3000, 2), (200, 40000, 3), (130, 33, 1),
+                                           (1200, 700, 2), (81, 5000, 1), (239, 2500, 2)])
 def test_split_cta_pair_equals_single_cta(nbas, npair, nw):
-    """The CTA-pair kernel (cta_group::2) and the one-CTA kernel sum the same exact
-    integers and add one FP64 term per element per launch: results are identical."""
+    """The CTA-pair kernel (cta_group::2), the one-CTA kernel on 64 x 64 tiles and the
+    one on 64 x 80 tiles (N = 160 MMAs) sum the same exact integers and add one FP64
+    term per element per launch: results are identical (ragged 80-column blocks
+    included)."""
     m, d, om = random_case(nbas, npair, nw, seed=nbas + 3 * npair, degfrac=0.01)
     outs = []
-    for variant in (1, 2):
+    for variant in (1, 2, 5):
         with spx.Context(0, split_variant=variant) as c:
             outs.append(run_dev(c, m, d, om, None, 0.5, precision="split"))
     assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[0], outs[2])
     ref = oracle.chi0(m, oracle.weights(d, om, None, 0.5), accurate=True)
     emax, fro = normalized_error(outs[1], ref, nbas)
     assert emax <= SPLIT_TOL and fro <= SPLIT_FRO, (emax, fro)
