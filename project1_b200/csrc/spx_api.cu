@@ -206,10 +206,13 @@ static int check_chi0_args(spx_ctx* ctx, const double* cprod, int64_t ldc, int64
 
 // Accumulates one slab of band pairs already on the device into the device
 // output. `W` is workspace for npair*nw weights (ldw = round_up(npair, 16)).
+// `plan` (variant, slab, tile), when given, replaces the per-call choice: a caller
+// that streams one array in chunks keeps one kernel and one slab size for all of it.
 static int chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N,
                      const double* ediff, const double* wscale, double scale_all, int nw,
                      const double* omega, int precision, double2* out, double* W,
-                     void* split_ws, size_t split_ws_bytes, cudaStream_t s, int* launches) {
+                     void* split_ws, size_t split_ws_bytes, cudaStream_t s, int* launches,
+                     const int* plan = nullptr) {
   const int64_t ldw = (int64_t)align_up((size_t)std::max<int64_t>(P, 1), 16);
   timing_mark(ctx, s, 0);
   int rc = launch_weights(ctx, P, ldw, ediff, wscale, scale_all, nw, omega, W, s);
@@ -223,7 +226,8 @@ static int chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int
     // kernel variant and slab from the context's tuning table when the caller left
     // the variant open and the table has this shape (smaller slabs need less scratch)
     int variant, slab, tile;
-    split_choice(ctx, N, P, nw, &variant, &slab, &tile);
+    if (plan) variant = plan[0], slab = plan[1], tile = plan[2];
+    else split_choice(ctx, N, P, nw, &variant, &slab, &tile);
     if (variant == 3) {
       // the persistent schedule forms its weights from ediff itself
       timing_mark(ctx, s, 1);
@@ -536,19 +540,24 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
   const bool pinned = is_pinned_or_device(cprod, &dev);
   if (dev) return set_error(ctx, SPX_EINVAL, "cprod is a device pointer; use spx_chi0_accumulate_dev");
 
+  // One split kernel and slab size for the whole array (chosen for npair), so that
+  // the chunks' exact slabs are the device call's: chunk boundaries stay on
+  // multiples of that slab and the result equals the device call's bit for bit.
+  int plan[3] = {0, 0, 64 + 3 * 256};
+  if (precision == SPX_SPLIT) split_choice(ctx, nbas, npair, nw, &plan[0], &plan[1], &plan[2]);
+  const int64_t align = precision == SPX_SPLIT ? (plan[1] > 0 ? plan[1] : 32768) : 16384;
   // slab size: band pairs per streamed chunk
   // By default the first chunk is short, since its copy overlaps nothing, and the
-  // chunks then grow by half each time, up to 262144 pairs: each chunk exposes one
-  // split-path operand preparation, and a chunk's copy (about 0.35 us per pair at
-  // N = 1200 over PCIe 5) must stay within the previous chunk's accumulation
-  // (about 0.6 us per pair). Boundaries stay on multiples of 32768, the exact-slab
-  // size of the split path. Pageable arrays keep 65536-pair chunks so that their
+  // chunks then grow by an eighth each time, up to 262144 pairs: a chunk's copy
+  // (about 0.35 us per pair at N = 1200 over PCIe 5) must stay within the previous
+  // chunk's accumulation (about 0.39 us per pair), and each chunk exposes one
+  // operand preparation. Pageable arrays keep 65536-pair chunks so that their
   // pinned staging stays small.
   const bool ramp = ctx->opt.chunk_pairs <= 0;
   int64_t slab = ctx->opt.chunk_pairs > 0 ? ctx->opt.chunk_pairs : (pinned ? 262144 : 65536);
   slab = std::min<int64_t>(slab, npair);
   slab = (int64_t)align_up((size_t)slab, 16);
-  const int64_t first = ramp ? std::min<int64_t>(slab, 32768) : slab;
+  const int64_t first = ramp ? std::min<int64_t>(slab, (int64_t)align_up(16384, (size_t)align)) : slab;
   const int nslab_buf = 2;
   const int64_t npack = (int64_t)nbas * (nbas + 1) / 2;
   const size_t out_bytes = align_up(sizeof(double) * 2 * (size_t)npack * nw, 256);
@@ -610,7 +619,7 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
     const int b = (int)(k & 1);
     const int64_t want =
         k == 0 ? first
-               : (ramp ? std::min<int64_t>(slab, (int64_t)align_up((size_t)(len * 3 / 2), 32768))
+               : (ramp ? std::min<int64_t>(slab, (int64_t)align_up((size_t)(len + len / 8), (size_t)align))
                        : slab);
     len = std::min<int64_t>(want, npair - p0);
     cudaStreamWaitEvent(xs, ev_free[b], 0);
@@ -638,7 +647,8 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
     cudaEventRecord(ev_copied[b], xs);
     cudaStreamWaitEvent(cs, ev_copied[b], 0);
     rc = chi0_slab(ctx, d_slab[b], len, len, nbas, d_e[b], wscale ? d_ws[b] : nullptr, scale_all,
-                   nw, d_om, precision, d_out, d_w, d_split, s_bytes, cs, &launches);
+                   nw, d_om, precision, d_out, d_w, d_split, s_bytes, cs, &launches,
+                   precision == SPX_SPLIT ? plan : nullptr);
     if (rc) return rc;
     cudaEventRecord(ev_free[b], cs);
   }

@@ -565,12 +565,13 @@ size_t pb_plan_bytes(int nq, const spx_q_desc* qd, const int* S, int nw, int nsl
   return per_slot * nslot + desc + ctr + 4096;
 }
 
-// Builds the schedule into `mem` (device, pb_plan_bytes large): descriptors are
-// copied there synchronously; the counters (the first `*ctr_bytes` bytes at
-// *ctr) must be zeroed before every launch.
+// Builds the schedule into `mem` (device, pb_plan_bytes large): the descriptors are
+// copied there in order on `s`, after whatever `s` already runs (a previous launch
+// on the same scratch still reads its own); the counters (the first `*ctr_bytes`
+// bytes at *ctr) must be zeroed before every launch.
 int pb_build(spx_ctx* ctx, int nq, const spx_q_desc* qd, const int* S, int nw, int nslot,
              PbConfig cfg, const double* omega, char* mem, size_t mem_bytes, PbParams* out,
-             void** ctr, size_t* ctr_bytes) {
+             void** ctr, size_t* ctr_bytes, cudaStream_t s) {
   (void)mem_bytes;
   // q order: most work first
   std::vector<int> order;
@@ -688,10 +689,12 @@ int pb_build(spx_ctx* ctx, int nq, const spx_q_desc* qd, const int* S, int nw, i
     }
   }
   int rc;
-  if ((rc = check_cuda(ctx, cudaMemcpy(dq, q.data(), sizeof(PbQ) * nq, cudaMemcpyHostToDevice), "plan copy")) ||
-      (rc = check_cuda(ctx, cudaMemcpy(dsl, slabs.data(), sizeof(PbSlab) * nslab, cudaMemcpyHostToDevice), "plan copy")) ||
-      (rc = check_cuda(ctx, cudaMemcpy(dslot, slot.data(), sizeof(PbSlot) * nslot, cudaMemcpyHostToDevice), "plan copy")) ||
-      (rc = check_cuda(ctx, cudaMemcpy(dmaps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice), "plan copy")))
+  // pageable sources: each copy is staged before the call returns, so the vectors may
+  // go; the transfer itself is ordered on `s`
+  if ((rc = check_cuda(ctx, cudaMemcpyAsync(dq, q.data(), sizeof(PbQ) * nq, cudaMemcpyHostToDevice, s), "plan copy")) ||
+      (rc = check_cuda(ctx, cudaMemcpyAsync(dsl, slabs.data(), sizeof(PbSlab) * nslab, cudaMemcpyHostToDevice, s), "plan copy")) ||
+      (rc = check_cuda(ctx, cudaMemcpyAsync(dslot, slot.data(), sizeof(PbSlot) * nslot, cudaMemcpyHostToDevice, s), "plan copy")) ||
+      (rc = check_cuda(ctx, cudaMemcpyAsync(dmaps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice, s), "plan copy")))
     return rc;
   PbParams& p = *out;
   std::memset(&p, 0, sizeof(p));
@@ -802,7 +805,7 @@ int pb_run(spx_ctx* ctx, int nq, const spx_q_desc* q, int nw, const double* omeg
       scratch_bytes = ctx->ws_bytes;
     }
     if ((rc = pb_build(ctx, nq, q, S.data(), nw, PB_NSLOT, cfg, omega, scratch, scratch_bytes,
-                       &prm, &ctr, &ctr_bytes)))
+                       &prm, &ctr, &ctr_bytes, s)))
       return rc;
     if ((rc = pb_launch(ctx, prm, cfg, ctr, ctr_bytes, s))) return rc;
     *launches = 1;
@@ -825,7 +828,10 @@ int pb_run(spx_ctx* ctx, int nq, const spx_q_desc* q, int nw, const double* omeg
       cudaGetLastError();
       return set_error(ctx, SPX_ENOMEM, "persistent batch: cannot allocate " + std::to_string(bytes) + " bytes");
     }
-    rc = pb_build(ctx, nq, q, S.data(), nw, PB_NSLOT, cfg, omega, (char*)mem, bytes, &prm, &ctr, &ctr_bytes);
+    rc = pb_build(ctx, nq, q, S.data(), nw, PB_NSLOT, cfg, omega, (char*)mem, bytes, &prm, &ctr, &ctr_bytes,
+                  ctx->stream);
+    // the graph may be launched on another stream: the plan must have landed first
+    if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "plan copy");
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     if (!rc) rc = check_cuda(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed), "begin capture");

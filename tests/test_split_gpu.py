@@ -134,9 +134,10 @@ def test_split_persistent_single_call_equals_slab_kernels(nbas, npair, nw):
 
 
 def test_split_host_ramp_equals_device_path(ctx):
-    """With default chunking, the host-pointer call streams chunks of 32768, 65536,
-    98304, ... pairs. They fall on the 32768-pair exact slabs of the split path, so
-    its result equals the device call's bit for bit (pinned source)."""
+    """With default chunking, the host-pointer call streams growing chunks whose
+    boundaries fall on the exact slabs (32768 pairs untuned) of the split path, and it
+    keeps one kernel for all chunks, so its result equals the device call's bit for
+    bit (pinned source)."""
     nbas, npair = 72, 150000
     m, d, om = random_case(nbas, npair, 2, seed=21, degfrac=0.01)
     dev = run_dev(ctx, m, d, om, None, 0.5, precision="split")
@@ -146,4 +147,26 @@ def test_split_host_ramp_equals_device_path(ctx):
         st = c.chi0_accumulate_host_ptr(t.data_ptr(), npair, npair, nbas, d, om, out,
                                         scale_all=0.5, precision="split")
     assert st["h2d_bytes"] >= m.nbytes
+    assert np.array_equal(out, dev)
+
+
+@pytest.mark.parametrize("variant,slab", [(5, 8192), (1, 16384), (3, 8192)])
+def test_split_host_ramp_equals_device_path_tuned(tmp_path, variant, slab):
+    """With a tuning entry (kernel and slab) for the array's shape, the host-pointer
+    call cuts its chunks on that slab and runs that kernel for every chunk, so it
+    still equals the device call bit for bit."""
+    import json
+    nbas, npair, nw = 72, 150000, 2
+    m, d, om = random_case(nbas, npair, nw, seed=22, degfrac=0.01)
+    table = tmp_path / "tune.json"
+    table.write_text(json.dumps({"format": "spexgpu-tune-1", "entries": [
+        {"nbas_bucket": 1, "npair_bucket": 2, "nw": nw, "variant": variant, "slab_pairs": slab,
+         "tile": 64 + 3 * 256 if variant == 3 else 0, "tflops": 1.0}]}))
+    with spx.Context(0) as c:
+        c.tune_load(str(table))
+        dev = run_dev(c, m, d, om, None, 0.5, precision="split")
+        t = torch.from_numpy(np.ascontiguousarray(m.T)).pin_memory()
+        out = np.zeros((nbas * (nbas + 1) // 2, nw), complex, order="F")
+        c.chi0_accumulate_host_ptr(t.data_ptr(), npair, npair, nbas, d, om, out,
+                                   scale_all=0.5, precision="split")
     assert np.array_equal(out, dev)
