@@ -448,6 +448,7 @@ def run_ours(args):
                                                scale_all=1.0 / w.nk, precision=head)
             if it >= 1:
                 h2d, d2h = st["h2d_bytes"], st["d2h_bytes"]
+                e2e_dev = (st["ms_gram"], st["ms_prep"])
         dt = (time.perf_counter() - t0) / args.e2e_steps
         if world > 1:
             t = torch.tensor([dt], device=dev, dtype=torch.float64)
@@ -472,6 +473,9 @@ def run_ours(args):
         h2d_gbs = 16.0 * nbw / (c0.elapsed_time(c1) * 1e-3) / 1e9
         del dst
         e2e["h2d_link_gbs"] = h2d_gbs
+        # device time inside the call (accumulation kernels; preparation the compute
+        # stream waited for), the rest waits for the host copies
+        e2e["accumulation_ms"], e2e["preparation_ms"] = e2e_dev
         e2e["copy_bound_ms"] = (h2d + d2h) / (h2d_gbs * 1e9) * 1e3
         e2e["roofline"] = {"bound": "host link (PCIe)", "achieved_gbs": (h2d + d2h) / dt / 1e9,
                            "peak_gbs": h2d_gbs, "frac": (h2d + d2h) / dt / 1e9 / h2d_gbs,

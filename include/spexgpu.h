@@ -406,7 +406,7 @@ typedef struct spx_tune_entry {
   double  tflops;           /* measured throughput of the chosen configuration        */
 } spx_tune_entry;
 
-/* Measures the candidates on a seeded probe of (nbas, min(npair, 65536), nw),
+/* Measures the candidates on a seeded probe of (nbas, min(npair, 131072), nw),
  * stores the best in the table and returns it in *out (may be NULL). */
 int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
                        spx_tune_entry* out);

@@ -547,12 +547,12 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
   if (precision == SPX_SPLIT) split_choice(ctx, nbas, npair, nw, &plan[0], &plan[1], &plan[2]);
   const int64_t align = precision == SPX_SPLIT ? (plan[1] > 0 ? plan[1] : 32768) : 16384;
   // slab size: band pairs per streamed chunk
-  // By default the first chunk is short, since its copy overlaps nothing, and the
-  // chunks then grow by an eighth each time, up to 262144 pairs: a chunk's copy
-  // (about 0.35 us per pair at N = 1200 over PCIe 5) must stay within the previous
-  // chunk's accumulation (about 0.39 us per pair), and each chunk exposes one
-  // operand preparation. Pageable arrays keep 65536-pair chunks so that their
-  // pinned staging stays small.
+  // By default the first chunk is short, since its copy overlaps nothing; the
+  // chunks then grow by an eighth each time, up to 262144 pairs (a chunk's copy, about
+  // 0.35-0.4 us per pair at N = 1200 over PCIe 5, against about 0.32-0.38 us of
+  // accumulation), and halve again over the last quarter or so, so that little
+  // accumulation is left once the last copy has landed. Pageable arrays keep
+  // 65536-pair chunks so that their pinned staging stays small.
   const bool ramp = ctx->opt.chunk_pairs <= 0;
   int64_t slab = ctx->opt.chunk_pairs > 0 ? ctx->opt.chunk_pairs : (pinned ? 262144 : 65536);
   slab = std::min<int64_t>(slab, npair);
@@ -588,21 +588,17 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
   base += w_bytes;
   void* d_split = s_bytes ? (void*)base : nullptr;
 
-  double* stage = nullptr;
-  if (!pinned) {
-    if ((rc = ensure_pinned(ctx, 2 * slab_bytes))) return rc;
-    stage = (double*)ctx->pinned;
-  }
+  const size_t out_host_bytes = sizeof(double) * 2 * (size_t)npack * nw;
+  // pinned staging: the pageable slabs' gather, then the sums on their way back
+  if ((rc = ensure_pinned(ctx, std::max(pinned ? (size_t)0 : 2 * slab_bytes, out_host_bytes)))) return rc;
+  double* stage = pinned ? nullptr : (double*)ctx->pinned;
   cudaStream_t cs = ctx->stream, xs = ctx->copy_stream;
   int64_t h2d = 0, d2h = 0;
   int launches = 0;
-  const size_t out_host_bytes = sizeof(double) * 2 * (size_t)npack * nw;
-  // the output accumulates: bring the caller's values to the device once
-  if ((rc = check_cuda(ctx, cudaMemcpyAsync(d_out, susceph, out_host_bytes,
-                                            cudaMemcpyHostToDevice, cs),
-                       "copy susceph")))
+  // The device sums this call's contribution from zero; the host adds it to the
+  // caller's susceph at the end (no upload of the output, a pinned download).
+  if ((rc = check_cuda(ctx, cudaMemsetAsync(d_out, 0, out_host_bytes, cs), "zero output")))
     return rc;
-  h2d += out_host_bytes;
   if ((rc = check_cuda(ctx, cudaMemcpyAsync(d_om, omega, sizeof(double) * nw,
                                             cudaMemcpyHostToDevice, cs),
                        "copy omega")))
@@ -612,16 +608,25 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
   cudaEvent_t ev_free[2] = {ctx->ev[4], ctx->ev[5]};
   cudaEventRecord(ev_free[0], cs);
   cudaEventRecord(ev_free[1], cs);
+  // device time of the accumulation and preparation (marks on the compute stream); the
+  // rest of the call waits for the host copies
+  ctx->timing = stats != nullptr;
+  ctx->nmarks = 0;
   const int nthr = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
   int64_t k = 0;
   int64_t len = 0;
   for (int64_t p0 = 0; p0 < npair; p0 += len, ++k) {
     const int b = (int)(k & 1);
-    const int64_t want =
+    int64_t want =
         k == 0 ? first
                : (ramp ? std::min<int64_t>(slab, (int64_t)align_up((size_t)(len + len / 8), (size_t)align))
                        : slab);
-    len = std::min<int64_t>(want, npair - p0);
+    // near the end the chunks halve: the accumulation left after the last copy lands
+    // is that of a short chunk (the copies are the slower stream over PCIe)
+    const int64_t left = npair - p0;
+    if (ramp && k > 0 && left <= 2 * want)
+      want = std::max<int64_t>(align, (int64_t)align_up((size_t)((left + 1) / 2), (size_t)align));
+    len = std::min<int64_t>(want, left);
     cudaStreamWaitEvent(xs, ev_free[b], 0);
     const size_t bytes = sizeof(double) * 2 * (size_t)len;
     if (pinned) {
@@ -636,7 +641,10 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
       rc = check_cuda(ctx, cudaMemcpyAsync(d_slab[b], st, bytes * nbas, cudaMemcpyHostToDevice, xs),
                       "copy cprod slab");
     }
-    if (rc) return rc;
+    if (rc) {
+      ctx->timing = false;
+      return rc;
+    }
     h2d += (int64_t)bytes * nbas;
     cudaMemcpyAsync(d_e[b], ediff + p0, sizeof(double) * len, cudaMemcpyHostToDevice, xs);
     h2d += sizeof(double) * len;
@@ -649,17 +657,34 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
     rc = chi0_slab(ctx, d_slab[b], len, len, nbas, d_e[b], wscale ? d_ws[b] : nullptr, scale_all,
                    nw, d_om, precision, d_out, d_w, d_split, s_bytes, cs, &launches,
                    precision == SPX_SPLIT ? plan : nullptr);
-    if (rc) return rc;
+    if (rc) {
+      ctx->timing = false;
+      return rc;
+    }
     cudaEventRecord(ev_free[b], cs);
   }
-  if ((rc = check_cuda(ctx, cudaMemcpyAsync(susceph, d_out, out_host_bytes,
-                                            cudaMemcpyDeviceToHost, cs),
-                       "copy susceph back")))
+  ctx->timing = false;
+  double* sums = (double*)ctx->pinned;
+  if ((rc = check_cuda(ctx, cudaMemcpyAsync(sums, d_out, out_host_bytes, cudaMemcpyDeviceToHost, cs),
+                       "copy the sums back")))
     return rc;
   d2h += out_host_bytes;
   rc = collect_status(ctx, cs, "chi0_accumulate");
   if (rc) return rc;
+  {
+    // susceph += sums, on the host threads
+    const int64_t n = 2 * npack * nw;
+    auto add = [&](int t) {
+      const int64_t a = n * t / nthr, e = n * (t + 1) / nthr;
+      for (int64_t i = a; i < e; ++i) susceph[i] += sums[i];
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nthr; ++t) th.emplace_back(add, t);
+    add(0);
+    for (auto& x : th) x.join();
+  }
   if (stats) {
+    timing_collect(ctx, &stats->ms_prep, &stats->ms_gram);
     stats->h2d_bytes = h2d;
     stats->d2h_bytes = d2h;
     stats->kernel_launches = launches;

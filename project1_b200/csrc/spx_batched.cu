@@ -337,7 +337,9 @@ extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int
   if (nbas <= 0 || npair <= 0 || nw <= 0) return set_error(ctx, SPX_EINVAL, "empty probe");
   if (nbas > 46340) return set_error(ctx, SPX_EINVAL, "nbas too large");
   cudaSetDevice(ctx->device);
-  const int64_t P = std::min<int64_t>(npair, 2 * (int64_t)kDefaultSlab);
+  // a probe of up to 131072 pairs: 16 slabs of 8192, long enough that the choice
+  // between close candidates is not decided by noise
+  const int64_t P = std::min<int64_t>(npair, 4 * (int64_t)kDefaultSlab);
   const int64_t ld = (int64_t)align_up((size_t)P, 16);
   const int64_t npack = (int64_t)nbas * (nbas + 1) / 2;
   // smaller slabs cost more epilogues but keep a round's operand blocks in L2
