@@ -401,21 +401,22 @@ typedef struct spx_tune_entry {
                                3 the persistent schedule, 5 one CTA per 64 x 80 tile;
                                4 an entry of the batched table                        */
   int32_t slab_pairs;
-  int32_t tile;             /* variants 3 and 4: tile columns (64 or 32) + 256 *
-                               pipeline stages (3 or 4); 0 otherwise                  */
+  int32_t tile;             /* variants 3 and 4: tile columns (64, 32 or 80) + 256 *
+                               pipeline stages (2 to 4); 0 otherwise                  */
   double  tflops;           /* measured throughput of the chosen configuration        */
 } spx_tune_entry;
 
-/* Measures the candidates on a seeded probe of (nbas, min(npair, 131072), nw),
+/* Measures the candidates on a seeded probe of (nbas, min(npair, 262144), nw),
  * stores the best in the table and returns it in *out (may be NULL). */
 int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
                        spx_tune_entry* out);
 /* SPX_OK and *out if the bucket of (nbas, npair, nw) is in the table, else SPX_ENOTSUP. */
 int spx_tune_lookup(const spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
                     spx_tune_entry* out);
-/* The same for the persistent batched schedule: measures its tile shapes (64 or 32
- * complex columns per tile, 3 or 4 pipeline stages) and slab sizes on a seeded
- * probe of one q, stores the fastest (variant 4), and looks entries up. */
+/* The same for the persistent batched schedule: measures its tile shapes (64 x 64
+ * complex with 3 pipeline stages, 64 x 32 with 3 or 4, 64 x 80 with 2) and slab
+ * sizes on a seeded probe of one q, stores the fastest (variant 4), and looks
+ * entries up. */
 int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
                          spx_tune_entry* out);
 int spx_tune_lookup_batched(const spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,

@@ -558,7 +558,7 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
   slab = std::min<int64_t>(slab, npair);
   slab = (int64_t)align_up((size_t)slab, 16);
   const int64_t first = ramp ? std::min<int64_t>(slab, (int64_t)align_up(16384, (size_t)align)) : slab;
-  const int nslab_buf = 2;
+  const int nslab_buf = 3;  // chunk k's copy waits only for chunk k-3's accumulation
   const int64_t npack = (int64_t)nbas * (nbas + 1) / 2;
   const size_t out_bytes = align_up(sizeof(double) * 2 * (size_t)npack * nw, 256);
   const size_t slab_bytes = align_up(sizeof(double) * 2 * (size_t)slab * nbas, 256);
@@ -571,10 +571,10 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
   char* base = (char*)ctx->ws;
   double2* d_out = (double2*)base;
   base += out_bytes;
-  double2* d_slab[2];
-  double* d_e[2];
-  double* d_ws[2];
-  for (int b = 0; b < 2; ++b) {
+  double2* d_slab[nslab_buf];
+  double* d_e[nslab_buf];
+  double* d_ws[nslab_buf];
+  for (int b = 0; b < nslab_buf; ++b) {
     d_slab[b] = (double2*)base;
     base += slab_bytes;
     d_e[b] = (double*)base;
@@ -590,7 +590,7 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
 
   const size_t out_host_bytes = sizeof(double) * 2 * (size_t)npack * nw;
   // pinned staging: the pageable slabs' gather, then the sums on their way back
-  if ((rc = ensure_pinned(ctx, std::max(pinned ? (size_t)0 : 2 * slab_bytes, out_host_bytes)))) return rc;
+  if ((rc = ensure_pinned(ctx, std::max(pinned ? (size_t)0 : nslab_buf * slab_bytes, out_host_bytes)))) return rc;
   double* stage = pinned ? nullptr : (double*)ctx->pinned;
   cudaStream_t cs = ctx->stream, xs = ctx->copy_stream;
   int64_t h2d = 0, d2h = 0;
@@ -604,10 +604,9 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
                        "copy omega")))
     return rc;
   h2d += sizeof(double) * nw;
-  cudaEvent_t ev_copied[2] = {ctx->ev[2], ctx->ev[3]};
-  cudaEvent_t ev_free[2] = {ctx->ev[4], ctx->ev[5]};
-  cudaEventRecord(ev_free[0], cs);
-  cudaEventRecord(ev_free[1], cs);
+  cudaEvent_t ev_copied[nslab_buf] = {ctx->ev[2], ctx->ev[3], ctx->ev[4]};
+  cudaEvent_t ev_free[nslab_buf] = {ctx->ev[5], ctx->ev[6], ctx->ev[7]};
+  for (int b = 0; b < nslab_buf; ++b) cudaEventRecord(ev_free[b], cs);
   // device time of the accumulation and preparation (marks on the compute stream); the
   // rest of the call waits for the host copies
   ctx->timing = stats != nullptr;
@@ -616,7 +615,7 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
   int64_t k = 0;
   int64_t len = 0;
   for (int64_t p0 = 0; p0 < npair; p0 += len, ++k) {
-    const int b = (int)(k & 1);
+    const int b = (int)(k % nslab_buf);
     int64_t want =
         k == 0 ? first
                : (ramp ? std::min<int64_t>(slab, (int64_t)align_up((size_t)(len + len / 8), (size_t)align))
@@ -634,7 +633,7 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
                                              bytes, nbas, cudaMemcpyHostToDevice, xs),
                       "copy cprod slab");
     } else {
-      // the staging half `b` is free once the previous copy out of it finished
+      // the staging part `b` is free once the previous copy out of it finished
       cudaEventSynchronize(ev_free[b]);
       double* st = stage + (size_t)b * (slab_bytes / sizeof(double));
       gather_slab(cprod, ldc, p0, len, nbas, st, nthr);

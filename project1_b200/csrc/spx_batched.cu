@@ -211,7 +211,7 @@ extern "C" int spx_chi0_batched(spx_ctx* ctx, int32_t nq, const spx_q_desc* q, i
           return rc;
       }
     cudaStream_t s = pick_stream(ctx, stream);
-    cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+    cudaEvent_t e0 = ctx->ev[8], e1 = ctx->ev[9];
     if (stats) cudaEventRecord(e0, s);
     int launches = 0;
     if ((rc = pb_run(ctx, nq, q, nw, omega, flags, s, &launches, nullptr, 0, nullptr, 0))) return rc;
@@ -243,7 +243,7 @@ extern "C" int spx_chi0_batched(spx_ctx* ctx, int32_t nq, const spx_q_desc* q, i
   if ((rc = ensure_workspace(ctx, need + 1024))) return rc;
   cudaStream_t s = pick_stream(ctx, stream);
   int launches = 0;
-  cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+  cudaEvent_t e0 = ctx->ev[8], e1 = ctx->ev[9];
   if (stats) cudaEventRecord(e0, s);
   const bool timing = ctx->timing;
   ctx->timing = false;
@@ -337,9 +337,9 @@ extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int
   if (nbas <= 0 || npair <= 0 || nw <= 0) return set_error(ctx, SPX_EINVAL, "empty probe");
   if (nbas > 46340) return set_error(ctx, SPX_EINVAL, "nbas too large");
   cudaSetDevice(ctx->device);
-  // a probe of up to 131072 pairs: 16 slabs of 8192, long enough that the choice
+  // a probe of up to 262144 pairs (32 slabs of 8192), long enough that the choice
   // between close candidates is not decided by noise
-  const int64_t P = std::min<int64_t>(npair, 4 * (int64_t)kDefaultSlab);
+  const int64_t P = std::min<int64_t>(npair, 8 * (int64_t)kDefaultSlab);
   const int64_t ld = (int64_t)align_up((size_t)P, 16);
   const int64_t npack = (int64_t)nbas * (nbas + 1) / 2;
   // smaller slabs cost more epilogues but keep a round's operand blocks in L2
@@ -382,7 +382,7 @@ extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int
   best.nw = nw;
   best.tflops = -1;
   const double flops = 8.0 * (double)nbas * nbas * (double)P * nw;
-  cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+  cudaEvent_t e0 = ctx->ev[8], e1 = ctx->ev[9];
   // Candidates: variants 1, 5 and 2 (the slab kernels with the quantizer beside them:
   // one CTA per 64 x 64 tile, one CTA per 64 x 80 tile, the CTA pair) and 3 (the
   // persistent schedule with its own preparation warps, 64 x 64 tiles, 3 stages), at
@@ -398,21 +398,27 @@ extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int
       if (sl == 32768 && npair <= 16384) continue;  // one slab either way
       cands.push_back({variant, sl, 1e30f});
     }
+  // Each measurement runs the probe kPasses times back to back: a window of a few
+  // hundred milliseconds, so that the power-capped clock settles to the candidate's
+  // own level (a faster kernel draws more power and runs at a lower clock).
+  constexpr int kPasses = 3;
   for (int round = 0; round < 3; ++round)  // round 0 warms up
     for (auto& c : cands) {
       int launches = 0;
       cudaEventRecord(e0, s);
-      if (c.variant == 3)
-        rc = pb_single(ctx, M, ld, P, nbas, E, nullptr, 1.0, nw, OM, O, 64 + 3 * 256, c.slab, (char*)S,
-                       sws, s, &launches);
-      else
-        rc = split_chi0_slab(ctx, M, ld, P, nbas, W, ld, nw, O, S, sws, s, &launches, c.variant, c.slab);
+      for (int pass = 0; pass < kPasses && !rc; ++pass) {
+        if (c.variant == 3)
+          rc = pb_single(ctx, M, ld, P, nbas, E, nullptr, 1.0, nw, OM, O, 64 + 3 * 256, c.slab, (char*)S,
+                         sws, s, &launches);
+        else
+          rc = split_chi0_slab(ctx, M, ld, P, nbas, W, ld, nw, O, S, sws, s, &launches, c.variant, c.slab);
+      }
       if (rc) return rc;
       cudaEventRecord(e1, s);
       if ((rc = collect_status(ctx, s, "autotune"))) return rc;
       float ms = 0;
       cudaEventElapsedTime(&ms, e0, e1);
-      if (round) c.ms = std::min(c.ms, ms);
+      if (round) c.ms = std::min(c.ms, ms / kPasses);
     }
   for (const auto& c : cands) {
     const double tf = flops / (c.ms * 1e-3) / 1e12;

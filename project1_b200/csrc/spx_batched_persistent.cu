@@ -529,6 +529,7 @@ struct PbConfig {
 
 static size_t pb_smem(PbConfig c) {
   if (c.bn == 64) return sizeof(PbSmem<64, 3>) + 1024;
+  if (c.bn == 80) return sizeof(PbSmem<80, 2>) + 1024;
   return c.stages == 4 ? sizeof(PbSmem<32, 4>) + 1024 : sizeof(PbSmem<32, 3>) + 1024;
 }
 
@@ -555,7 +556,7 @@ size_t pb_plan_bytes(int nq, const spx_q_desc* qd, const int* S, int nw, int nsl
                align_up(sizeof(double) * (size_t)R, 256) + 2 * align_up(sizeof(double) * (size_t)nw, 256) +
                (qd[i].cprod ? 0 : align_up(sizeof(double2) * (size_t)N * S[i], 256));
     per_slot = std::max(per_slot, b);
-    seq += (size_t)pb_ntile<32>(N) * nw;   // the larger of the two tilings
+    seq += (size_t)pb_ntile<32>(N) * nw;   // the largest of the tilings (32, 64, 80 columns)
     nslab += (qd[i].npair + S[i] - 1) / S[i];
   }
   const size_t desc = align_up(sizeof(PbQ) * nq, 256) + align_up(sizeof(PbSlab) * nslab, 256) +
@@ -594,7 +595,7 @@ int pb_build(spx_ctx* ctx, int nq, const spx_q_desc* qd, const int* S, int nw, i
     x.P = d.npair;
     if (x.N <= 0 || x.P <= 0) continue;
     x.nblk = (x.N + 63) / 64;
-    x.ntile = cfg.bn == 64 ? pb_ntile<64>(x.N) : pb_ntile<32>(x.N);
+    x.ntile = cfg.bn == 64 ? pb_ntile<64>(x.N) : (cfg.bn == 80 ? pb_ntile<80>(x.N) : pb_ntile<32>(x.N));
     x.R = (int64_t)((x.nblk + 1) / 2 * 2) * SP_ROWS;
     x.npad = (int)(x.R / 2);
     x.S = S[i];
@@ -727,6 +728,10 @@ int pb_launch(spx_ctx* ctx, const PbParams& prm, PbConfig cfg, void* ctr, size_t
   if (cfg.bn == 64) {
     cudaFuncSetAttribute(pb_kernel<64, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     pb_kernel<64, 3><<<grid, PB_THREADS, smem, s>>>(prm);
+  } else if (cfg.bn == 80) {
+    // 64 x 80 tiles (N = 160 MMAs): two stages fit beside the epilogue's staging
+    cudaFuncSetAttribute(pb_kernel<80, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    pb_kernel<80, 2><<<grid, PB_THREADS, smem, s>>>(prm);
   } else if (cfg.stages == 4) {
     cudaFuncSetAttribute(pb_kernel<32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     pb_kernel<32, 4><<<grid, PB_THREADS, smem, s>>>(prm);
@@ -756,6 +761,7 @@ static const spx_tune_entry* pb_find_tune(const spx_ctx* ctx, int N, int64_t P, 
 static PbConfig pb_cfg_of(int tile) {
   const int bn = tile & 255, st = tile >> 8;
   if (bn == 32 && (st == 3 || st == 4)) return {32, st};
+  if (bn == 80 && st == 2) return {80, 2};
   return PB_DEFAULT_CFG;
 }
 
@@ -919,7 +925,7 @@ extern "C" int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, i
   if (nbas > 46340) return set_error(ctx, SPX_EINVAL, "nbas too large");
   cudaSetDevice(ctx->device);
   const int slabs[3] = {8192, 16384, 32768};
-  const PbConfig cfgs[3] = {{64, 3}, {32, 3}, {32, 4}};
+  const PbConfig cfgs[4] = {{64, 3}, {32, 3}, {32, 4}, {80, 2}};
   const int64_t P = std::min<int64_t>(npair, 4 * (int64_t)SP_SLAB);
   const int64_t npack = (int64_t)nbas * (nbas + 1) / 2;
   // probe arrays in a private allocation (the schedule itself uses the workspace)
@@ -958,7 +964,7 @@ extern "C" int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, i
   d.scale_all = 1.0;
   d.susceph = O;
   const double flops = 8.0 * (double)nbas * nbas * (double)P * nw;
-  cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+  cudaEvent_t e0 = ctx->ev[8], e1 = ctx->ev[9];
   // rounds interleave the candidates (tile shape x slab) so that clock drift under the
   // power cap favours none of them; round 0 warms up, each keeps its best round
   struct Cand {
@@ -966,7 +972,7 @@ extern "C" int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, i
     float ms;
   };
   std::vector<Cand> cands;
-  for (int ci = 0; ci < 3; ++ci)
+  for (int ci = 0; ci < 4; ++ci)
     for (int sl : slabs) {
       if (sl == 32768 && P <= 16384) continue;
       cands.push_back({ci, sl, 1e30f});

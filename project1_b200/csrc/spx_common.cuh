@@ -28,7 +28,7 @@ struct spx_ctx {
   // pinned host staging for pageable host arrays
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
-  cudaEvent_t ev[8] = {};
+  cudaEvent_t ev[12] = {};          // 2-7: host-path chunk copies / frees (3 buffers), 8-9: tuners
   // optional per-kernel timing: marks recorded on the stream, summed after a sync
   bool timing = false;
   std::vector<cudaEvent_t> mark_pool;
