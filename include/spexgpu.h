@@ -414,7 +414,7 @@ int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
 int spx_tune_lookup(const spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
                     spx_tune_entry* out);
 /* The same for the persistent batched schedule: measures its tile shapes (64 x 64
- * complex with 3 pipeline stages, 64 x 32 with 3 or 4, 64 x 80 with 2) and slab
+ * complex with 3 pipeline stages, 64 x 32 with 3 or 4, 64 x 80 with 3) and slab
  * sizes on a seeded probe of one q, stores the fastest (variant 4), and looks
  * entries up. */
 int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,

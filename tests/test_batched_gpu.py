@@ -155,7 +155,7 @@ def test_autotuned_batch(ctx):
     for q in qs:
         t = ctx.tune_lookup_batched(q["nbas"], q["npair"], 2)
         assert t is not None and t["variant"] == 4 and t["tile"] in (64 + 3 * 256, 32 + 3 * 256, 32 + 4 * 256,
-                                                                      80 + 2 * 256)
+                                                                      80 + 3 * 256)
         assert torch.isfinite(torch.view_as_real(q["susceph"])).all()
         assert q["susceph"].abs().max() > 0
 
@@ -183,7 +183,7 @@ def _force_tile(c, tmp_path, qs, nw, tile, slab):
     c.tune_load(path)
 
 
-@pytest.mark.parametrize("tile", [64 + 3 * 256, 32 + 3 * 256, 32 + 4 * 256, 80 + 2 * 256])
+@pytest.mark.parametrize("tile", [64 + 3 * 256, 32 + 3 * 256, 32 + 4 * 256, 80 + 3 * 256])
 def test_persistent_tile_shapes_equal_per_q_calls(tmp_path, tile):
     """Every tile shape of the persistent schedule gives the per-q result bit for bit,
     with the slab ring reused many times (4096-pair slabs, 3 buffers) and a q whose
