@@ -514,7 +514,7 @@ def run_ours(args):
         tr = measured_traffic(kname, N, nw, slab, Pr, upper_tiles(N, variant))
         if tr:
             nblk = (N + 63) // 64
-            R = (nblk + 1) // 2 * 2 * 128
+            R = ((nblk + 1) // 2 * 2 if variant == 2 else nblk) * 128   # plane rows (the pair needs even blocks)
             roof["traffic"] = tr["bytes_per_launch"]
             roof["traffic_detail"] = dict(tr, kernel=kname, unit="bytes per launch (one slab, all frequencies)",
                                           operand_plane_bytes_per_launch=3.0 * nw * R * min(slab, Pr))

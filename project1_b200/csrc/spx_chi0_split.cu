@@ -871,6 +871,9 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
   if (variant == 0) variant = ctx->opt.split_variant;
   const bool pair = variant != 1 && variant != 5;  // 0 (auto) and 2 select the CTA pair
   const bool wide = variant == 5;                  // one CTA per 64 x 80 tile (N = 160)
+  // only the CTA pair needs an even number of 64-column blocks in the planes (the
+  // buffers are sized for it either way)
+  if (!pair) L.R = (int64_t)L.nblk * SP_ROWS;
   CUtensorMap mapF[2], mapFh[2], mapW[2];
   for (int b = 0; b < nbuf; ++b) {
     const uint64_t st[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};
