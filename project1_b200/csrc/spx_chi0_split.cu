@@ -119,10 +119,10 @@ __device__ __forceinline__ void fold_epilogue(uint32_t tl, int q, int lane, int 
   }
 }
 
-// The -DINV (real) epilogue: columns [j0, j0 + ncol) of a 128 x 128 tile of real chi,
+// The -DINV (real) epilogue: columns [j0, j0 + ncol) of a 128 x BROWS tile of real chi,
 // TMEM lane = row i of the block, column = j; read and added 16 columns at a time,
 // then the accumulator is released.
-template <class Release>
+template <int BROWS, class Release>
 __device__ __forceinline__ void real_epilogue(uint32_t tl, int q, int lane, int bi, int bj, int f,
                                               const SplitParams& prm, Release release, int j0,
                                               int ncol) {
@@ -132,10 +132,10 @@ __device__ __forceinline__ void real_epilogue(uint32_t tl, int q, int lane, int 
 #pragma unroll 1
   for (int cc = 0; cc < ncol / 16; ++cc) {
     double T[16];
-    load_fold16(tl + (uint32_t)(j0 + 16 * cc), 128u, T);
+    load_fold16(tl + (uint32_t)(j0 + 16 * cc), (uint32_t)BROWS, T);
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-      const int gj = bj * SP_ROWS + j0 + 16 * cc + k;
+      const int gj = bj * BROWS + j0 + 16 * cc + k;
       if (gi < prm.N && gi <= gj && gj < prm.N)
         atomicAdd(of + (int64_t)gj * (gj + 1) / 2, fac * prm.sA[gj] * T[k]);
     }
@@ -151,7 +151,8 @@ __global__ void __maxnreg__(SP1_REGS)
                       SplitParams prm) {
   constexpr int BROWS = 2 * BN;
   constexpr uint32_t IDESC = sp_idesc(BROWS);
-  static_assert(!REAL || BN == SP_TILE, "the -DINV form uses square tiles");
+  // the -DINV form: tiles of 128 real rows x BROWS real columns (the same block
+  // arithmetic as 64 x BN complex tiles)
   using Smem = SplitSmemT<BROWS>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(
@@ -281,7 +282,7 @@ __global__ void __maxnreg__(SP1_REGS)
         if (lane == 0) mbar_arrive(&sm.tempty);
       };
       constexpr int NC = BN * 4 / SP1_EPI;  // complex columns per epilogue warp
-      if constexpr (REAL) real_epilogue(tl, q, lane, bi, bj, f, prm, release, 2 * NC * h, 2 * NC);
+      if constexpr (REAL) real_epilogue<BROWS>(tl, q, lane, bi, bj, f, prm, release, 2 * NC * h, 2 * NC);
       else fold_epilogue<NC, BN>(tl, q, lane, bi, bj, f, prm, release, NC * h);
     }
   }
@@ -1032,7 +1033,8 @@ size_t split_workspace_bytes_real(int64_t P, int N, int nw) {
 
 // The -DINV accumulation (src/susceptibility.f:1197, re(k) = cprod(k,i) * cprod(k,j)):
 // real M (ldc, N), real packed out (npack, nw), the folded 6-product int8 contraction
-// on 128 x 128 real tiles, one CTA per tile.
+// on 128 x 160 real tiles (N = 160 MMAs; 128 x 128 when the context's split variant is
+// 1), one CTA per tile.
 int split_chi0_real_slab(spx_ctx* ctx, const double* M, int64_t ldc, int64_t P, int N,
                          const double* W, int64_t ldw, int nw, double* out, void* ws,
                          size_t ws_bytes, cudaStream_t stream, int* launches) {
@@ -1055,17 +1057,27 @@ int split_chi0_real_slab(spx_ctx* ctx, const double* M, int64_t ldc, int64_t P, 
     wsgn[b] = (int*)(s0 + L.f_bytes + L.g_bytes + L.s_bytes + L.w_bytes);
   }
   const uint64_t nkb = (uint64_t)(L.Ps / SP_KB);
-  CUtensorMap mapF[2];
+  const bool wide = ctx->opt.split_variant != 1;
+  CUtensorMap mapF[2], mapW[2];
   for (int b = 0; b < nbuf; ++b) {
     const uint64_t st[3] = {SP_KB, (uint64_t)L.R * SP_KB, nkb * L.R * SP_KB};
     const uint64_t d[4] = {SP_KB, (uint64_t)L.R, nkb, (uint64_t)SP_SLOT * nw};
     const uint32_t bx[4] = {SP_KB, SP_ROWS, 1, SP_SF};
     int rc0 = make_tmap_u8_4d(ctx, &mapF[b], F[b], d, st, bx, CU_TENSOR_MAP_SWIZZLE_64B);
     if (rc0) return rc0;
+    const uint32_t bw[4] = {SP_KB, 2 * SP_WIDE_BN, 1, SP_SF};
+    rc0 = make_tmap_u8_4d(ctx, &mapW[b], F[b], d, st, bw, CU_TENSOR_MAP_SWIZZLE_64B);
+    if (rc0) return rc0;
   }
   const size_t smem = sizeof(SplitSmem) + 1024;
+  const size_t smemw = sizeof(SplitSmemT<2 * SP_WIDE_BN>) + 1024;
   cudaFuncSetAttribute(split_gram_kernel<true, SP_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const int ntile = L.nblk * (L.nblk + 1) / 2;
+  cudaFuncSetAttribute(split_gram_kernel<true, SP_WIDE_BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemw);
+  // tiles in 128-row blocks of the real rows; wide tiles in 160-column blocks
+  const int nbr = L.nblk;
+  int ntilew = 0;
+  for (int bj = 0; bj * 2 * SP_WIDE_BN < N; ++bj) ntilew += split_rows_of(bj, SP_WIDE_BN, nbr);
+  const int ntile = wide ? ntilew : L.nblk * (L.nblk + 1) / 2;
   const int nitems = ntile * nw;
   const int grid = std::min(nitems, ctx->num_sms);
   const int npad = (int)L.R;
@@ -1107,7 +1119,7 @@ int split_chi0_real_slab(spx_ctx* ctx, const double* M, int64_t ldc, int64_t P, 
     timing_mark(ctx, stream, 1);
     SplitParams prm;
     prm.N = N;
-    prm.nbr = (N + SP_ROWS - 1) / SP_ROWS;
+    prm.nbr = nbr;
     prm.ntile = ntile;
     prm.nw = nw;
     prm.nitems = nitems;
@@ -1119,7 +1131,10 @@ int split_chi0_real_slab(spx_ctx* ctx, const double* M, int64_t ldc, int64_t P, 
     prm.npack = (int64_t)N * (N + 1) / 2;
     prm.status = ctx->d_status;
     prm.timeout_ns = (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
-    split_gram_kernel<true, SP_TILE><<<grid, SP1_THREADS, smem, stream>>>(mapF[b], mapF[b], prm);
+    if (wide)
+      split_gram_kernel<true, SP_WIDE_BN><<<grid, SP1_THREADS, smemw, stream>>>(mapF[b], mapW[b], prm);
+    else
+      split_gram_kernel<true, SP_TILE><<<grid, SP1_THREADS, smem, stream>>>(mapF[b], mapF[b], prm);
     if ((rc = check_cuda(ctx, cudaGetLastError(), "split_gram_kernel (real) launch"))) return rc;
     *launches += 1;
     timing_mark(ctx, stream, 2);

@@ -214,3 +214,23 @@ def test_real_variant_matches_oracle(precision, tol, nbas, npair, nw, ldpad):
     idx = ju * (ju + 1) // 2 + iu
     err = np.abs(got[idx] - ref[idx]) / np.sqrt(dg[iu] * dg[ju])
     assert err.max() <= tol, err.max()
+
+
+@pytest.mark.parametrize("nbas,npair", [(300, 9000), (161, 5000), (1200, 700)])
+def test_real_wide_tiles_equal_square_tiles(nbas, npair):
+    """The -DINV split path on 128 x 160 real tiles (N = 160 MMAs, the default) and on
+    128 x 128 tiles (split variant 1) sums the same exact integers per element and
+    slab: identical results, ragged column blocks included."""
+    rng = np.random.default_rng(nbas * 7 + npair)
+    m = rng.standard_normal((npair, nbas)) / np.sqrt(nbas)
+    d = rng.uniform(0.5, 40.0, npair)
+    om = inputs.frequencies(2)
+    cp = torch.from_numpy(np.ascontiguousarray(m.T)).to(DEV)
+    outs = []
+    for variant in (0, 1):
+        out = torch.zeros((2, nbas * (nbas + 1) // 2), dtype=torch.float64, device=DEV)
+        with spx.Context(0, split_variant=variant) as c:
+            c.chi0_accumulate_real_dev(cp, torch.from_numpy(d).to(DEV), torch.from_numpy(om).to(DEV), out,
+                                       scale_all=0.5, precision="split", npair=npair)
+        outs.append(out.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
