@@ -652,6 +652,8 @@ def bench_products(args, dev, stream):
     out = torch.zeros((w.nw, spx.npack(w.nbas)), dtype=torch.complex128, device=dev)
     ctx = spx.Context(dev.index or 0)
     sc = stream.cuda_stream
+    # the accumulation kernel and slab for the chi0 part of this shape (untimed)
+    tuned4 = ctx.autotune_split(w.nbas, w.npair, w.nw) if args.autotune else None
 
     def timed(fn, warmup, steps):
         for _ in range(warmup):
@@ -719,6 +721,7 @@ def bench_products(args, dev, stream):
            "pw_split_ms": pws_ms, "pw_split_tflops_equiv": fl_pw / (pws_ms * 1e-3) / 1e12,
            "pw_fft_branch_ms": pwf_ms, "pw_fft_grid": 48,
            "kernels_per_step": st["kernel_launches"], "m_bytes_on_device": 16 * w.nbas * w.npair,
+           "chi0_autotuned": None if tuned4 is None else {k: tuned4[k] for k in ("variant", "slab_pairs", "tflops")},
            "accuracy": acc}
     # rooflines of the products: the GEMMs against the tensor pipes they run on, and
     # the HBM bytes the products must move (the M columns they write) against the

@@ -67,7 +67,8 @@ typedef struct spx_options {
   int64_t pinned_limit;     /* pinned host staging bytes, 0 = auto               */
   int32_t chunk_pairs;      /* band pairs per streamed chunk, 0 = auto           */
   int32_t timeout_ms;       /* bound on every device-side wait, 0 = 4000 ms      */
-  int32_t split_variant;    /* split-path kernel: 0 auto, 1 one CTA per 64 x 64
+  int32_t split_variant;    /* split-path kernel: 0 auto (the tuning table's choice,
+                               else 5), 1 one CTA per 64 x 64
                                tile, 2 CTA pair (tcgen05 cta_group::2), 3 the
                                persistent schedule with its own preparation warps,
                                5 one CTA per 64 x 80 tile (N = 160 MMAs)         */

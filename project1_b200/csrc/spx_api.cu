@@ -44,7 +44,7 @@ int pb_single(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N, con
               int tile, int slab, char* scratch, size_t scratch_bytes, cudaStream_t s, int* launches);
 
 // The split variant and slab a call of this shape runs with: the context's forced
-// variant, else the tuning table's, else the CTA-pair kernel with 32768-pair slabs.
+// variant, else the tuning table's, else one CTA per 64 x 80 tile with 32768-pair slabs.
 static void split_choice(spx_ctx* ctx, int N, int64_t P, int nw, int* variant, int* slab, int* tile) {
   *variant = ctx->opt.split_variant;
   *slab = 0;

@@ -52,7 +52,7 @@ int pb_single(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N, con
               const double* wscale, double scale_all, int nw, const double* omega, double2* out,
               int tile, int slab, char* scratch, size_t scratch_bytes, cudaStream_t s, int* launches);
 
-constexpr int kDefaultVariant = 2;
+constexpr int kDefaultVariant = 5;  // one CTA per 64 x 80 tile
 constexpr int kDefaultSlab = 32768;
 constexpr int64_t kChunkSlabs = 8;   // pairs per generated / weighted chunk, in slabs
 constexpr size_t kMaxGraphs = 8;

@@ -870,7 +870,8 @@ int split_chi0_slab(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int 
   // with increasing strides; a box (K, rows, 1, 3 planes) lands as [plane][row][K]
   const uint64_t nkb = (uint64_t)(L.Ps / SP_KB);
   if (variant == 0) variant = ctx->opt.split_variant;
-  const bool pair = variant != 1 && variant != 5;  // 0 (auto) and 2 select the CTA pair
+  if (variant == 0) variant = 5;  // untuned: one CTA per 64 x 80 tile
+  const bool pair = variant == 2;
   const bool wide = variant == 5;                  // one CTA per 64 x 80 tile (N = 160)
   // only the CTA pair needs an even number of 64-column blocks in the planes (the
   // buffers are sized for it either way)
