@@ -405,7 +405,7 @@ def run_ours(args):
         tuned = {"variant": args.variant or 1, "slab_pairs": args.slab, "tflops": 0.0}
         entry = {"nbas_bucket": (N + 127) // 128, "npair_bucket": 0 if Pr <= 16384 else (1 if Pr <= 32768 else 2),
                  "nw": nw, "variant": tuned["variant"], "slab_pairs": args.slab,
-                 "tile": 64 + 3 * 256 if tuned["variant"] == 3 else 0, "tflops": 0.0}
+                 "tile": 80 + 3 * 256 if tuned["variant"] == 3 else 0, "tflops": 0.0}
         with tempfile.TemporaryDirectory() as td:
             with open(os.path.join(td, "tune.json"), "w") as fh:
                 json.dump({"format": "spexgpu-tune-1", "entries": [entry]}, fh)
@@ -565,7 +565,12 @@ def bench_batched(args, dev, stream):
     import project1_b200 as spx
     from project1_b200 import _lib, inputs
     bw = inputs.BATCHED_CONFIGS["c3"]
+    if args.c3_kpts:
+        import dataclasses
+        bw = dataclasses.replace(bw, nk=args.c3_kpts)
     qws = inputs.batched_qs(bw)
+    if args.c3_qs:
+        qws = qws[:args.c3_qs]
     omega = torch.from_numpy(inputs.frequencies(bw.nw)).to(dev)
     ctx = spx.Context(dev.index or 0)
     qs = []
@@ -576,16 +581,21 @@ def bench_batched(args, dev, stream):
                        susceph=torch.zeros((bw.nw, spx.npack(qw.nbas)), dtype=torch.complex128,
                                            device=dev)))
     flops = sum(q.flops for q in qws)
+    # role cycle counters of the persistent kernel (captured with the graph)
+    ctx.pb_profile_enable(True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for i in range(args.batched_warmup):
         for q in qs:
             q["susceph"].zero_()
-        ctx.chi0_batched(qs, omega, flags=_lib.SPX_BATCH_AUTOTUNE if i == 0 else 0,
+        ctx.chi0_batched(qs, omega, flags=_lib.SPX_BATCH_AUTOTUNE if i == 0 and args.autotune else 0,
                          stream=stream.cuda_stream, stats=True)
     warm_s = time.perf_counter() - t0
+    ctx.pb_profile_enable(True)   # zeroed: the timed batches only
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     kernels = 0
+    sampler = ClockSampler(dev.index or 0)
+    sampler.start()
     e0.record(stream)
     for _ in range(args.batched_steps):
         for q in qs:
@@ -594,7 +604,13 @@ def bench_batched(args, dev, stream):
         kernels = st["kernel_launches"]
     e1.record(stream)
     torch.cuda.synchronize()
+    clocks = sampler.stop()
     ms = e0.elapsed_time(e1) / args.batched_steps
+    prof = ctx.pb_profile_read()
+    ctx.pb_profile_enable(False)
+    cta = prof.pop("cta") or 1.0
+    role = {k: round(v / cta, 4) for k, v in prof.items() if not k.endswith("_items")}
+    role.update({k: int(v) for k, v in prof.items() if k.endswith("_items")})
     tune = [ctx.tune_lookup_batched(q["nbas"], q["npair"], bw.nw) for q in qs]
     # accuracy at full size on three q (the two cheapest and the median by flops):
     # the same batched call in FP64 against the split result of the timed batch
@@ -611,7 +627,7 @@ def bench_batched(args, dev, stream):
                "max_normalized": max(x["max_normalized"] for x in per_q),
                "raw_rel_max": max(x["raw_rel_max"] for x in per_q)}
         del sub
-    res = {"workload": f"c3: {bw.nq} q, N_MB U{{{bw.nbas_range[0]}..{bw.nbas_range[1]}}}, "
+    res = {"workload": f"c3: {len(qws)} q, N_MB U{{{bw.nbas_range[0]}..{bw.nbas_range[1]}}}, "
                        f"occ U{{{bw.occ_range[0]}..{bw.occ_range[1]}}} x unocc "
                        f"U{{{bw.unocc_range[0]}..{bw.unocc_range[1]}}}, {bw.nk} k, {bw.nw} freqs, split",
            "value": flops / (ms * 1e-3) / 1e12, "unit": UNIT, "ms_per_step": ms,
@@ -624,7 +640,10 @@ def bench_batched(args, dev, stream):
                                     for t in tune if t}),
            "schedule": "one persistent kernel per batch (accumulation and operand-preparation "
                        "queues on every SM), captured in a CUDA graph",
-           "m_generated_on_device": True, "accuracy": acc}
+           "m_generated_on_device": True, "clocks": clocks,
+           "role_profile": dict(role, note="cycles of one thread per role and CTA as a fraction of the "
+                                           "CTAs' cycles (spx_pb_profile_read), summed over the timed batches"),
+           "accuracy": acc}
     ctx.close()
     return res
 
@@ -838,6 +857,8 @@ def main():
     ap.add_argument("--batched-steps", type=int, default=1, help="timed batches of the batched q-point workload (0: skip)")
     ap.add_argument("--batched-warmup", type=int, default=1)
     ap.add_argument("--c4-kpts", type=int, default=0, help="override the products workload's k-point count (profiling)")
+    ap.add_argument("--c3-kpts", type=int, default=0, help="override the batched workload's k-point count (profiling)")
+    ap.add_argument("--c3-qs", type=int, default=0, help="only the first n q points of the batched workload (profiling)")
     ap.add_argument("--precision", choices=["split", "fp64"], default=None,
                     help="force the measured path (profiling captures)")
     ap.add_argument("--variant", type=int, default=0, choices=[0, 1, 2, 3, 5],

@@ -403,7 +403,7 @@ typedef struct spx_tune_entry {
                                4 an entry of the batched table                        */
   int32_t slab_pairs;
   int32_t tile;             /* variants 3 and 4: tile columns (64, 32 or 80) + 256 *
-                               pipeline stages (2 to 4); 0 otherwise                  */
+                               pipeline stages (3, or 4 for 32 columns); 0 otherwise  */
   double  tflops;           /* measured throughput of the chosen configuration        */
 } spx_tune_entry;
 
@@ -415,9 +415,9 @@ int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
 int spx_tune_lookup(const spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
                     spx_tune_entry* out);
 /* The same for the persistent batched schedule: measures its tile shapes (64 x 64
- * complex with 3 pipeline stages, 64 x 32 with 3 or 4, 64 x 80 with 3) and slab
- * sizes on a seeded probe of one q, stores the fastest (variant 4), and looks
- * entries up. */
+ * complex with 3 pipeline stages, 64 x 80 with 3, 64 x 32 with 4; tables may also
+ * name 64 x 32 with 3) and slab sizes on a seeded probe of one q, stores the fastest
+ * (variant 4), and looks entries up. Untuned batches run 64 x 80 tiles. */
 int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
                          spx_tune_entry* out);
 int spx_tune_lookup_batched(const spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
@@ -425,6 +425,26 @@ int spx_tune_lookup_batched(const spx_ctx* ctx, int32_t nbas, int64_t npair, int
 /* The table as a JSON file, and back (entries are merged into the table). */
 int spx_tune_save(const spx_ctx* ctx, const char* path);
 int spx_tune_load(spx_ctx* ctx, const char* path);
+
+/* Role profile of the persistent schedule (no counterpart in the reference, which
+ * has no device schedule): while enabled, every launch of the persistent kernel
+ * (batched split calls, single calls of variant 3) adds per-CTA cycle counts of its
+ * roles into the context's counters. Launches captured into a cached graph keep
+ * the setting they were captured with. enable(1) allocates the counters on first
+ * use and zeroes them; read waits for the device and returns the first n (at most
+ * SPX_PB_PROF_N) counters:
+ *   0 CTA cycles                       7 epilogue: waiting for slab s-1's adds
+ *   1 TMA: waiting for a slab's planes 8 preparation: waiting (buffer, maxima)
+ *   2 TMA: waiting for a free stage    9 preparation: M and column maxima
+ *   3 MMA: waiting for operands       10 preparation: weights and factors
+ *   4 MMA: waiting for the epilogue   11 preparation: digit planes
+ *   5 MMA: waiting for an item        12 accumulation items
+ *   6 epilogue: waiting for a tile    13 preparation items
+ * (cycles of one thread per role and CTA, summed over CTAs; 6 and 7 of the first
+ * epilogue warp). */
+#define SPX_PB_PROF_N 14
+int spx_pb_profile_enable(spx_ctx* ctx, int32_t on);
+int spx_pb_profile_read(spx_ctx* ctx, double* out, int32_t n);
 
 /* ---- diagnostics ------------------------------------------------------------
  * Runs one kernel that waits, with the library's bounded device wait, on a barrier

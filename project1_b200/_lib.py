@@ -158,6 +158,8 @@ SIGNATURES = {
     "spx_autotune_batched": (C.c_int, [_P, _I32, _I64, _I32, C.POINTER(spx_tune_entry)]),
     "spx_tune_lookup_batched": (C.c_int, [_P, _I32, _I64, _I32, C.POINTER(spx_tune_entry)]),
     "spx_tune_save": (C.c_int, [_P, C.c_char_p]),
+    "spx_pb_profile_enable": (C.c_int, [_P, _I32]),
+    "spx_pb_profile_read": (C.c_int, [_P, _P, _I32]),
     "spx_tune_load": (C.c_int, [_P, C.c_char_p]),
     "spx_gen_normal_host": (None, [C.c_uint64, C.c_uint32, _I64, _I64, C.c_double, _P]),
     "spx_gen_normal_dev": (C.c_int, [_P, C.c_uint64, C.c_uint32, _I64, _I64, C.c_double, _P, _P]),

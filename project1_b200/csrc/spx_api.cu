@@ -37,6 +37,7 @@ int launch_chi0_fp64(spx_ctx*, const double2*, int64_t, int64_t, int, const doub
 int split_chi0_slab(spx_ctx*, const double2*, int64_t, int64_t, int, const double*, int64_t,
                     int, double2*, void*, size_t, cudaStream_t, int*, int variant, int slab);
 size_t split_workspace_bytes(int64_t P, int N, int nw);
+size_t split_workspace_bytes(int64_t P, int N, int nw, int slab);
 size_t split_workspace_bytes_real(int64_t P, int N, int nw);
 size_t pb_single_bytes(int64_t P, int N, int nw, int slab);
 int pb_single(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N, const double* ediff,
@@ -48,7 +49,7 @@ int pb_single(spx_ctx* ctx, const double2* M, int64_t ldc, int64_t P, int N, con
 static void split_choice(spx_ctx* ctx, int N, int64_t P, int nw, int* variant, int* slab, int* tile) {
   *variant = ctx->opt.split_variant;
   *slab = 0;
-  *tile = 64 + 3 * 256;
+  *tile = kPbDefaultTile;
   spx_tune_entry te;
   if (*variant == 0 && spx_tune_lookup(ctx, N, P, nw, &te) == SPX_OK) {
     *variant = te.variant;
@@ -62,12 +63,18 @@ static void split_choice(spx_ctx* ctx, int N, int64_t P, int nw, int* variant, i
 static size_t split_scratch_bytes(spx_ctx* ctx, int64_t P, int N, int nw) {
   int variant, slab, tile;
   split_choice(ctx, N, P, nw, &variant, &slab, &tile);
+  // a slab below P takes two buffers of that slab, which can exceed one buffer of
+  // P pairs (P = 16000 at 8192-pair slabs)
   size_t b = split_workspace_bytes(P, N, nw);
-  // the host path cuts P into chunks whose buckets may choose differently: any
-  // persistent entry for this width sizes the scratch for it
+  if (slab > 0) b = std::max(b, split_workspace_bytes(P, N, nw, slab));
+  // the host path runs the plan chosen for the whole array on shorter chunks: every
+  // entry for this width sizes the scratch for its slab and kernel
   bool persistent = variant == 3;
-  for (const auto& e : ctx->tune)
-    if (e.variant == 3 && e.nw == nw) persistent = true;
+  for (const auto& e : ctx->tune) {
+    if (e.nw != nw || e.variant == 4) continue;
+    if (e.variant == 3) persistent = true;
+    if (e.slab_pairs > 0) b = std::max(b, split_workspace_bytes(P, N, nw, e.slab_pairs));
+  }
   if (persistent) b = std::max(b, pb_single_bytes(P, N, nw, 32768));
   return b;
 }
@@ -336,6 +343,7 @@ extern "C" int spx_ctx_destroy(spx_ctx* ctx) {
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->d_prof) cudaFree(ctx->d_prof);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   if (ctx->prep_stream) cudaStreamDestroy(ctx->prep_stream);
@@ -543,7 +551,7 @@ extern "C" int spx_chi0_accumulate(spx_ctx* ctx, const double* cprod, int64_t ld
   // One split kernel and slab size for the whole array (chosen for npair), so that
   // the chunks' exact slabs are the device call's: chunk boundaries stay on
   // multiples of that slab and the result equals the device call's bit for bit.
-  int plan[3] = {0, 0, 64 + 3 * 256};
+  int plan[3] = {0, 0, kPbDefaultTile};
   if (precision == SPX_SPLIT) split_choice(ctx, nbas, npair, nw, &plan[0], &plan[1], &plan[2]);
   const int64_t align = precision == SPX_SPLIT ? (plan[1] > 0 ? plan[1] : 32768) : 16384;
   // slab size: band pairs per streamed chunk

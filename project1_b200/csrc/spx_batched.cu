@@ -385,7 +385,7 @@ extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int
   cudaEvent_t e0 = ctx->ev[8], e1 = ctx->ev[9];
   // Candidates: variants 1, 5 and 2 (the slab kernels with the quantizer beside them:
   // one CTA per 64 x 64 tile, one CTA per 64 x 80 tile, the CTA pair) and 3 (the
-  // persistent schedule with its own preparation warps, 64 x 64 tiles, 3 stages), at
+  // persistent schedule with its own preparation warps, 64 x 80 tiles, 3 stages), at
   // each slab size. The rounds interleave the candidates, so a clock that drifts under
   // the power cap while the probe runs favours none of them; each keeps its best round.
   struct Cand {
@@ -408,7 +408,7 @@ extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int
       cudaEventRecord(e0, s);
       for (int pass = 0; pass < kPasses && !rc; ++pass) {
         if (c.variant == 3)
-          rc = pb_single(ctx, M, ld, P, nbas, E, nullptr, 1.0, nw, OM, O, 64 + 3 * 256, c.slab, (char*)S,
+          rc = pb_single(ctx, M, ld, P, nbas, E, nullptr, 1.0, nw, OM, O, kPbDefaultTile, c.slab, (char*)S,
                          sws, s, &launches);
         else
           rc = split_chi0_slab(ctx, M, ld, P, nbas, W, ld, nw, O, S, sws, s, &launches, c.variant, c.slab);
@@ -426,7 +426,7 @@ extern "C" int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int
       best.tflops = tf;
       best.variant = c.variant;
       best.slab_pairs = c.slab;
-      best.tile = c.variant == 3 ? 64 + 3 * 256 : 0;
+      best.tile = c.variant == 3 ? kPbDefaultTile : 0;
     }
   }
   store_tune(ctx, best);
@@ -500,7 +500,7 @@ extern "C" int spx_tune_load(spx_ctx* ctx, const char* path) {
     json_field(obj, "tflops", &tf);
     json_field(obj, "tile", &tile);
     if (var < 1 || var > 5 || sl < 64 || sl > 32768 || nb < 1 || nw < 1 || pb < 0 || pb > 2 ||
-        tile < 0 || tile > 4 * 256 + 64)
+        tile < 0 || tile > 4 * 256 + 80)
       return set_error(ctx, SPX_EINVAL, "tuning entry out of range");
     spx_tune_entry t{};
     t.nbas_bucket = (int)nb;

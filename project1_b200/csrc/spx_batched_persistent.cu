@@ -40,6 +40,7 @@
 
 namespace spx {
 
+constexpr int PB_EPI = 4;         // epilogue warps (one per TMEM lane quarter)
 constexpr int PB_THREADS = 384;   // warps 0-5 accumulation, 6-11 preparation
 constexpr int PB_PREP0 = 192;     // first preparation thread
 constexpr int PB_NPREP = 192;
@@ -95,6 +96,7 @@ struct PbParams {
   int* gdone;                 // per slab: finished accumulation items
   int* status;
   uint64_t timeout_ns;
+  unsigned long long* prof;   // SPX_PB_PROF_N role counters, or NULL
 };
 
 #if defined(__CUDACC__)
@@ -110,9 +112,9 @@ __device__ __forceinline__ void fence_proxy_async_global() {
   asm volatile("fence.proxy.async.global;" ::: "memory");
 }
 // Bounded wait until *ctr >= target (acquire). False on timeout (status set) or
-// when another worker has already given up.
-__device__ __noinline__ bool gwait(const int* ctr, int target, uint64_t timeout_ns, int* status) {
-  if (ld_acquire(ctr) >= target) return true;
+// when another worker has already given up. The first look is inline (the counter is
+// usually there already); the spinning is a call, so its code exists once.
+__device__ __noinline__ bool gwait_spin(const int* ctr, int target, uint64_t timeout_ns, int* status) {
   const uint64_t t0 = global_ns();
   for (uint32_t n = 1;; ++n) {
     __nanosleep(64);
@@ -126,6 +128,9 @@ __device__ __noinline__ bool gwait(const int* ctr, int target, uint64_t timeout_
     }
   }
 }
+__device__ __forceinline__ bool gwait(const int* ctr, int target, uint64_t timeout_ns, int* status) {
+  return ld_acquire(ctr) >= target || gwait_spin(ctr, target, timeout_ns, status);
+}
 // The last index k with key(k) <= v over a nondecreasing array (first entry <= v).
 __device__ __forceinline__ int pb_find(const PbSlab* sl, int n, int64_t v, bool prep) {
   int lo = 0, hi = n - 1;
@@ -136,34 +141,33 @@ __device__ __forceinline__ int pb_find(const PbSlab* sl, int n, int64_t v, bool 
   }
   return lo;
 }
-// Tile t of the upper region for BN-column tiles -> (bi 64-row block, bj BN-column
-// block), column-major: column block bj holds row blocks 0..(bj*BN + BN - 1)/64.
-template <int BN>
-__device__ __forceinline__ void pb_decode_tile(int t, int* bi, int* bj) {
-  if constexpr (BN == 64) {
-    split_decode_tile(t, bi, bj);
-  } else {
-    int j = 0, c = 0;
-    while (c + (j * BN + BN - 1) / 64 + 1 <= t) {
-      c += (j * BN + BN - 1) / 64 + 1;
-      ++j;
-    }
-    *bj = j;
-    *bi = t - c;
-  }
-}
 #endif
 
+// Tiles of the upper region for 64-row x BN-column tiles, column-major (column block
+// bj holds the row blocks that reach its last column, at most the last of N's).
 template <int BN>
-constexpr int pb_ntile(int N) {
-  int nb = (N + BN - 1) / BN, c = 0;
-  for (int j = 0; j < nb; ++j) c += (j * BN + BN - 1) / 64 + 1;
+inline int pb_ntile(int N) {
+  const int nb = (N + BN - 1) / BN, nbr = (N + 63) / 64;
+  int c = 0;
+  for (int j = 0; j < nb; ++j) c += split_rows_of(j, BN, nbr);
   return c;
 }
 
 // Columns of a tile the epilogue stages in shared memory: all of them, except for the
 // 64 x 80 tile, whose second half stays in registers (three pipeline stages then fit).
 constexpr int pb_sbn(int bn) { return bn == 80 ? 40 : bn; }
+
+// An accumulation item as the pipeline roles read it (taken from the queue and
+// decoded ahead of use, so that no role waits on global memory between items).
+struct PbItem {
+  int k;                // slab (-1: the queue is empty)
+  int tile, f, bi, bj;  // tile (round-aware order), frequency, its row / column blocks
+  int nk, jr;           // 64-pair stages, K direction of the round
+  int qi, slot, nc;     // q point, operand buffer, digit items that make the planes ready
+  int same;             // set by the TMA producer: A doubles as B (diagonal 64 x 64 tile)
+  int pad;
+  const int* wsgn;      // the buffer's per-frequency weight signs
+};
 
 template <int BN, int ST>
 struct __align__(1024) PbSmem {
@@ -173,10 +177,10 @@ struct __align__(1024) PbSmem {
                                          // pb_sbn(BN) columns; the rest in registers)
   uint64_t full[ST], empty[ST];
   uint64_t tfull, tempty, mdone;
-  uint64_t ifull[PB_RING], ifree[PB_RING];
-  int4 desc[PB_RING];                   // item: slab k, tile, frequency, flags
+  uint64_t ifull[PB_RING];
+  PbItem item[PB_RING];                 // accumulation items taken ahead, decoded
   long long prep_item;
-  int eflag;
+  int ecount[PB_RING];                  // epilogue warps done with a ring entry's item
   double red[PB_NPREP / 32];
   int redi[2][PB_NPREP / 32];
   uint32_t tmem_base;
@@ -186,15 +190,21 @@ struct __align__(1024) PbSmem {
 // ---------------- preparation workers (192 threads) ----------------
 __device__ __forceinline__ void pb_prep_bar() { named_bar_sync(1, PB_NPREP); }
 
+// Adds a role's cycle counts to the launch's profile (prm.prof, when given).
+__device__ __forceinline__ void pb_prof_add(const PbParams& prm, int k, unsigned long long v) {
+  if (prm.prof && v) atomicAdd(prm.prof + k, v);
+}
+
 template <int BN, int ST>
 __device__ void pb_prep(PbSmem<BN, ST>& sm, const PbParams& prm, int pt) {
   const int pw = pt >> 5, lane = pt & 31;
+  unsigned long long c_wait = 0, c_kind[3] = {0, 0, 0}, n_items = 0;
   for (;;) {
     if (pt == 0) sm.prep_item = (long long)atomicAdd(&prm.heads[1], 1ull);
     pb_prep_bar();
     const int64_t item = sm.prep_item;
     pb_prep_bar();  // everyone has read it before thread 0 may overwrite it
-    if (item >= prm.nprep) return;
+    if (item >= prm.nprep) break;
     const int k = pb_find(prm.slab, prm.nslab, item, true);
     const PbSlab& sl = prm.slab[k];
     const PbQ& q = prm.q[sl.q];
@@ -205,6 +215,7 @@ __device__ void pb_prep(PbSmem<BN, ST>& sm, const PbParams& prm, int pt) {
     // the buffer must be free (the slab that used it last fully accumulated), and a
     // quantizer item needs its slab's maxima and factors
     int ok = 1;
+    const long long t0 = clock64();
     if (pt == 0) {
       if (k >= prm.nslot) {
         const PbSlab& prev = prm.slab[k - prm.nslot];
@@ -216,7 +227,8 @@ __device__ void pb_prep(PbSmem<BN, ST>& sm, const PbParams& prm, int pt) {
     pb_prep_bar();
     ok = sm.redi[0][0];
     pb_prep_bar();
-    if (!ok) return;
+    if (!ok) break;
+    const long long t1 = clock64();
 
     if (kind == 0) {
       // (a) column i: M values of the slab (generated into the buffer, or the
@@ -307,7 +319,48 @@ __device__ void pb_prep(PbSmem<BN, ST>& sm, const PbParams& prm, int pt) {
     __threadfence();
     pb_prep_bar();
     if (pt == 0) red_release_add(kind == 2 ? &prm.ready[k] : &prm.ab[k], 1);
+    c_wait += (unsigned long long)(t1 - t0);
+    c_kind[kind] += (unsigned long long)(clock64() - t1);
+    ++n_items;
   }
+  if (pt == 0) {
+    pb_prof_add(prm, 8, c_wait);
+    for (int k = 0; k < 3; ++k) pb_prof_add(prm, 9 + k, c_kind[k]);
+    pb_prof_add(prm, 13, n_items);
+  }
+}
+
+// Takes the next accumulation item from the queue into `it`. A CTA's items come in
+// increasing order, so the slab is searched forward from `kprev` (the slab of the
+// CTA's previous item), with a binary search when it lies further on.
+template <int BN>
+__device__ __forceinline__ void pb_take_item(const PbParams& prm, int kprev, PbItem* it) {
+  const int64_t g = kprev < 0 ? prm.ngram : (int64_t)atomicAdd(&prm.heads[0], 1ull);
+  if (g >= prm.ngram) {
+    it->k = -1;
+    return;
+  }
+  int k = kprev, n = 0;
+  while (k + 1 < prm.nslab && prm.slab[k + 1].g0 <= g && ++n <= 8) ++k;
+  if (n > 8) k = pb_find(prm.slab, prm.nslab, g, false);
+  const PbSlab& sl = prm.slab[k];
+  const PbQ& q = prm.q[sl.q];
+  const int local = (int)(g - sl.g0);
+  const int tile = split_round_tile(local % q.ntile, q.ntile, g - local % q.ntile, gridDim.x);
+  int bi, bj;
+  split_decode_tile_bn<BN>(tile, q.nblk, &bi, &bj);
+  it->k = k;
+  it->tile = tile;
+  it->f = local / q.ntile;
+  it->bi = bi;
+  it->bj = bj;
+  it->nk = sl.nk;
+  it->jr = (int)((g / gridDim.x) & 1);
+  it->qi = sl.q;
+  it->slot = sl.slot;
+  it->nc = sl.nc;
+  it->same = 0;
+  it->wsgn = prm.slot[sl.slot].wsgn;
 }
 
 template <int BN, int ST>
@@ -320,6 +373,7 @@ __global__ void __launch_bounds__(PB_THREADS, 1) pb_kernel(PbParams prm) {
   constexpr uint32_t IDESC = sp_idesc(BROWS);
   constexpr uint32_t OSTRIDE = BROWS;            // TMEM columns per order
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long t_start = clock64();
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < ST; ++s) {
@@ -328,10 +382,10 @@ __global__ void __launch_bounds__(PB_THREADS, 1) pb_kernel(PbParams prm) {
     }
     for (int r = 0; r < PB_RING; ++r) {
       mbar_init(&sm.ifull[r], 1);
-      mbar_init(&sm.ifree[r], 1);
+      sm.ecount[r] = 0;
     }
     mbar_init(&sm.tfull, 1);
-    mbar_init(&sm.tempty, 4);
+    mbar_init(&sm.tempty, PB_EPI);
     mbar_init(&sm.mdone, 1);
     fence_barrier_init();
   }
@@ -344,58 +398,46 @@ __global__ void __launch_bounds__(PB_THREADS, 1) pb_kernel(PbParams prm) {
   if (threadIdx.x >= PB_PREP0) {
     pb_prep<BN, ST>(sm, prm, threadIdx.x - PB_PREP0);
   } else if (warp == 0) {
-    // ---------------- TMA producer: takes the items ----------------
+    // ---------------- TMA producer ----------------
     if (lane == 0) {
       int st = 0;
       uint32_t ph = 0;
       bool issued[ST];
       uint32_t last_ph[ST];
+      unsigned long long c_ready = 0, c_empty = 0, n_items = 0;
       for (int s = 0; s < ST; ++s) issued[s] = false, last_ph[s] = 0;
       for (int j = 0;; ++j) {
         const int r = j % PB_RING;
-        // the ring entry of item j - PB_RING has been retired by the epilogue
-        if (j >= PB_RING &&
-            !mbar_wait(&sm.ifree[r], (uint32_t)((j / PB_RING - 1) & 1), prm.timeout_ns, prm.status)) {
-          sm.desc[r] = make_int4(-1, 0, 0, 0);
-          mbar_arrive(&sm.ifull[r]);
-          break;
-        }
-        const int64_t g = (int64_t)atomicAdd(&prm.heads[0], 1ull);
-        if (g >= prm.ngram) {
-          sm.desc[r] = make_int4(-1, 0, 0, 0);
-          mbar_arrive(&sm.ifull[r]);
-          break;
-        }
-        const int k = pb_find(prm.slab, prm.nslab, g, false);
-        const PbSlab& sl = prm.slab[k];
-        const PbQ& q = prm.q[sl.q];
-        const int local = (int)(g - sl.g0);
-        const int f = local / q.ntile;
-        const int tile = split_round_tile(local % q.ntile, q.ntile, g - local % q.ntile, gridDim.x);
-        const int jr = (int)((g / gridDim.x) & 1);  // this round's K direction
-        int bi, bj;
-        pb_decode_tile<BN>(tile, &bi, &bj);
+        if (!mbar_wait(&sm.ifull[r], (uint32_t)((j / PB_RING) & 1), prm.timeout_ns, prm.status)) break;
+        const PbItem it = sm.item[r];
+        if (it.k < 0) break;
         // the slab's planes must be ready before the first copy
-        const bool okr = gwait(&prm.ready[k], sl.nc, prm.timeout_ns, prm.status);
-        const int sg = okr ? prm.slot[sl.slot].wsgn[f] : 1;
-        const bool same = BN == SP_TILE && sg != 0 && bi == bj;
-        sm.desc[r] = make_int4(okr ? k : -1, tile, f, same ? 1 : 0);
-        mbar_arrive(&sm.ifull[r]);
+        long long tw = clock64();
+        const bool okr = gwait(&prm.ready[it.k], it.nc, prm.timeout_ns, prm.status);
+        c_ready += (unsigned long long)(clock64() - tw);
+        ++n_items;
         if (!okr) break;
+        const int sg = it.wsgn[it.f];
+        const bool same = BN == SP_TILE && sg != 0 && it.bi == it.bj;
+        // read by the MMA issuer once the item's first stage has landed (the stage's
+        // barrier orders this store before that read)
+        sm.item[r].same = same ? 1 : 0;
         fence_proxy_async_global();
-        const CUtensorMap* mA = prm.maps + 2 * ((int64_t)sl.q * prm.nslot + sl.slot);
+        const CUtensorMap* mA = prm.maps + 2 * ((int64_t)it.qi * prm.nslot + it.slot);
         const CUtensorMap* mB = mA + 1;
-        const int za = f * SP_SLOT, zb = za + (sg == 0 ? SP_SF : 0);
+        const int za = it.f * SP_SLOT, zb = za + (sg == 0 ? SP_SF : 0);
         bool ok = true;
-        for (int ks = 0; ks < sl.nk; ++ks) {
+        for (int ks = 0; ks < it.nk; ++ks) {
+          tw = clock64();
           if (!mbar_wait(&sm.empty[st], ph ^ 1u, prm.timeout_ns, prm.status)) {
             ok = false;
             break;
           }
+          c_empty += (unsigned long long)(clock64() - tw);
           mbar_arrive_expect_tx(&sm.full[st], (uint32_t)(SP_SF * (SP_PLANE + (same ? 0 : BROWS * SP_KB))));
-          const int kc = split_k_order(jr, ks, sl.nk);
-          tma_load_4d(&sm.a[st][0][0], mA, 0, bi * SP_ROWS, kc, za, &sm.full[st]);
-          if (!same) tma_load_4d(&sm.b[st][0][0], mB, 0, bj * BROWS, kc, zb, &sm.full[st]);
+          const int kc = split_k_order(it.jr, ks, it.nk);
+          tma_load_4d(&sm.a[st][0][0], mA, 0, it.bi * SP_ROWS, kc, za, &sm.full[st]);
+          if (!same) tma_load_4d(&sm.b[st][0][0], mB, 0, it.bj * BROWS, kc, zb, &sm.full[st]);
           issued[st] = true;
           last_ph[st] = ph;
           if (++st == ST) st = 0, ph ^= 1u;
@@ -404,6 +446,9 @@ __global__ void __launch_bounds__(PB_THREADS, 1) pb_kernel(PbParams prm) {
       }
       for (int s = 0; s < ST; ++s)
         if (issued[s]) mbar_drain(&sm.full[s], last_ph[s], prm.timeout_ns);
+      pb_prof_add(prm, 1, c_ready);
+      pb_prof_add(prm, 2, c_empty);
+      pb_prof_add(prm, 12, n_items);
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
@@ -411,22 +456,30 @@ __global__ void __launch_bounds__(PB_THREADS, 1) pb_kernel(PbParams prm) {
       int st = 0;
       uint32_t ph = 0;
       bool committed = false;
+      unsigned long long c_item = 0, c_acc = 0, c_full = 0;
       for (int j = 0;; ++j) {
         const int r = j % PB_RING;
+        long long tw = clock64();
         if (!mbar_wait_idle(&sm.ifull[r], (uint32_t)((j / PB_RING) & 1), prm.timeout_ns, prm.status)) break;
-        const int4 d = sm.desc[r];
-        if (d.x < 0) break;
-        const int nk = prm.slab[d.x].nk;
-        const bool same = d.w != 0;
+        c_item += (unsigned long long)(clock64() - tw);
+        const int kslab = sm.item[r].k;
+        if (kslab < 0) break;
+        const int nk = sm.item[r].nk;
+        bool same = false;
+        tw = clock64();
         if (!mbar_wait(&sm.tempty, (uint32_t)(j & 1) ^ 1u, prm.timeout_ns, prm.status)) break;
+        c_acc += (unsigned long long)(clock64() - tw);
         tc_fence_after();
         bool ok = true;
         for (int ks = 0; ks < nk; ++ks) {
+          tw = clock64();
           if (!mbar_wait(&sm.full[st], ph, prm.timeout_ns, prm.status)) {
             ok = false;
             break;
           }
+          c_full += (unsigned long long)(clock64() - tw);
           tc_fence_after();
+          if (ks == 0) same = sm.item[r].same != 0;
 #pragma unroll
           for (int kk = 0; kk < SP_NKS; ++kk) {
             uint64_t da[SP_SF], db[SP_SF];
@@ -454,6 +507,9 @@ __global__ void __launch_bounds__(PB_THREADS, 1) pb_kernel(PbParams prm) {
         tc_commit(&sm.mdone);
         mbar_drain(&sm.mdone, 0u, prm.timeout_ns);
       }
+      pb_prof_add(prm, 3, c_full);
+      pb_prof_add(prm, 4, c_acc);
+      pb_prof_add(prm, 5, c_item);
     }
   } else {
     // ---------------- epilogue: warps 2-5, TMEM lane quarter warp % 4 ----------------
@@ -461,20 +517,30 @@ __global__ void __launch_bounds__(PB_THREADS, 1) pb_kernel(PbParams prm) {
     const int row = 32 * qd + lane;          // TMEM lane = real-stacked row of the tile
     const int c = lane & 1;
     const uint32_t tl = tmem + ((uint32_t)(32 * qd) << 16);
-    const int et = threadIdx.x - 64;         // 0..127
+    unsigned long long c_tile = 0, c_seq = 0;
+    if (threadIdx.x == 64) {
+      // the first PB_RING items; afterwards each entry is refilled by the warp that
+      // retires its item
+      int kprev = pb_find(prm.slab, prm.nslab, 0, false);
+      for (int r = 0; r < PB_RING; ++r) {
+        pb_take_item<BN>(prm, kprev, &sm.item[r]);
+        kprev = sm.item[r].k;
+        mbar_arrive(&sm.ifull[r]);
+      }
+    }
     for (int j = 0;; ++j) {
       const int r = j % PB_RING;
+      long long tw = clock64();
       if (!mbar_wait_idle(&sm.ifull[r], (uint32_t)((j / PB_RING) & 1), prm.timeout_ns, prm.status)) break;
-      const int4 d = sm.desc[r];
-      if (d.x < 0) break;
+      const int kslab = sm.item[r].k;
+      if (kslab < 0) break;
+      const int tile = sm.item[r].tile, f = sm.item[r].f, bi = sm.item[r].bi, bj = sm.item[r].bj;
       if (!mbar_wait_idle(&sm.tfull, (uint32_t)(j & 1), prm.timeout_ns, prm.status)) break;
+      c_tile += (unsigned long long)(clock64() - tw);
       tc_fence_after();
-      const PbSlab& sl = prm.slab[d.x];
+      const PbSlab& sl = prm.slab[kslab];
       const PbQ& q = prm.q[sl.q];
       const PbSlot& slot = prm.slot[sl.slot];
-      int bi, bj;
-      pb_decode_tile<BN>(d.y, &bi, &bj);
-      const int f = d.z;
       // the accumulator, combined into complex values, into shared memory (columns
       // below SBN) and registers (the rest)
       constexpr int SBN = pb_sbn(BN);
@@ -504,11 +570,15 @@ __global__ void __launch_bounds__(PB_THREADS, 1) pb_kernel(PbParams prm) {
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&sm.tempty);  // the MMAs of the next item may start
-      // slab s of this q adds into the tile after slab s-1 did (the order of per-q calls)
-      int* seq = q.seq + (int64_t)f * q.ntile + d.y;
-      if (et == 0) sm.eflag = sl.s == 0 || gwait(seq, sl.s, prm.timeout_ns, prm.status);
-      named_bar_sync(2, 128);
-      const int ok = sm.eflag;
+      // slab s of this q adds into the tile after slab s-1 did (the order of per-q calls);
+      // each warp adds only its own rows (its staged values), so the warps need no
+      // barrier among themselves
+      int* seq = q.seq + (int64_t)f * q.ntile + tile;
+      int ok = 1;
+      tw = clock64();
+      if (lane == 0 && sl.s > 0) ok = gwait(seq, sl.s, prm.timeout_ns, prm.status);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      c_seq += (unsigned long long)(clock64() - tw);
       const int gil = bi * SP_TILE + row / 2;
       if (ok && gil < q.N) {
         const double fac = fold_row_factor(slot.wsgn[f], slot.sA[gil], slot.wmax[f]);
@@ -527,14 +597,23 @@ __global__ void __launch_bounds__(PB_THREADS, 1) pb_kernel(PbParams prm) {
           }
         }
       }
+      // the last warp done with the item publishes it (the tile's order counter, the
+      // slab's count) and refills the ring entry with the item PB_RING further on (no
+      // CTA barrier, so a warp that gave up on a wait cannot hold the others)
       __threadfence();
-      named_bar_sync(2, 128);
-      if (et == 0) {
+      __syncwarp();
+      if (lane == 0 && atomicAdd(&sm.ecount[r], 1) % PB_EPI == PB_EPI - 1) {
+        __threadfence();
         red_release_add(seq, 1);
-        red_release_add(&prm.gdone[d.x], 1);
-        mbar_arrive(&sm.ifree[r]);
+        red_release_add(&prm.gdone[kslab], 1);
+        pb_take_item<BN>(prm, sm.item[(r + PB_RING - 1) % PB_RING].k, &sm.item[r]);
+        mbar_arrive(&sm.ifull[r]);
       }
       if (!ok) break;
+    }
+    if (warp == 2 && lane == 0) {
+      pb_prof_add(prm, 6, c_tile);
+      pb_prof_add(prm, 7, c_seq);
     }
   }
 
@@ -542,6 +621,7 @@ __global__ void __launch_bounds__(PB_THREADS, 1) pb_kernel(PbParams prm) {
   __syncthreads();
   tc_fence_after();
   if (warp == 1) tmem_dealloc(tmem, SP_TMEM_COLS);
+  if (threadIdx.x == 0) pb_prof_add(prm, 0, (unsigned long long)(clock64() - t_start));
 }
 #endif
 
@@ -743,6 +823,7 @@ int pb_build(spx_ctx* ctx, int nq, const spx_q_desc* qd, const int* S, int nw, i
   p.gdone = gdone;
   p.status = ctx->d_status;
   p.timeout_ns = (uint64_t)(ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 4000) * 1000000ull;
+  p.prof = ctx->prof_on ? ctx->d_prof : nullptr;
   return SPX_OK;
 }
 
@@ -770,9 +851,13 @@ int pb_launch(spx_ctx* ctx, const PbParams& prm, PbConfig cfg, void* ctr, size_t
   return check_cuda(ctx, cudaGetLastError(), "persistent batch launch");
 }
 
-constexpr int PB_NSLOT = 3;
+// Operand buffers in the ring: four (the preparation runs up to three slabs ahead of
+// the accumulation) while they take at most 24 GiB, else three.
+static int pb_nslot(int nq, const spx_q_desc* q, const int* S, int nw) {
+  return pb_plan_bytes(nq, q, S, nw, 4) <= ((size_t)24 << 30) ? 4 : 3;
+}
 constexpr int PB_DEFAULT_SLAB = 16384;
-constexpr PbConfig PB_DEFAULT_CFG = {64, 3};
+constexpr PbConfig PB_DEFAULT_CFG = {80, 3};
 constexpr size_t PB_MAX_GRAPHS = 8;
 
 static int pb_nbas_bucket(int N) { return (N + 127) / 128; }
@@ -804,7 +889,7 @@ static uint64_t pb_fnv(uint64_t h, const void* p, size_t n) {
 
 // One persistent launch for the whole batch (split precision). Slab sizes: the
 // descriptor's, else the tuned, else 16384; tile shape: the tuned shape of the q
-// with most work, else 64 x 64 with 3 stages (`force` overrides both when set).
+// with most work, else 64 x 80 with 3 stages (`force` overrides both when set).
 int pb_run(spx_ctx* ctx, int nq, const spx_q_desc* q, int nw, const double* omega, int flags,
            cudaStream_t s, int* launches, const PbConfig* force, int force_slab, char* scratch,
            size_t scratch_bytes) {
@@ -824,7 +909,8 @@ int pb_run(spx_ctx* ctx, int nq, const spx_q_desc* q, int nw, const double* omeg
     }
   }
   if (force) cfg = *force;
-  const size_t bytes = pb_plan_bytes(nq, q, S.data(), nw, PB_NSLOT);
+  const int nslot = pb_nslot(nq, q, S.data(), nw);
+  const size_t bytes = pb_plan_bytes(nq, q, S.data(), nw, nslot);
   PbParams prm;
   void* ctr = nullptr;
   size_t ctr_bytes = 0;
@@ -838,7 +924,7 @@ int pb_run(spx_ctx* ctx, int nq, const spx_q_desc* q, int nw, const double* omeg
       scratch = (char*)ctx->ws;
       scratch_bytes = ctx->ws_bytes;
     }
-    if ((rc = pb_build(ctx, nq, q, S.data(), nw, PB_NSLOT, cfg, omega, scratch, scratch_bytes,
+    if ((rc = pb_build(ctx, nq, q, S.data(), nw, nslot, cfg, omega, scratch, scratch_bytes,
                        &prm, &ctr, &ctr_bytes, s)))
       return rc;
     if ((rc = pb_launch(ctx, prm, cfg, ctr, ctr_bytes, s))) return rc;
@@ -852,6 +938,7 @@ int pb_run(spx_ctx* ctx, int nq, const spx_q_desc* q, int nw, const double* omeg
   key = pb_fnv(key, S.data(), sizeof(int) * nq);
   key = pb_fnv(key, &cfg, sizeof(cfg));
   key = pb_fnv(key, &nw, sizeof(nw));
+  key = pb_fnv(key, &ctx->prof_on, sizeof(ctx->prof_on));
   key = pb_fnv(key, &omega, sizeof(omega));
   spx_ctx::BatchGraph* hit = nullptr;
   for (auto& g : ctx->graphs)
@@ -862,7 +949,7 @@ int pb_run(spx_ctx* ctx, int nq, const spx_q_desc* q, int nw, const double* omeg
       cudaGetLastError();
       return set_error(ctx, SPX_ENOMEM, "persistent batch: cannot allocate " + std::to_string(bytes) + " bytes");
     }
-    rc = pb_build(ctx, nq, q, S.data(), nw, PB_NSLOT, cfg, omega, (char*)mem, bytes, &prm, &ctr, &ctr_bytes,
+    rc = pb_build(ctx, nq, q, S.data(), nw, nslot, cfg, omega, (char*)mem, bytes, &prm, &ctr, &ctr_bytes,
                   ctx->stream);
     // the graph may be launched on another stream: the plan must have landed first
     if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "plan copy");
@@ -908,7 +995,7 @@ size_t pb_single_bytes(int64_t P, int N, int nw, int slab) {
   d.npair = P;
   d.cprod = reinterpret_cast<const double*>(16);   // explicit M: no generation buffer
   const int S = std::max(SP_KB, std::min(SP_SLAB, slab / SP_KB * SP_KB));
-  return pb_plan_bytes(1, &d, &S, nw, PB_NSLOT);
+  return pb_plan_bytes(1, &d, &S, nw, pb_nslot(1, &d, &S, nw));
 }
 
 // One spx_chi0_accumulate_dev-style call (HILBERT NONE weights from ediff, explicit
@@ -1042,6 +1129,37 @@ extern "C" int spx_autotune_batched(spx_ctx* ctx, int32_t nbas, int64_t npair, i
     }
   if (!stored) ctx->tune.push_back(best);
   if (out) *out = best;
+  return SPX_OK;
+}
+
+extern "C" int spx_pb_profile_enable(spx_ctx* ctx, int32_t on) {
+  if (!ctx) return SPX_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (on) {
+    const size_t bytes = sizeof(unsigned long long) * SPX_PB_PROF_N;
+    if (!ctx->d_prof && cudaMalloc(&ctx->d_prof, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      ctx->d_prof = nullptr;
+      return set_error(ctx, SPX_ENOMEM, "profile counters");
+    }
+    int rc = check_cuda(ctx, cudaMemsetAsync(ctx->d_prof, 0, bytes, ctx->stream), "profile counters");
+    if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "profile counters");
+    if (rc) return rc;
+  }
+  ctx->prof_on = on != 0;
+  return SPX_OK;
+}
+
+extern "C" int spx_pb_profile_read(spx_ctx* ctx, double* out, int32_t n) {
+  if (!ctx || !out || n < 0) return SPX_EINVAL;
+  cudaSetDevice(ctx->device);
+  unsigned long long v[SPX_PB_PROF_N] = {};
+  if (ctx->d_prof) {
+    int rc = check_cuda(ctx, cudaDeviceSynchronize(), "profile read");
+    if (!rc) rc = check_cuda(ctx, cudaMemcpy(v, ctx->d_prof, sizeof(v), cudaMemcpyDeviceToHost), "profile read");
+    if (rc) return rc;
+  }
+  for (int k = 0; k < n && k < SPX_PB_PROF_N; ++k) out[k] = (double)v[k];
   return SPX_OK;
 }
 

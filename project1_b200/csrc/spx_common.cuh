@@ -47,12 +47,19 @@ struct spx_ctx {
   std::vector<BatchGraph> graphs;
   uint64_t graph_clock = 0;
   void* dn = nullptr;  // dense-solver handle of the dielectric inversion, made on first use
+  // role profile of the persistent schedule (spx_pb_profile_*)
+  unsigned long long* d_prof = nullptr;
+  bool prof_on = false;
 };
 
 namespace spx {
 
 // device status codes written by kernels into ctx->d_status
 enum : int { kStatusOk = 0, kStatusTimeout = 1, kStatusBadLaunch = 2 };
+
+// Tile code of the persistent schedule (tile columns + 256 x pipeline stages) when no
+// tuning entry names one: 64 x 80 complex tiles, three stages.
+constexpr int kPbDefaultTile = 80 + 3 * 256;
 
 int set_error(spx_ctx* ctx, int code, const std::string& msg);
 int check_cuda(spx_ctx* ctx, cudaError_t e, const char* what);

@@ -345,6 +345,22 @@ class Context:
         rc = self.lib.spx_tune_lookup_batched(self.handle, nbas, npair, nw, C.byref(e))
         return _stats(e) if rc == 0 else None
 
+    PB_PROFILE_FIELDS = ("cta", "tma_wait_planes", "tma_wait_stage", "mma_wait_operands",
+                         "mma_wait_epilogue", "mma_wait_item", "epilogue_wait_tile",
+                         "epilogue_wait_order", "prep_wait", "prep_m", "prep_weights",
+                         "prep_planes", "accumulation_items", "preparation_items")
+
+    def pb_profile_enable(self, on: bool = True) -> None:
+        """Role cycle counters of the persistent schedule: zeroed and switched on (or off)."""
+        self._check(self.lib.spx_pb_profile_enable(self.handle, 1 if on else 0), "spx_pb_profile_enable")
+
+    def pb_profile_read(self) -> dict:
+        """The counters summed since the last enable (waits for the device)."""
+        n = len(self.PB_PROFILE_FIELDS)
+        out = (C.c_double * n)()
+        self._check(self.lib.spx_pb_profile_read(self.handle, out, n), "spx_pb_profile_read")
+        return dict(zip(self.PB_PROFILE_FIELDS, list(out)))
+
     def tune_save(self, path: str) -> None:
         self._check(self.lib.spx_tune_save(self.handle, str(path).encode()), "spx_tune_save")
 

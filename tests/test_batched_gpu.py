@@ -154,8 +154,7 @@ def test_autotuned_batch(ctx):
     ctx.chi0_batched(qs, omega, flags=_lib.SPX_BATCH_AUTOTUNE, stats=True)
     for q in qs:
         t = ctx.tune_lookup_batched(q["nbas"], q["npair"], 2)
-        assert t is not None and t["variant"] == 4 and t["tile"] in (64 + 3 * 256, 32 + 3 * 256, 32 + 4 * 256,
-                                                                      80 + 3 * 256)
+        assert t is not None and t["variant"] == 4 and t["tile"] in (64 + 3 * 256, 80 + 3 * 256, 32 + 4 * 256)
         assert torch.isfinite(torch.view_as_real(q["susceph"])).all()
         assert q["susceph"].abs().max() > 0
 
@@ -186,7 +185,7 @@ def _force_tile(c, tmp_path, qs, nw, tile, slab):
 @pytest.mark.parametrize("tile", [64 + 3 * 256, 32 + 3 * 256, 32 + 4 * 256, 80 + 3 * 256])
 def test_persistent_tile_shapes_equal_per_q_calls(tmp_path, tile):
     """Every tile shape of the persistent schedule gives the per-q result bit for bit,
-    with the slab ring reused many times (4096-pair slabs, 3 buffers) and a q whose
+    with the slab ring reused many times (4096-pair slabs, 4 buffers) and a q whose
     weights change sign (negative energy differences)."""
     omega = torch.from_numpy(inputs.frequencies(3)).to(DEV)
     with spx.Context(0) as c:
@@ -224,3 +223,27 @@ def test_persistent_and_kernel_schedules_agree(ctx):
     assert st["kernel_launches"] > 1
     for q, x in zip(qs, a):
         assert torch.equal(q["susceph"], x)
+
+
+def test_persistent_role_profile():
+    """The role counters count every accumulation item of the batch (tiles x
+    frequencies x slabs, 64 x 80 tiles untuned) and each role's waits fit inside
+    the CTAs' cycles."""
+    omega = torch.from_numpy(inputs.frequencies(2)).to(DEV)
+    with spx.Context(0) as c:
+        qs = [_q(n, p, 2, 80 + i, gen, slab=8192) for i, (n, p, gen) in
+              enumerate([(200, 20000, True), (96, 9000, False)])]
+        c.pb_profile_enable(True)
+        c.chi0_batched(qs, omega, flags=_lib.SPX_BATCH_NOGRAPH)
+        prof = c.pb_profile_read()
+        c.pb_profile_enable(False)
+
+    def ntile80(n):   # 64-row blocks x 80-column blocks of the upper triangle
+        nbr = (n + 63) // 64
+        return sum(min((j * 80 + 79) // 64, nbr - 1) + 1 for j in range((n + 79) // 80))
+    items = sum(ntile80(q["nbas"]) * 2 * -(-q["npair"] // 8192) for q in qs)
+    assert prof["accumulation_items"] == items
+    assert prof["preparation_items"] > 0 and prof["cta"] > 0
+    for k, v in prof.items():
+        if not k.endswith("_items"):
+            assert 0 <= v <= prof["cta"], k

@@ -170,3 +170,23 @@ def test_split_host_ramp_equals_device_path_tuned(tmp_path, variant, slab):
         c.chi0_accumulate_host_ptr(t.data_ptr(), npair, npair, nbas, d, om, out,
                                    scale_all=0.5, precision="split")
     assert np.array_equal(out, dev)
+
+
+@pytest.mark.parametrize("variant", [5, 1])
+def test_split_tuned_slab_below_one_slab_of_pairs(tmp_path, variant):
+    """A tuned 8192-pair slab on 16000 pairs takes two buffers of 8192 pairs, more
+    than one buffer of the 16000 pairs the untuned call needs: the call sizes its
+    scratch for the slab it runs."""
+    import json
+    nbas, npair, nw = 100, 16000, 2
+    m, d, om = random_case(nbas, npair, nw, seed=23, degfrac=0.01)
+    table = tmp_path / "tune.json"
+    table.write_text(json.dumps({"format": "spexgpu-tune-1", "entries": [
+        {"nbas_bucket": 1, "npair_bucket": 0, "nw": nw, "variant": variant, "slab_pairs": 8192,
+         "tile": 0, "tflops": 1.0}]}))
+    ref = oracle.chi0(m, oracle.weights(d, om, None, 0.5), accurate=True)
+    with spx.Context(0) as c:
+        c.tune_load(str(table))
+        got = run_dev(c, m, d, om, None, 0.5, precision="split")
+    emax, fro = normalized_error(got, ref, nbas)
+    assert emax <= SPLIT_TOL and fro <= SPLIT_FRO, (emax, fro)
