@@ -627,6 +627,22 @@ def bench_batched(args, dev, stream):
                "max_normalized": max(x["max_normalized"] for x in per_q),
                "raw_rel_max": max(x["raw_rel_max"] for x in per_q)}
         del sub
+    # the same batch as per-slab kernels (generation, quantizer, one-CTA accumulation)
+    # replayed from one graph: the schedule the persistent kernel replaces, for comparison
+    for q in qs:
+        q["susceph"].zero_()
+    ctx.chi0_batched(qs, omega, flags=_lib.SPX_BATCH_KERNELS | (_lib.SPX_BATCH_AUTOTUNE if args.autotune else 0),
+                     stream=stream.cuda_stream)
+    for q in qs:
+        q["susceph"].zero_()
+    e0.record(stream)
+    stk = ctx.chi0_batched(qs, omega, flags=_lib.SPX_BATCH_KERNELS, stream=stream.cuda_stream, stats=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_k = e0.elapsed_time(e1)
+    slab_kernels = {"value": flops / (ms_k * 1e-3) / 1e12, "ms_per_step": ms_k,
+                    "kernels_per_step": stk["kernel_launches"],
+                    "note": "SPX_BATCH_KERNELS: the per-slab kernels of the single call in one graph"}
     res = {"workload": f"c3: {len(qws)} q, N_MB U{{{bw.nbas_range[0]}..{bw.nbas_range[1]}}}, "
                        f"occ U{{{bw.occ_range[0]}..{bw.occ_range[1]}}} x unocc "
                        f"U{{{bw.unocc_range[0]}..{bw.unocc_range[1]}}}, {bw.nk} k, {bw.nw} freqs, split",
@@ -640,7 +656,7 @@ def bench_batched(args, dev, stream):
                                     for t in tune if t}),
            "schedule": "one persistent kernel per batch (accumulation and operand-preparation "
                        "queues on every SM), captured in a CUDA graph",
-           "m_generated_on_device": True, "clocks": clocks,
+           "m_generated_on_device": True, "clocks": clocks, "slab_kernels": slab_kernels,
            "role_profile": dict(role, note="cycles of one thread per role and CTA as a fraction of the "
                                            "CTAs' cycles (spx_pb_profile_read), summed over the timed batches"),
            "accuracy": acc}

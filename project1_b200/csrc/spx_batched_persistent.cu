@@ -116,8 +116,10 @@ __device__ __forceinline__ void fence_proxy_async_global() {
 // usually there already); the spinning is a call, so its code exists once.
 __device__ __noinline__ bool gwait_spin(const int* ctr, int target, uint64_t timeout_ns, int* status) {
   const uint64_t t0 = global_ns();
+  uint32_t nap = 64;  // doubling up to 2 us: long waits (a buffer, a slab) poll rarely
   for (uint32_t n = 1;; ++n) {
-    __nanosleep(64);
+    __nanosleep(nap);
+    if (nap < 2048) nap <<= 1;
     if (ld_acquire(ctr) >= target) return true;
     if ((n & 31) == 0) {
       if (global_ns() - t0 > timeout_ns) {
