@@ -407,8 +407,10 @@ typedef struct spx_tune_entry {
   double  tflops;           /* measured throughput of the chosen configuration        */
 } spx_tune_entry;
 
-/* Measures the candidates on a seeded probe of (nbas, min(npair, 262144), nw),
- * stores the best in the table and returns it in *out (may be NULL). */
+/* Measures the candidates (kernel variants 1, 5, 2, 3 x slabs of 8192, 12288, 16384
+ * and 32768 pairs) on a seeded probe of (nbas, min(npair, 262144), nw), stores the
+ * best in the table (the best kernel's smallest slab within 2 % of its fastest) and
+ * returns it in *out (may be NULL). */
 int spx_autotune_split(spx_ctx* ctx, int32_t nbas, int64_t npair, int32_t nw,
                        spx_tune_entry* out);
 /* SPX_OK and *out if the bucket of (nbas, npair, nw) is in the table, else SPX_ENOTSUP. */

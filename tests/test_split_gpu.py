@@ -150,7 +150,7 @@ def test_split_host_ramp_equals_device_path(ctx):
     assert np.array_equal(out, dev)
 
 
-@pytest.mark.parametrize("variant,slab", [(5, 8192), (1, 16384), (3, 8192)])
+@pytest.mark.parametrize("variant,slab", [(5, 8192), (5, 12288), (1, 16384), (3, 8192)])
 def test_split_host_ramp_equals_device_path_tuned(tmp_path, variant, slab):
     """With a tuning entry (kernel and slab) for the array's shape, the host-pointer
     call cuts its chunks on that slab and runs that kernel for every chunk, so it
